@@ -1,0 +1,378 @@
+#!/usr/bin/env python3
+"""Benchmark: Mrays/s of the plain GPU wavefront on config 2 (1 x B200 per rank).
+
+Workload (config 2): icosphere level 8 (1,310,720 triangles) displaced by 4-octave value noise
+of amplitude 0.15 r, GGX conductor roughness 0.3, 50x50 ground quad, sun 3.0 + gradient sky,
+1920x1080, max depth 10, Russian roulette from bounce 3; synthetic, seed 1. One step = one
+sample of every pixel (2,073,600 paths: camera rays, bounce rays and NEE shadow rays).
+
+  value        rays traced (closest + shadow) / device time of the K timed steps (CUDA events on
+               the renderer's stream), summed over ranks / max over ranks
+  e2e          the same metric through the public C ABI with host buffers: xb_render + xb_resolve
+               into pinned host memory every step (the framebuffer hand-off CudaRenderer does per
+               sample), host wall clock
+  roofline     the closest-hit traversal kernel (extend): algorithmic bytes per launch ÷ its
+               average launch time (CUDA events around each launch), against measured HBM GB/s
+  cpu_baseline the reference's own CPU backend (render_frame_tiled, Release flags, all host
+               threads) on a bounded sample of the same view; its Mrays/s uses the rays per path
+               this GPU run measured (the reference counts no rays)
+
+Multi-GPU (torchrun): each rank renders its own sample indices (rank r renders samples
+r*K+1 ...), so per-GPU work is fixed (weak scaling); the only exchange is one NCCL reduce of
+the framebuffer after the timed region.
+
+--impl reference times the reference's CPU implementation of this path on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s; equal-time relMSE, guided vs plain GPU wavefront (1×B200)"
+WORKLOAD = "config2: displaced icosphere L8 (1,310,722 tris incl. ground) 1920x1080, depth 10, 1 spp/step"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = config 2)")
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--thread-per-ray", action="store_true", help="one-ray-per-thread traversal kernels")
+    return ap.parse_args()
+
+
+def load_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(n_gpus: int):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def allreduce_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_sample(desc, rays_per_path: float | None, budget_s: float, threads_note: bool = True) -> dict:
+    """The reference CPU backend on a bounded sample of the same view (fewer pixels, same camera)."""
+    from oracle import ref
+    if not ref.available("fast"):
+        return {"value": None, "unit": "Mrays/s", "cores": None, "kind": "reference",
+                "sample": "oracle/_ref/libxnref_fast.so not built"}
+    L = ref.lib("fast")
+    cores = int(L.xr_hardware_threads())
+    w, h = desc.width // 8, desc.height // 8
+    rs = ref.RefScene(desc, flavour="fast")
+    rr = ref.RefRenderer(w, h, desc.min_bounces, desc.max_bounces, flavour="fast")
+    _, t1 = rr.render(rs, desc.eye, desc.target, desc.fov, 1, 1)
+    spp = int(max(1, min(256, budget_s / max(t1, 1e-3))))
+    _, secs = rr.render(rs, desc.eye, desc.target, desc.fov, 2, spp)
+    paths = w * h * spp
+    msps = paths / secs / 1e6
+    out = {"unit": "Mrays/s", "cores": cores, "kind": "reference",
+           "msamples_per_s": msps, "seconds": secs,
+           "sample": f"{w}x{h} px (1/64 of the pixels, same camera) x {spp} spp of config 2, "
+                     f"render_frame_tiled with Release flags on {cores} threads; Mrays/s = Msamples/s x "
+                     f"rays per path measured on the GPU for this config (derived: the reference counts no rays)"}
+    out["value"] = msps * rays_per_path if rays_per_path else None
+    return out
+
+
+def rays_per_path_port(desc, paths: int = 4096) -> float:
+    """Rays per path of this estimator, counted by the CPU restatement (oracle/) on a sample."""
+    from oracle import port
+    return port.rays_per_path(desc, paths)
+
+
+def run_reference(args):
+    """--impl reference: the reference's own CPU implementation of the path, host threads."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import ref
+    from xenon_b200 import scenes
+    desc = scenes.icosphere_scene(level=args.level, width=args.width, height=args.height)
+    if not ref.available("fast"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libxnref_fast.so was not built"}))
+        return 0
+    try:
+        rpp = rays_per_path_port(desc)
+    except Exception as e:  # the restatement is missing: report samples only
+        rpp = None
+    L = ref.lib("fast")
+    cores = int(L.xr_hardware_threads())
+    w, h = desc.width // 8, desc.height // 8
+    rs = ref.RefScene(desc, flavour="fast")
+    rr = ref.RefRenderer(w, h, desc.min_bounces, desc.max_bounces, flavour="fast")
+    spp_per_step = 1
+    for s in range(args.warmup):
+        rr.render(rs, desc.eye, desc.target, desc.fov, 1 + s, spp_per_step)
+    secs = 0.0
+    for s in range(args.steps):
+        _, t = rr.render(rs, desc.eye, desc.target, desc.fov, 1000 + s, spp_per_step)
+        secs += t
+    paths = w * h * spp_per_step * args.steps
+    msps = paths / secs / 1e6
+    value = msps * rpp if rpp else msps
+    unit = "Mrays/s" if rpp else "Msamples/s"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": unit, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": WORKLOAD, "sample_per_step": f"{w}x{h} px x {spp_per_step} spp (1/64 of the pixels)",
+                       "rays_per_path": rpp, "msamples_per_s": msps},
+            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "reference",
+                             "sample": f"{w}x{h} px x {spp_per_step} spp per step, render_frame_tiled, Release flags, {cores} threads"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    ws, rank, local = dist_setup(args.gpus)
+    import torch
+    import xenon_b200 as xb
+    from xenon_b200 import abi, scenes
+
+    torch.cuda.set_device(local)
+    desc = scenes.icosphere_scene(level=args.level, width=args.width, height=args.height)
+    W, H = desc.width, desc.height
+    hs = xb.HostScene.from_desc(desc)
+    r = xb.Renderer(W, H, desc.max_bounces, desc.min_bounces, device=local,
+                    flags=abi.XB_FLAG_THREAD_PER_RAY if args.thread_per_ray else 0)
+    r.upload_scene(hs)
+    cam = xb.camera(desc.eye, desc.target, desc.fov, W / H)
+    npix = W * H
+
+    # traversal work per ray (untimed pass with counters), for the roofline's algorithmic bytes
+    r.set_profiling(abi.XB_PROFILE_COUNT_TRAVERSAL)
+    r.reset_stats()
+    r.reset_profile()
+    r.render_range(cam, 100000, 1)
+    cst = r.stats()
+    cpr = r.profile()
+    n_ext = cst.rays_closest
+    ext_bytes_per_ray = (64 * cpr.ext_blas_nodes + 48 * cpr.ext_tris + 32 * cpr.ext_tlas_nodes +
+                         48 * cpr.ext_instances) / n_ext + 32 + 20
+    n_sh = max(cst.rays_shadow, 1)
+    work = {"blas_nodes_per_ray": cpr.ext_blas_nodes / n_ext, "tris_per_ray": cpr.ext_tris / n_ext,
+            "tlas_nodes_per_ray": cpr.ext_tlas_nodes / n_ext, "instances_per_ray": cpr.ext_instances / n_ext,
+            "shadow_blas_nodes_per_ray": cpr.sh_blas_nodes / n_sh, "shadow_tris_per_ray": cpr.sh_tris / n_sh}
+    r.reset()
+
+    # warm-up
+    r.set_profiling(0)
+    base = rank * (args.steps + args.warmup + 8) + 1
+    for s in range(args.warmup):
+        r.render_range(cam, base + s, 1)
+    r.reset()
+    r.reset_stats()
+    r.reset_profile()
+    r.set_profiling(abi.XB_PROFILE_STAGE_TIMES)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    barrier(ws)
+    torch.cuda.synchronize()
+    dev_ms = 0.0
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            flush.zero_()                      # L2 flush between timed steps (outside the events)
+            torch.cuda.synchronize()
+            r.render_range(cam, base + args.warmup + s, 1)
+            dev_ms += r.stats().last_ms
+    torch.cuda.synchronize()
+    barrier(ws)
+    st = r.stats()
+    prof = r.profile()
+    rays = st.rays_closest + st.rays_shadow
+    t_max = allreduce_max(dev_ms, ws)
+    rays_all = allreduce_sum(float(rays), ws)
+    value = rays_all / (t_max * 1e-3) / 1e6
+    msamples = allreduce_sum(float(st.paths), ws) / (t_max * 1e-3) / 1e6
+    rays_per_path = rays / st.paths
+    launches = (prof.raygen_launches + prof.extend_launches + prof.shade_launches + prof.shadow_launches +
+                prof.accumulate_launches)
+
+    # roofline of the extend kernel: algorithmic bytes per launch / mean launch time
+    peaks = load_peaks()
+    ext_bytes = ext_bytes_per_ray * st.rays_closest
+    ext_launch_ms = prof.extend_ms / max(prof.extend_launches, 1)
+    ext_bytes_per_launch = ext_bytes / max(prof.extend_launches, 1)
+    achieved = ext_bytes_per_launch / (ext_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "extend_kernel_config2.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        if tj.get("dram_bytes_per_closest_ray"):
+            traffic = tj["dram_bytes_per_closest_ray"] * st.rays_closest / max(prof.extend_launches, 1)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                "peak_source": peaks["source"], "kernel": "extend_kernel (closest-hit traversal)",
+                "algorithmic_bytes_per_ray": ext_bytes_per_ray, "extend_share_of_step":
+                    prof.extend_ms / max(dev_ms, 1e-9), **work}
+
+    # e2e through the public API with host buffers: render + resolve to pinned host memory
+    host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True)
+    r.reset()
+    r.reset_stats()
+    r.set_profiling(0)
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_steps = max(3, min(args.steps, 10))
+    L = xb.lib()
+    for s in range(e2e_steps):
+        xb.native.check(L.xb_render(r.h, ctypes.byref(cam), 1), r.h)
+        xb.native.check(L.xb_resolve(r.h, ctypes.c_void_p(host.data_ptr())), r.h)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = allreduce_max(e2e_s, ws)
+    st2 = r.stats()
+    e2e_rays = allreduce_sum(float(st2.rays_closest + st2.rays_shadow), ws)
+    e2e = {"value": e2e_rays / e2e_s / 1e6, "unit": "Mrays/s",
+           "h2d_bytes_per_step": int(ctypes.sizeof(cam)),
+           "d2h_bytes_per_step": int(W * H * 3 * 4)}
+
+    # the single exchange of the multi-GPU path: framebuffer reduce to rank 0 (untimed)
+    if ws > 1:
+        import torch.distributed as dist
+        img = torch.from_numpy(r.resolve()).cuda()
+        dist.reduce(img, dst=0)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_sample(desc, rays_per_path, args.cpu_seconds)
+        except Exception as e:
+            cpu = {"value": None, "unit": "Mrays/s", "cores": None, "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded procedural scene, seed 1)",
+                "config": {"workload": WORKLOAD, "paths_per_step": npix, "rays_per_path": rays_per_path,
+                           "msamples_per_s": msamples, "l2": "flushed between timed steps (256 MiB write)",
+                           "parallelism": f"sample-sharded x{ws}" if ws > 1 else "1 GPU",
+                           "stage_ms_per_step": {k: getattr(prof, k) / args.steps for k in
+                                                 ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms")}},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clk.summary()}
+        print(json.dumps(line))
+    r.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,329 @@
+/*
+ * xenon_b200.h — C ABI of the B200-native wavefront path tracer.
+ *
+ * This is the drop-in boundary for Xenon's GPU backend. Each entry point names the
+ * reference interface it replaces (paths are relative to the Xenon source tree):
+ *
+ *   xb_create / xb_destroy     xn::CudaRenderer::CudaRenderer / ~CudaRenderer
+ *                              (src/cuda/cuda_renderer.cuh:16-17, cuda_renderer.cu:446-456)
+ *   xb_upload_scene            xn::CudaRenderer::upload_scene (cuda_renderer.cuh:23) and
+ *                              xn::GpuSceneHost::upload (src/cuda/gpu_scene.cu:38)
+ *   xb_render                  xn::CudaRenderer::render_frame (cuda_renderer.cuh:26), which adds
+ *                              one sample per pixel; here `spp_to_add` samples per call
+ *   xb_resolve                 the framebuffer hand-off TripleSwapchain::get_write_buffer()
+ *                              + swap_writer() (src/render/swapchain.h:30-46), with the CPU
+ *                              backend's top-down row order (src/render/cpu_tiled.cpp:224-236)
+ *   xb_get_spp                 xn::CudaRenderer::spp (cuda_renderer.cuh:28)
+ *   xb_reset                   xn::WavefrontRenderer::reset_accumulation (src/render/wavefront.h:22)
+ *   xb_set_bounces             xn::WavefrontRenderer::set_bounces (src/render/wavefront.h:30)
+ *   xb_trace_rays              xn::Scene::intersect / intersects (src/scene/scene.h:124-129)
+ *   xb_bsdf_eval               xn::bsdf_eval_for_nee / bsdf_pdf_for_nee (src/material/bsdf.h:601-657)
+ *   xb_bsdf_sample             xn::bsdf_sample (src/material/bsdf.h:666-708)
+ *   xb_scene_*                 xn::Scene building (src/scene/scene.h:52-121), the .xenon loader
+ *                              xn::load_scene (src/scene/scene_file.h:22) and the .mat loader
+ *                              xn::load_material (src/material/material.h:81)
+ *
+ * Conventions: every function returns XB_OK (0) or a negative XB_E_* status and never aborts.
+ * xb_last_error() returns the message of the last failure on the calling thread. One renderer
+ * is used by one host thread at a time. Host pointers unless a name says `device`.
+ */
+#ifndef XENON_B200_H
+#define XENON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ── status codes ─────────────────────────────────────────────────────────── */
+#define XB_OK             0
+#define XB_E_INVALID     -1   /* bad argument */
+#define XB_E_CUDA        -2   /* a CUDA runtime call failed */
+#define XB_E_OOM         -3   /* device or host allocation failed */
+#define XB_E_STATE       -4   /* call out of order (e.g. render before upload) */
+#define XB_E_IO          -5   /* file missing or unparsable */
+#define XB_E_OVERFLOW    -6   /* a device queue or traversal stack overflowed (work dropped) */
+#define XB_E_TIMEOUT     -7   /* a bounded device wait gave up */
+#define XB_E_UNSUPPORTED -8
+
+/* ── scene data formats (POD, identical bytes to the reference structs) ─────── */
+
+/* Principled material authoring parameters (src/material/material.h:19-36). */
+typedef struct xb_material {
+  float base_color[3];
+  float roughness;
+  float metallic;
+  float ior;
+  float transmission;
+  float subsurface;
+  float subsurface_color[3];
+  float anisotropy;
+  float emission[3];
+  float subsurface_mfp[3];
+  float clearcoat;
+  float clearcoat_roughness;
+  float emission_temperature;
+} xb_material;
+
+/* Values material_prepare derives (src/material/material.h:55-75). */
+#define XB_MAT_CONDUCTOR    1
+#define XB_MAT_TRANSMISSIVE 2
+#define XB_MAT_SUBSURFACE   4
+#define XB_MAT_DELTA        8
+#define XB_MAT_EMISSIVE     16
+typedef struct xb_material_derived {
+  float alpha, alpha_x, alpha_y;
+  float f0[3];
+  int32_t flags;
+} xb_material_derived;
+
+/* BVH node: BLASNode / TLASNode / PrimBLASNode (src/geometry/blas.h:21-27), 32 bytes.
+ * count == 0: internal, children at `child` and `child + 1`; count > 0: leaf. */
+typedef struct xb_bvh_node {
+  float mn[3];
+  float mx[3];
+  uint32_t child;
+  uint32_t count;
+} xb_bvh_node;
+
+/* Analytic primitive (src/geometry/primitives.h:54-318). Parameter layout per type:
+ *   SPHERE center[3] radius          PLANE normal[3] offset
+ *   BOX    center[3] half[3]         DISK  center[3] normal[3] radius
+ *   QUAD   origin[3] u[3] v[3] */
+#define XB_PRIM_SPHERE 0
+#define XB_PRIM_PLANE  1
+#define XB_PRIM_BOX    2
+#define XB_PRIM_DISK   3
+#define XB_PRIM_QUAD   4
+typedef struct xb_prim {
+  int32_t type;
+  int32_t mat_id;
+  float p[10];
+} xb_prim;
+
+/* Triangle mesh (src/geometry/mesh.h:21-31) with its BLAS (src/geometry/blas.h:61-62). */
+typedef struct xb_mesh_view {
+  int32_t num_vertices;
+  int32_t num_triangles;
+  const float *vx, *vy, *vz;          /* positions, SoA */
+  const float *nx, *ny, *nz;          /* shading normals, SoA; NULL → geometric normal */
+  const int32_t *indices;             /* 3 per triangle */
+  const int32_t *mat_ids;             /* 1 per triangle */
+  const xb_bvh_node *blas_nodes;
+  int32_t num_blas_nodes;
+  const uint32_t *blas_prims;         /* num_triangles entries */
+} xb_mesh_view;
+
+/* TLAS instance (src/geometry/tlas.h:76-87): column-major 3x4 affine matrices
+ * (c0, c1, c2 basis columns, c3 translation; src/geometry/transform.h:32-63). */
+#define XB_GEOM_PRIMS (-1)
+typedef struct xb_instance_view {
+  int32_t geom;                       /* mesh index, or XB_GEOM_PRIMS for the prim group */
+  int32_t instance_id;
+  float local_to_world[12];
+  float world_to_local[12];
+} xb_instance_view;
+
+/* Area light: one emitting triangle (src/scene/scene.h:19-24). */
+typedef struct xb_light {
+  uint32_t mesh_id;
+  uint32_t tri_idx;
+  float emission[3];
+  float area;
+} xb_light;
+
+/* Directional light (src/scene/scene.h:43-49). direction points toward the light. */
+typedef struct xb_sun {
+  float direction[3];
+  float color[3];
+  float intensity;
+} xb_sun;
+
+/* Gradient sky (src/scene/environment.h:14-39). */
+typedef struct xb_sky {
+  float zenith[3];
+  float horizon[3];
+  float ground[3];
+  float sharpness;
+  float intensity;
+} xb_sky;
+
+/* Flattened scene: everything the device needs. Pointers are host memory, owned by the
+ * caller; xb_upload_scene copies them. */
+typedef struct xb_scene_view {
+  int32_t num_meshes;
+  const xb_mesh_view *meshes;
+  int32_t num_prims;
+  const xb_prim *prims;
+  const xb_bvh_node *prim_nodes;
+  int32_t num_prim_nodes;
+  const uint32_t *prim_indices;
+  int32_t num_instances;
+  const xb_instance_view *instances;
+  const xb_bvh_node *tlas_nodes;
+  int32_t num_tlas_nodes;
+  const uint32_t *tlas_inst_indices;
+  int32_t num_materials;
+  const xb_material *materials;
+  int32_t num_lights;
+  const xb_light *lights;
+  int32_t num_suns;
+  const xb_sun *suns;
+  xb_sky sky;
+} xb_scene_view;
+
+/* Ray (src/math/ray.h:119-126) as two 16-byte halves. */
+typedef struct xb_ray {
+  float org[3];
+  float tmin;
+  float dir[3];
+  float tmax;
+} xb_ray;
+
+/* Hit record (src/math/ray.h:131-143). A miss has t = +inf and ids = -1. */
+typedef struct xb_hit {
+  float t, u, v;
+  int32_t prim_id;
+  int32_t instance_id;
+  int32_t mat_id;
+  int32_t front_face;
+  float pos[3];
+  float normal[3];
+  float geo_normal[3];
+} xb_hit;
+
+/* Pinhole camera as the device sees it (Camera::look_at, src/camera/camera.h:15-31). */
+typedef struct xb_camera {
+  float eye[3];
+  float lower_left[3];
+  float horizontal[3];
+  float vertical[3];
+} xb_camera;
+
+/* ── host scene: loaders and the TLAS/BLAS build ──────────────────────────── */
+
+typedef struct xb_scene xb_scene;
+
+typedef struct xb_scene_config {     /* xn::SceneConfig (src/scene/scene_file.h:11-19) */
+  int32_t width, height, samples;
+  int32_t min_bounces, max_bounces;
+} xb_scene_config;
+
+typedef struct xb_camera_desc {      /* the .xenon `camera` line */
+  float eye[3];
+  float target[3];
+  float fov_y_deg;
+} xb_camera_desc;
+
+void xb_material_default(xb_material *m);
+int  xb_material_prepare(const xb_material *m, xb_material_derived *out);
+int  xb_material_load(const char *path, xb_material *out, char *name, size_t name_len);
+int  xb_camera_look_at(const float eye[3], const float target[3], const float up[3],
+                       float fov_y_deg, float aspect, xb_camera *out);
+
+int  xb_scene_create(xb_scene **out);
+void xb_scene_destroy(xb_scene *s);
+/* Each add returns the new object's id (>= 0) or a negative status. */
+int  xb_scene_add_material(xb_scene *s, const char *name, const xb_material *m);
+int  xb_scene_add_mesh(xb_scene *s, int32_t num_vertices, const float *positions,
+                       const float *normals, int32_t num_triangles, const int32_t *indices,
+                       const int32_t *mat_ids, int32_t default_mat_id);
+int  xb_scene_transform_mesh(xb_scene *s, int32_t mesh, const float pos[3], float scale,
+                             const float rot_deg[3]);
+int  xb_scene_add_prim(xb_scene *s, const xb_prim *p);
+int  xb_scene_add_light(xb_scene *s, uint32_t mesh_id, uint32_t tri_idx,
+                        const float emission[3], float area);
+int  xb_scene_add_sun(xb_scene *s, const float direction[3], const float color[3],
+                      float intensity);
+int  xb_scene_set_sky(xb_scene *s, const xb_sky *sky);
+/* Explicit TLAS instances (AffineTransform::from_trs, src/geometry/transform.h:105). With none,
+ * xb_scene_build makes one identity instance per mesh plus one for the prim group, as
+ * Scene::build_acceleration does (src/scene/scene.h:79-121). */
+int  xb_scene_add_instance(xb_scene *s, int32_t geom, const float translation[3], float scale,
+                           const float rot_deg[3], int32_t instance_id);
+int  xb_scene_build(xb_scene *s);
+int  xb_scene_get_view(const xb_scene *s, xb_scene_view *out);
+int  xb_scene_load(const char *path, xb_scene **out, xb_scene_config *cfg, xb_camera_desc *cam);
+
+/* ── renderer ─────────────────────────────────────────────────────────────── */
+
+typedef struct xb_renderer xb_renderer;
+
+#define XB_FLAG_FP64_ACCUM      1   /* FP64 per-pixel sum + Welford M2 (oracle renders) */
+#define XB_FLAG_THREAD_PER_RAY  2   /* one-ray-per-thread traversal instead of persistent warps */
+
+typedef struct xb_config {
+  int32_t width, height;
+  int32_t max_bounces, min_bounces;  /* CudaRenderer(width, height, max_bounces, min_bounces) */
+  int32_t device;                    /* CUDA device ordinal */
+  int32_t flags;                     /* XB_FLAG_* */
+  int32_t wave_paths;                /* paths in flight per wave; 0 = automatic */
+  int32_t block_size;                /* threads per block of the trace kernels; 0 = automatic */
+} xb_config;
+
+int  xb_create(const xb_config *cfg, xb_renderer **out);
+void xb_destroy(xb_renderer *r);
+int  xb_last_error(const xb_renderer *r, char *buf, size_t len);
+int  xb_upload_scene(xb_renderer *r, const xb_scene_view *view);
+int  xb_set_bounces(xb_renderer *r, int32_t min_bounces, int32_t max_bounces);
+/* Adds spp_to_add samples per pixel; sample k of pixel p is seeded exactly as the CPU backend
+ * seeds it (seed_pcg(p + k * 0xdeadbeef), src/render/cpu_tiled.cpp:22-23). */
+int  xb_render(xb_renderer *r, const xb_camera *cam, int32_t spp_to_add);
+/* Mean radiance, float[W*H*3], top-down rows. */
+int  xb_resolve(xb_renderer *r, float *out_rgb);
+/* FP64 per-pixel sums and Welford M2 (needs XB_FLAG_FP64_ACCUM); each double[W*H*3]. */
+int  xb_resolve_fp64(xb_renderer *r, double *sum_rgb, double *m2_rgb);
+int  xb_get_spp(const xb_renderer *r);
+int  xb_reset(xb_renderer *r);
+/* Renders samples [spp_first, spp_first + spp_count) of the sequence (1-based), e.g. one shard
+ * of a multi-GPU job; xb_render(r, cam, n) equals xb_render_range(r, cam, spp + 1, n). */
+int  xb_render_range(xb_renderer *r, const xb_camera *cam, int32_t spp_first, int32_t spp_count);
+
+typedef struct xb_render_stats {
+  int64_t rays_closest;   /* closest-hit rays traced (camera + bounce) */
+  int64_t rays_shadow;    /* any-hit shadow rays traced */
+  int64_t paths;          /* paths started */
+  int64_t overflow;       /* items dropped by a full queue or traversal stack (must be 0) */
+  float   last_ms;        /* device time of the last xb_render / xb_render_range call */
+} xb_render_stats;
+int  xb_get_render_stats(const xb_renderer *r, xb_render_stats *out);
+int  xb_reset_render_stats(xb_renderer *r);
+
+/* Profiling (tracing subsystem): per-stage device time from CUDA events recorded around every
+ * stage launch on the renderer's stream, and per-ray traversal work counters. */
+#define XB_PROFILE_STAGE_TIMES     1
+#define XB_PROFILE_COUNT_TRAVERSAL 2
+typedef struct xb_profile {
+  double raygen_ms, extend_ms, shade_ms, shadow_ms, accumulate_ms;
+  int64_t raygen_launches, extend_launches, shade_launches, shadow_launches, accumulate_launches;
+  /* traversal work (XB_PROFILE_COUNT_TRAVERSAL): closest-hit (ext_*) and shadow (sh_*) rays */
+  int64_t ext_blas_nodes, ext_tris, ext_tlas_nodes, ext_instances;
+  int64_t sh_blas_nodes, sh_tris, sh_tlas_nodes, sh_instances;
+} xb_profile;
+int  xb_set_profiling(xb_renderer *r, int32_t flags);
+int  xb_get_profile(const xb_renderer *r, xb_profile *out);
+int  xb_reset_profile(xb_renderer *r);
+
+/* Ray queries against the uploaded scene. mode 0 = closest hit (Scene::intersect),
+ * 1 = any hit (Scene::intersects: hits[i].t = 0 when occluded, +inf when not). */
+#define XB_TRACE_CLOSEST 0
+#define XB_TRACE_ANY     1
+int  xb_trace_rays(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit *hits, int32_t mode);
+/* Same on device memory and a caller stream (cudaStream_t, NULL = default). */
+int  xb_trace_rays_device(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit *hits,
+                          int32_t mode, void *stream);
+
+/* BSDF on the device, host buffers: wo, wi float[n*3] in the shading frame (z = normal). */
+int  xb_bsdf_eval(const xb_material *m, int64_t n, const float *wo, const float *wi,
+                  float *f_rgb, float *pdf);
+/* rng_state: uint64[n] PCG32 states (increment 1), advanced in place. flags bit0 = sample valid,
+ * bit1 = delta lobe. */
+int  xb_bsdf_sample(const xb_material *m, int64_t n, const float *wo, uint64_t *rng_state,
+                    float *wi, float *f_rgb, float *pdf, int32_t *flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XENON_B200_H */

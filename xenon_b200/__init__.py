@@ -1,0 +1,227 @@
+"""xenon_b200 — B200-native wavefront path tracer behind Xenon's renderer-backend API.
+
+Python face of the C ABI in include/xenon_b200.h (the C++17 face is csrc/b200_renderer.h):
+
+    scene = HostScene.from_desc(desc)          # or HostScene.load("scene.xenon")
+    r = Renderer(width, height, max_bounces, min_bounces)   # CudaRenderer(w, h, max, min)
+    r.upload_scene(scene)                      # CudaRenderer::upload_scene
+    r.render_frame(camera, spp=1)              # CudaRenderer::render_frame (adds samples)
+    img = r.resolve()                          # float32 [H, W, 3], top-down rows
+    r.spp                                      # CudaRenderer::spp
+
+Every call goes to libxenon_b200.so; there is no CPU path. Failures raise XenonError.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import abi
+from .native import XenonError, check, lib
+
+__all__ = ["HostScene", "Renderer", "XenonError", "camera", "abi", "lib"]
+
+
+def _p(a):
+    # data_as keeps a reference to the array for as long as the pointer object lives
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def camera(eye, target, fov: float, aspect: float, up=(0.0, 1.0, 0.0)) -> abi.Camera:
+    """Camera::look_at (src/camera/camera.h:15-31) → the device camera."""
+    c = abi.Camera()
+    e = np.asarray(eye, np.float32)
+    t = np.asarray(target, np.float32)
+    u = np.asarray(up, np.float32)
+    check(lib().xb_camera_look_at(_p(e), _p(t), _p(u), float(fov), float(aspect), ctypes.byref(c)))
+    return c
+
+
+def material_prepare(m: np.ndarray) -> abi.MaterialDerived:
+    out = abi.MaterialDerived()
+    mm = np.ascontiguousarray(m, np.float32)
+    check(lib().xb_material_prepare(_p(mm), ctypes.byref(out)))
+    return out
+
+
+class HostScene:
+    """Host-side scene: meshes, prims, materials, lights, sky and the TLAS/BLAS build."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        check(lib().xb_scene_create(ctypes.byref(h)))
+        self.h = h
+        self.config = None
+        self.camera_desc = None
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().xb_scene_destroy(self.h)
+            self.h = None
+
+    @classmethod
+    def from_desc(cls, desc) -> "HostScene":
+        s = cls()
+        L = lib()
+        for name, m in zip(desc.material_names, desc.materials):
+            arr = np.ascontiguousarray(m, np.float32)
+            check(L.xb_scene_add_material(s.h, name.encode(), _p(arr)))
+        for mesh in desc.meshes:
+            pos = np.ascontiguousarray(mesh.positions, np.float32)
+            nrm = None if mesh.normals is None else np.ascontiguousarray(mesh.normals, np.float32)
+            idx = np.ascontiguousarray(mesh.indices, np.int32)
+            mat = None if mesh.mat_ids is None else np.ascontiguousarray(mesh.mat_ids, np.int32)
+            mid = check(L.xb_scene_add_mesh(s.h, len(pos), _p(pos), _p(nrm), len(idx), _p(idx), _p(mat),
+                                            int(mesh.default_mat)))
+            if mesh.transform is not None:
+                t, sc, r = mesh.transform
+                check(L.xb_scene_transform_mesh(s.h, mid, _p(np.asarray(t, np.float32)), float(sc),
+                                                _p(np.asarray(r, np.float32))))
+        for p in desc.prims:
+            arr = np.ascontiguousarray(p)
+            check(L.xb_scene_add_prim(s.h, _p(arr)))
+        for (mesh_id, tri, e, area) in desc.lights:
+            check(L.xb_scene_add_light(s.h, mesh_id, tri, _p(np.asarray(e, np.float32)), float(area)))
+        for (d, c, inten) in desc.suns:
+            check(L.xb_scene_add_sun(s.h, _p(np.asarray(d, np.float32)), _p(np.asarray(c, np.float32)),
+                                     float(inten)))
+        sky = np.ascontiguousarray(desc.sky, np.float32)
+        check(L.xb_scene_set_sky(s.h, _p(sky)))
+        for (geom, t, sc, r, iid) in desc.instances:
+            check(L.xb_scene_add_instance(s.h, int(geom), _p(np.asarray(t, np.float32)), float(sc),
+                                          _p(np.asarray(r, np.float32)), int(iid)))
+        check(L.xb_scene_build(s.h))
+        return s
+
+    @classmethod
+    def load(cls, path: str) -> "HostScene":
+        """The .xenon loader (src/scene/scene_file.cpp:49-231), builds the BVHs too."""
+        s = cls.__new__(cls)
+        h = ctypes.c_void_p()
+        cfg = abi.SceneConfig()
+        cam = abi.CameraDesc()
+        check(lib().xb_scene_load(str(path).encode(), ctypes.byref(h), ctypes.byref(cfg), ctypes.byref(cam)))
+        s.h = h
+        s.config = cfg
+        s.camera_desc = cam
+        return s
+
+    def view(self) -> abi.SceneView:
+        v = abi.SceneView()
+        check(lib().xb_scene_get_view(self.h, ctypes.byref(v)))
+        return v
+
+
+class Renderer:
+    """Mirrors xn::CudaRenderer (src/cuda/cuda_renderer.cuh:14-55) over the C ABI."""
+
+    def __init__(self, width: int, height: int, max_bounces: int = 8, min_bounces: int = 3,
+                 device: int = 0, fp64: bool = False, wave_paths: int = 0, flags: int = 0):
+        cfg = abi.Config(width, height, max_bounces, min_bounces, device,
+                         (abi.XB_FLAG_FP64_ACCUM if fp64 else 0) | flags, wave_paths, 0)
+        h = ctypes.c_void_p()
+        check(lib().xb_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.width, self.height = width, height
+        self.fp64 = fp64
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().xb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc):
+        return check(rc, self.h)
+
+    def upload_scene(self, scene) -> None:
+        """Accepts a HostScene or an abi.SceneView (e.g. exported from another builder)."""
+        v = scene.view() if isinstance(scene, HostScene) else scene
+        self._check(lib().xb_upload_scene(self.h, ctypes.byref(v)))
+
+    def set_bounces(self, min_bounces: int, max_bounces: int) -> None:
+        self._check(lib().xb_set_bounces(self.h, min_bounces, max_bounces))
+
+    def render_frame(self, cam: abi.Camera, spp: int = 1) -> None:
+        self._check(lib().xb_render(self.h, ctypes.byref(cam), int(spp)))
+
+    def render_range(self, cam: abi.Camera, spp_first: int, spp_count: int) -> None:
+        self._check(lib().xb_render_range(self.h, ctypes.byref(cam), int(spp_first), int(spp_count)))
+
+    def resolve(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.height, self.width, 3), np.float32)
+        self._check(lib().xb_resolve(self.h, _p(out)))
+        return out
+
+    def resolve_fp64(self):
+        s = np.empty((self.height, self.width, 3), np.float64)
+        m2 = np.empty_like(s)
+        self._check(lib().xb_resolve_fp64(self.h, _p(s), _p(m2)))
+        return s, m2
+
+    @property
+    def spp(self) -> int:
+        return int(lib().xb_get_spp(self.h))
+
+    def reset(self) -> None:
+        self._check(lib().xb_reset(self.h))
+
+    def stats(self) -> abi.RenderStats:
+        st = abi.RenderStats()
+        self._check(lib().xb_get_render_stats(self.h, ctypes.byref(st)))
+        return st
+
+    def reset_stats(self) -> None:
+        self._check(lib().xb_reset_render_stats(self.h))
+
+    def set_profiling(self, flags: int) -> None:
+        self._check(lib().xb_set_profiling(self.h, int(flags)))
+
+    def profile(self) -> abi.Profile:
+        p = abi.Profile()
+        self._check(lib().xb_get_profile(self.h, ctypes.byref(p)))
+        return p
+
+    def reset_profile(self) -> None:
+        self._check(lib().xb_reset_profile(self.h))
+
+    def trace_rays(self, rays: np.ndarray, mode: int = abi.XB_TRACE_CLOSEST) -> np.ndarray:
+        rays = np.ascontiguousarray(rays)
+        assert rays.dtype == abi.RAY_DTYPE
+        hits = np.empty(len(rays), abi.HIT_DTYPE)
+        self._check(lib().xb_trace_rays(self.h, _p(rays), len(rays), _p(hits), int(mode)))
+        return hits
+
+    def trace_rays_device(self, rays_ptr: int, n: int, hits_ptr: int, mode: int = 0, stream: int = 0) -> None:
+        self._check(lib().xb_trace_rays_device(self.h, ctypes.c_void_p(rays_ptr), int(n),
+                                               ctypes.c_void_p(hits_ptr), int(mode),
+                                               ctypes.c_void_p(stream) if stream else None))
+
+
+def bsdf_eval(mat: np.ndarray, wo: np.ndarray, wi: np.ndarray):
+    """GPU eval/pdf for NEE (bsdf_eval_for_nee / bsdf_pdf_for_nee)."""
+    wo = np.ascontiguousarray(wo, np.float32)
+    wi = np.ascontiguousarray(wi, np.float32)
+    n = len(wo)
+    f = np.empty((n, 3), np.float32)
+    pdf = np.empty(n, np.float32)
+    m = np.ascontiguousarray(mat, np.float32)
+    check(lib().xb_bsdf_eval(_p(m), n, _p(wo), _p(wi), _p(f), _p(pdf)))
+    return f, pdf
+
+
+def bsdf_sample(mat: np.ndarray, wo: np.ndarray, states):
+    wo = np.ascontiguousarray(wo, np.float32)
+    n = len(wo)
+    st = np.array(states, dtype=np.uint64, copy=True)
+    wi = np.empty((n, 3), np.float32)
+    f = np.empty((n, 3), np.float32)
+    pdf = np.empty(n, np.float32)
+    flags = np.empty(n, np.int32)
+    m = np.ascontiguousarray(mat, np.float32)
+    check(lib().xb_bsdf_sample(_p(m), n, _p(wo), _p(st), _p(wi), _p(f), _p(pdf), _p(flags)))
+    return wi, f, pdf, flags, st

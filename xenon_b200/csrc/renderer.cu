@@ -1,0 +1,1289 @@
+// renderer.cu — the B200 wavefront path tracer behind the C ABI (xb_create ... xb_destroy).
+//
+// One renderer owns one device, one stream and the device copy of one scene. A call to
+// xb_render adds samples in waves: a wave is `spp_per_wave` consecutive sample indices of
+// every pixel (wave_paths paths). Each wave runs, on the renderer's stream, with no host sync:
+//
+//   raygen                  camera rays into ray queue 0                (cpu_tiled.cpp:20-32)
+//   for depth in [0, max_bounces):
+//     extend(depth)         closest hit of queue (depth&1)              (scene.h:124, tlas.cpp:172)
+//     shade(depth)          miss→sky, emitter hit + MIS, area NEE and sun NEE shadow-ray
+//                           generation, Russian roulette, BSDF sampling into queue
+//                           ((depth+1)&1)                               (cpu_tiled.cpp:34-217)
+//     shadow(depth, area)   any hit; unoccluded → radiance += contribution (cpu_tiled.cpp:133-135)
+//     shadow(depth, sun)    same for the directional-light ray       (cpu_tiled.cpp:175-184)
+//   accumulate              per pixel, the wave's samples in sample order (cpu_tiled.cpp:218)
+//
+// Queue sizes live in device counters; every stage kernel is a persistent grid that reads
+// its item count on the device, so the host never waits inside a wave. Queue appends are
+// warp-aggregated (one atomic per warp). Per-path radiance is added in the CPU order:
+// emission / sky of bounce d, then area NEE of d, then sun NEE of d, then bounce d+1.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/xenon_b200.h"
+#include "capi_common.h"
+#include "dev_bsdf.cuh"
+#include "dev_math.cuh"
+#include "dev_scene.cuh"
+#include "scene_host.h"
+#include "trace_persistent.cuh"
+
+using namespace xbd;
+
+namespace {
+
+inline float u32_bits_to_f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+inline float i32_bits_to_f(int32_t i) { float f; std::memcpy(&f, &i, 4); return f; }
+
+constexpr int kMaxDepth = 64;
+constexpr int kCntStride = 8;        // counters per depth
+enum {
+  CNT_RAYS = 0,                      // rays in queue for this depth
+  CNT_SH_AREA = 1,                   // area-light shadow items produced at this depth
+  CNT_SH_SUN = 2,                    // sun shadow items produced at this depth
+  CNT_FETCH_EXT = 3,                 // work-fetch cursors
+  CNT_FETCH_SH_AREA = 4,
+  CNT_FETCH_SH_SUN = 5,
+};
+enum { STAT_RAYS = 0, STAT_SHADOW = 1, STAT_PATHS = 2, STAT_OVERFLOW = 3, STAT_NONFINITE = 4,
+       STAT_EXT_WORK = 8,    // 4 counters: blas nodes, tris, tlas nodes, instances (closest hit)
+       STAT_SH_WORK = 12,    // same for shadow rays
+       STAT_COUNT = 16 };
+
+__device__ __forceinline__ void flush_counters(unsigned long long* dst, const TraversalCounters& c) {
+  atomicAdd(dst + 0, (unsigned long long)c.nodes);
+  atomicAdd(dst + 1, (unsigned long long)c.tris);
+  atomicAdd(dst + 2, (unsigned long long)c.tlas);
+  atomicAdd(dst + 3, (unsigned long long)c.inst);
+}
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return set_err(r, XB_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+struct WaveBuffers {
+  int64_t capacity = 0;
+  float4* ray_o[2] = {nullptr, nullptr};
+  float4* ray_d[2] = {nullptr, nullptr};
+  float4* tp[2] = {nullptr, nullptr};     // throughput xyz, w = prev pdf (< 0: previous delta)
+  uint64_t* rng[2] = {nullptr, nullptr};
+  int32_t* path[2] = {nullptr, nullptr};
+  float4* hit = nullptr;                  // t, u, v, bits(prim)
+  int32_t* hit_inst = nullptr;
+  float4* sh_o[2] = {nullptr, nullptr};   // [0] area, [1] sun: origin xyz, w = tmax
+  float4* sh_d[2] = {nullptr, nullptr};   // dir xyz, w = bits(path)
+  float4* sh_c[2] = {nullptr, nullptr};   // contribution xyz
+  float4* L = nullptr;                    // per path radiance
+  int32_t* cnt = nullptr;                 // [kMaxDepth + 1][kCntStride]
+};
+
+}  // namespace
+
+struct xb_renderer {
+  xb_config cfg{};
+  int min_bounces = 3, max_bounces = 8;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  std::string err;
+  // scene
+  std::vector<void*> scene_mem;
+  DevScene scene{};
+  bool has_scene = false;
+  // framebuffer
+  float4* accum = nullptr;                // FP32 per-pixel sum
+  double* sum64 = nullptr;                // FP64 sum (flag)
+  double* m2_64 = nullptr;                // Welford M2 (flag)
+  double* mean64 = nullptr;
+  int spp = 0;
+  float* resolve_buf = nullptr;
+  WaveBuffers wb;
+  int spp_per_wave = 1;
+  unsigned long long* stats = nullptr;    // device totals
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  int grid_ext = 0, grid_shade = 0, grid_shadow = 0, block = 128;
+  int grid_pext = 0, grid_pshadow = 0;
+  bool thread_per_ray = false;   // XB_FLAG_THREAD_PER_RAY: one ray per thread traversal kernels
+  int refill = 8;                // persistent traversal: refill a warp when this many lanes idle
+  // profiling
+  int prof_flags = 0;
+  std::vector<cudaEvent_t> ev_pool;          // event pairs, reused each call
+  std::vector<int> ev_stage;                 // stage of each recorded pair
+  size_t ev_used = 0;
+  double stage_ms[5] = {0, 0, 0, 0, 0};      // raygen, extend, shade, shadow, accumulate
+  int64_t stage_launches[5] = {0, 0, 0, 0, 0};
+  // generic scratch for trace/bsdf helpers
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+};
+
+namespace {
+
+int set_err(xb_renderer* r, int code, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
+int set_err(xb_renderer* r, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (r) r->err = buf;
+  xb::g_last_error = buf;
+  return code;
+}
+
+// ── warp-aggregated queue append ──────────────────────────────────────────────
+// All 32 lanes must call it (convergent); returns the slot for lanes with pred, or -1.
+__device__ __forceinline__ int warp_append(int32_t* counter, bool pred, int capacity,
+                                           unsigned long long* overflow) {
+  const unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (m == 0) return -1;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (!pred) return -1;
+  const int idx = base + __popc(m & ((1u << lane) - 1u));
+  if (idx >= capacity) {
+    atomicAdd(overflow, 1ull);
+    return -1;
+  }
+  return idx;
+}
+
+// ── raygen (cpu_tiled.cpp:20-32) ────────────────────────────────────────────────
+struct CamDev {
+  V3 eye, ll, hor, ver;
+};
+
+__global__ void raygen_kernel(CamDev cam, int W, int H, int spp_first, int64_t paths,
+                              float4* ray_o, float4* ray_d, float4* tp, uint64_t* rng,
+                              int32_t* path, float4* L, int32_t* cnt) {
+  const int64_t npix = (int64_t)W * H;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < paths;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pixel = p % npix;
+    const int64_t s = spp_first + p / npix;
+    const int x = (int)(pixel % W), y = (int)(pixel / W);
+    Pcg g{pcg_seed_state((uint64_t)pixel + (uint64_t)s * 0xdeadbeefULL)};
+    const float u = (float)x + g.next_float();
+    const float v = (float)y + g.next_float();
+    const float su = u / (float)W, sv = v / (float)H;
+    V3 d = normalize(cam.ll + su * cam.hor + sv * cam.ver - cam.eye);
+    ray_o[p] = make_float4(cam.eye.x, cam.eye.y, cam.eye.z, kRayEps);
+    ray_d[p] = make_float4(d.x, d.y, d.z, kInf);
+    tp[p] = make_float4(1.f, 1.f, 1.f, -1.f);
+    rng[p] = g.state;
+    path[p] = (int32_t)p;
+    L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt[CNT_RAYS] = (int32_t)paths;
+}
+
+// ── extend: closest hit of the bounce's ray queue ─────────────────────────────
+template <bool kCount>
+__global__ void __launch_bounds__(128) extend_kernel(DevScene sc, const float4* __restrict__ ray_o,
+                                                     const float4* __restrict__ ray_d,
+                                                     float4* hit, int32_t* hit_inst, int32_t* cnt,
+                                                     unsigned long long* stats) {
+  __shared__ int s_base[4];
+  const int n = cnt[CNT_RAYS];
+  uint32_t tstack[kStackSize];
+  uint32_t bstack[kStackSize];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool overflow = false;
+  TraversalCounters tc{0, 0, 0, 0};
+  for (;;) {
+    if (lane == 0) s_base[warp] = atomicAdd(cnt + CNT_FETCH_EXT, 32);
+    __syncwarp();
+    const int base = s_base[warp];
+    __syncwarp();
+    if (base >= n) break;
+    const int i = base + lane;
+    if (i < n) {
+      const float4 o = ray_o[i], d = ray_d[i];
+      Ray r{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, d.w};
+      HitState h;
+      scene_closest<kCount>(sc, r, h, tstack, bstack, tc, overflow);
+      hit[i] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+      hit_inst[i] = h.inst;
+    }
+  }
+  if (overflow) atomicAdd(stats + STAT_OVERFLOW, 1ull);
+  if (kCount) flush_counters(stats + STAT_EXT_WORK, tc);
+}
+
+// ── shadow: any hit; unoccluded items add their contribution ──────────────────
+template <bool kCount>
+__global__ void __launch_bounds__(128) shadow_kernel(DevScene sc, const float4* __restrict__ so,
+                                                     const float4* __restrict__ sd,
+                                                     const float4* __restrict__ scn, float4* L,
+                                                     const int32_t* count, int32_t* fetch,
+                                                     unsigned long long* stats) {
+  __shared__ int s_base[4];
+  const int n = *count;
+  uint32_t tstack[kStackSize];
+  uint32_t bstack[kStackSize];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool overflow = false;
+  TraversalCounters tc{0, 0, 0, 0};
+  for (;;) {
+    if (lane == 0) s_base[warp] = atomicAdd(fetch, 32);
+    __syncwarp();
+    const int base = s_base[warp];
+    __syncwarp();
+    if (base >= n) break;
+    const int i = base + lane;
+    if (i < n) {
+      const float4 o = so[i], d = sd[i];
+      Ray r{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kShadowEps, o.w};
+      if (!scene_any<kCount>(sc, r, tstack, bstack, tc, overflow)) {
+        const float4 c = scn[i];
+        const int p = __float_as_int(d.w);
+        float4 l = L[p];
+        l.x = l.x + c.x; l.y = l.y + c.y; l.z = l.z + c.z;
+        L[p] = l;
+      }
+    }
+  }
+  if (overflow) atomicAdd(stats + STAT_OVERFLOW, 1ull);
+  if (kCount) flush_counters(stats + STAT_SH_WORK, tc);
+}
+
+// ── persistent-warp variants (trace_persistent.cuh) ────────────────────────────
+template <bool kCount>
+__global__ void __launch_bounds__(128) extend_persistent_kernel(DevScene sc, TraceQueue q, int refill) {
+  trace_queue_persistent<false, kCount>(sc, q, refill);
+}
+template <bool kCount>
+__global__ void __launch_bounds__(128) shadow_persistent_kernel(DevScene sc, TraceQueue q, int refill) {
+  trace_queue_persistent<true, kCount>(sc, q, refill);
+}
+
+// ── shade (cpu_tiled.cpp:34-217 for one bounce) ───────────────────────────────
+struct ShadeArgs {
+  DevScene sc;
+  const float4* ray_o; const float4* ray_d; const float4* tp; const uint64_t* rng;
+  const int32_t* path;
+  float4* nray_o; float4* nray_d; float4* ntp; uint64_t* nrng; int32_t* npath;
+  const float4* hit; const int32_t* hit_inst;
+  float4* sh_o[2]; float4* sh_d[2]; float4* sh_c[2];
+  float4* L;
+  int32_t* cnt;         // this depth's counters
+  int32_t* cnt_next;    // next depth's counters
+  int depth, min_bounces, max_bounces;
+  int capacity;
+  unsigned long long* stats;
+};
+
+__device__ __forceinline__ V3 sky_eval(const DevScene& sc, V3 d) {
+  // Environment::evaluate (src/scene/environment.h:24-36)
+  V3 hz = v3(sc.sky_horizon[0], sc.sky_horizon[1], sc.sky_horizon[2]);
+  if (d.y < 0.f) {
+    float t = smin(-d.y, 1.f);
+    return sc.sky_intensity * lerp(hz, v3(sc.sky_ground[0], sc.sky_ground[1], sc.sky_ground[2]), t);
+  }
+  float t = powf(d.y, sc.sky_inv_sharpness);
+  return sc.sky_intensity * lerp(hz, v3(sc.sky_zenith[0], sc.sky_zenith[1], sc.sky_zenith[2]), t);
+}
+
+__device__ __forceinline__ void add_L(float4* L, int p, V3 c) {
+  float4 l = L[p];
+  l.x = l.x + c.x; l.y = l.y + c.y; l.z = l.z + c.z;
+  L[p] = l;
+}
+
+__global__ void __launch_bounds__(128) shade_kernel(ShadeArgs a) {
+  const int n = a.cnt[CNT_RAYS];
+  const DevScene& sc = a.sc;
+  const bool last = (a.depth + 1 >= a.max_bounces);
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int slot = base + threadIdx.x;
+    bool emit_next = false, emit_area = false, emit_sun = false;
+    float4 n_o, n_d, n_tp;
+    uint64_t n_rng = 0;
+    int32_t pid = 0;
+    float4 a_o, a_d, a_c, s_o, s_d, s_c;
+    if (slot < n) {
+      const float4 ro = a.ray_o[slot], rd = a.ray_d[slot], tpv = a.tp[slot];
+      pid = a.path[slot];
+      Pcg rng{a.rng[slot]};
+      const Ray ray{v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), ro.w, rd.w};
+      V3 tp = v3(tpv.x, tpv.y, tpv.z);
+      const float prev_pdf = tpv.w;             // < 0: previous bounce was delta
+      const float4 hv = a.hit[slot];
+      const int hinst = a.hit_inst[slot];
+      do {
+        if (hinst < 0) {
+          if (sc.sky_intensity > 0.f) add_L(a.L, pid, tp * sky_eval(sc, ray.d));
+          break;
+        }
+        HitState h{hv.x, hv.y, hv.z, __float_as_int(hv.w), hinst};
+        FullHit fh;
+        complete_hit(sc, ray, h, fh);
+        const DevMaterial& mat = sc.mats[fh.mat_id];
+        // ── emitter hit + MIS (cpu_tiled.cpp:62-86) ──
+        bool hit_light = false;
+        for (int li = 0; li < sc.num_lights; ++li) {
+          const DevLight& lt = sc.lights[li];
+          if (__float_as_int(lt.p2.w) == fh.prim_id && __float_as_int(lt.p1.w) == fh.instance_id) {
+            float mis = 1.0f;
+            const float cos_l = smax(0.0f, dot(fh.geo_normal, -ray.d));
+            if (cos_l > 1e-6f) {
+              if (a.depth > 0 && !(prev_pdf < 0.f)) {
+                const float pdf_area = (1.0f / lt.p0.w) * (1.0f / (float)sc.num_lights);
+                const float dsq = h.t * h.t;
+                const float pdf_sa = (pdf_area * dsq) / cos_l;
+                mis = mis_power2(prev_pdf, pdf_sa);
+              }
+              add_L(a.L, pid, tp * v3(lt.emission.x, lt.emission.y, lt.emission.z) * mis);
+            }
+            hit_light = true;
+            break;
+          }
+        }
+        if (hit_light) break;
+        const bool is_delta = (mat.flags & kMatDelta) != 0;
+        // ── area-light NEE (cpu_tiled.cpp:89-139) ──
+        if (sc.num_lights > 0 && !is_delta) {
+          const float upick = rng.next_float();
+          int li = (int)(upick * (float)sc.num_lights);
+          li = li < 0 ? 0 : (li > sc.num_lights - 1 ? sc.num_lights - 1 : li);
+          const float pick_pdf = 1.f / (float)sc.num_lights;
+          const DevLight& lt = sc.lights[li];
+          const float u1 = rng.next_float();
+          const float u2 = rng.next_float();
+          const float su1 = sqrtf(u1);
+          const float b0 = 1.0f - su1;
+          const float b1 = u2 * su1;
+          const float b2 = 1.0f - b0 - b1;
+          const V3 lp = ld3(lt.p0) * b0 + ld3(lt.p1) * b1 + ld3(lt.p2) * b2;
+          const V3 ln = ld3(lt.n);
+          const V3 sdir = lp - fh.pos;
+          const float dsq = length_sq(sdir);
+          const float dist = sqrtf(dsq);
+          if (dist > 1e-6f) {
+            const V3 wi = sdir / dist;
+            const float cos_l = smax(0.0f, dot(ln, -wi));
+            const Onb onb(fh.geo_normal);
+            const V3 wo_l = onb.to_local(-ray.d);
+            const V3 wi_l = onb.to_local(wi);
+            if (cos_l > 1e-6f && wi_l.z > 1e-6f) {
+              const V3 f = bsdf_eval(wo_l, wi_l, mat);
+              const float bp = bsdf_pdf(wo_l, wi_l, mat);
+              const float lpdf = ((1.0f / lt.p0.w) * pick_pdf) * (dsq / cos_l);
+              const float mis = mis_power2(lpdf, bp);
+              const float cs = wi_l.z;
+              if (mis > 0.0f && lpdf > 1e-12f) {
+                const V3 org = offset_origin(fh.pos, fh.geo_normal, wi, kShadowEps);
+                const V3 c = tp * f * cs * (v3(lt.emission.x, lt.emission.y, lt.emission.z) / lpdf) * mis;
+                a_o = make_float4(org.x, org.y, org.z, dist - kShadowEps);
+                a_d = make_float4(wi.x, wi.y, wi.z, __int_as_float(pid));
+                a_c = make_float4(c.x, c.y, c.z, 0.f);
+                emit_area = true;
+              }
+            }
+          }
+        }
+        // ── directional-light NEE (cpu_tiled.cpp:148-187) ──
+        if (sc.num_suns > 0 && !is_delta) {
+          const float upick = rng.next_float();
+          int di = (int)(upick * (float)sc.num_suns);
+          di = di < 0 ? 0 : (di > sc.num_suns - 1 ? sc.num_suns - 1 : di);
+          const float dpick = 1.f / (float)sc.num_suns;
+          if (dpick > 0.f) {
+            const DevSun& sun = sc.suns[di];
+            const V3 sdir = v3(sun.dir[0], sun.dir[1], sun.dir[2]);
+            const Onb onb(fh.geo_normal);
+            const V3 wo_l = onb.to_local(-ray.d);
+            const V3 wi_l = onb.to_local(sdir);
+            if (wi_l.z > 1e-6f) {
+              const V3 f = bsdf_eval(wo_l, wi_l, mat);
+              const float bp = bsdf_pdf(wo_l, wi_l, mat);
+              const float cs = wi_l.z;
+              const float lpdf = 1e8f * dpick;
+              const float mis = mis_power2(lpdf, bp);
+              const V3 org = offset_origin(fh.pos, fh.geo_normal, sdir, kShadowEps);
+              const V3 em = v3(sun.emission[0], sun.emission[1], sun.emission[2]);
+              const V3 c = tp * f * cs * (em / lpdf) * mis;
+              s_o = make_float4(org.x, org.y, org.z, kInf);
+              s_d = make_float4(sdir.x, sdir.y, sdir.z, __int_as_float(pid));
+              s_c = make_float4(c.x, c.y, c.z, 0.f);
+              emit_sun = true;
+            }
+          }
+        }
+        if (last) break;   // the reference samples once more, but nothing of it is ever used
+        // ── Russian roulette (cpu_tiled.cpp:190-194) ──
+        if (a.depth >= a.min_bounces) {
+          const float p = smax(0.05f, max_component(tp));
+          if (rng.next_float() > p) break;
+          tp = tp / p;
+        }
+        // ── BSDF sampling and the next ray (cpu_tiled.cpp:197-216) ──
+        const Onb onb(fh.normal);
+        const V3 wo_l = onb.to_local(-ray.d);
+        BsdfSample s;
+        if (!bsdf_sample(wo_l, mat, rng, s)) break;
+        if (s.delta) {
+          tp = tp * s.f;
+        } else {
+          const float ci = fabsf(s.wi.z);
+          if (s.pdf < 1e-8f || ci < 1e-8f) break;
+          tp = tp * (s.f * ci / s.pdf);
+        }
+        const V3 wiw = onb.to_world(s.wi);
+        const V3 org = offset_origin(fh.pos, fh.geo_normal, wiw, kRayEps);
+        n_o = make_float4(org.x, org.y, org.z, kRayEps);
+        n_d = make_float4(wiw.x, wiw.y, wiw.z, kInf);
+        n_tp = make_float4(tp.x, tp.y, tp.z, s.delta ? -1.f : s.pdf);
+        n_rng = rng.state;
+        emit_next = true;
+      } while (false);
+    }
+    int idx = warp_append(a.cnt_next + CNT_RAYS, emit_next, a.capacity, a.stats + STAT_OVERFLOW);
+    if (idx >= 0) {
+      a.nray_o[idx] = n_o; a.nray_d[idx] = n_d; a.ntp[idx] = n_tp; a.nrng[idx] = n_rng;
+      a.npath[idx] = pid;
+    }
+    idx = warp_append(a.cnt + CNT_SH_AREA, emit_area, a.capacity, a.stats + STAT_OVERFLOW);
+    if (idx >= 0) { a.sh_o[0][idx] = a_o; a.sh_d[0][idx] = a_d; a.sh_c[0][idx] = a_c; }
+    idx = warp_append(a.cnt + CNT_SH_SUN, emit_sun, a.capacity, a.stats + STAT_OVERFLOW);
+    if (idx >= 0) { a.sh_o[1][idx] = s_o; a.sh_d[1][idx] = s_d; a.sh_c[1][idx] = s_c; }
+  }
+}
+
+// ── accumulate the wave into the framebuffer, in sample order ──────────────────
+__global__ void accumulate_kernel(const float4* L, int64_t npix, int spw, int spp_before,
+                                  float4* accum, double* sum64, double* m2_64, double* mean64,
+                                  const int32_t* cnt, int max_depth, int64_t paths,
+                                  unsigned long long* stats) {
+  for (int64_t px = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; px < npix;
+       px += (int64_t)gridDim.x * blockDim.x) {
+    float4 acc = accum[px];
+    double s0 = 0, s1 = 0, s2 = 0, m0 = 0, m1 = 0, m2 = 0, mu0 = 0, mu1 = 0, mu2 = 0;
+    if (sum64) {
+      s0 = sum64[3 * px]; s1 = sum64[3 * px + 1]; s2 = sum64[3 * px + 2];
+      m0 = m2_64[3 * px]; m1 = m2_64[3 * px + 1]; m2 = m2_64[3 * px + 2];
+      mu0 = mean64[3 * px]; mu1 = mean64[3 * px + 1]; mu2 = mean64[3 * px + 2];
+    }
+    for (int k = 0; k < spw; ++k) {
+      const float4 l = L[(int64_t)k * npix + px];
+      if (!(isfinite(l.x) && isfinite(l.y) && isfinite(l.z))) {
+        atomicAdd(stats + STAT_NONFINITE, 1ull);
+        continue;
+      }
+      acc.x = acc.x + l.x; acc.y = acc.y + l.y; acc.z = acc.z + l.z;
+      if (sum64) {
+        // Welford update over the sample sequence
+        const double nn = (double)(spp_before + k + 1);
+        double d;
+        s0 += l.x; d = l.x - mu0; mu0 += d / nn; m0 += d * (l.x - mu0);
+        s1 += l.y; d = l.y - mu1; mu1 += d / nn; m1 += d * (l.y - mu1);
+        s2 += l.z; d = l.z - mu2; mu2 += d / nn; m2 += d * (l.z - mu2);
+      }
+    }
+    accum[px] = acc;
+    if (sum64) {
+      sum64[3 * px] = s0; sum64[3 * px + 1] = s1; sum64[3 * px + 2] = s2;
+      m2_64[3 * px] = m0; m2_64[3 * px + 1] = m1; m2_64[3 * px + 2] = m2;
+      mean64[3 * px] = mu0; mean64[3 * px + 1] = mu1; mean64[3 * px + 2] = mu2;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long rays = 0, sh = 0;
+    for (int d = 0; d < max_depth; ++d) {
+      rays += (unsigned long long)cnt[d * kCntStride + CNT_RAYS];
+      sh += (unsigned long long)cnt[d * kCntStride + CNT_SH_AREA] +
+            (unsigned long long)cnt[d * kCntStride + CNT_SH_SUN];
+    }
+    atomicAdd(stats + STAT_RAYS, rays);
+    atomicAdd(stats + STAT_SHADOW, sh);
+    atomicAdd(stats + STAT_PATHS, (unsigned long long)paths);
+  }
+}
+
+// ── resolve: mean, top-down rows (cpu_tiled.cpp:224-236) ───────────────────────
+__global__ void resolve_kernel(const float4* accum, int W, int H, float inv_spp, float* out) {
+  const int64_t npix = (int64_t)W * H;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npix;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % W), y = (int)(i / W);
+    const float4 a = accum[i];
+    const int64_t d = ((int64_t)(H - 1 - y) * W + x) * 3;
+    out[d] = a.x * inv_spp;
+    out[d + 1] = a.y * inv_spp;
+    out[d + 2] = a.z * inv_spp;
+  }
+}
+
+// ── ray queries (xb_trace_rays) ─────────────────────────────────────────────────
+__global__ void __launch_bounds__(128) trace_full_kernel(DevScene sc, const xb_ray* rays,
+                                                         int64_t n, xb_hit* hits, int mode,
+                                                         unsigned long long* stats) {
+  uint32_t tstack[kStackSize];
+  uint32_t bstack[kStackSize];
+  bool overflow = false;
+  TraversalCounters tc{0, 0, 0, 0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const xb_ray rr = rays[i];
+    Ray r{v3(rr.org[0], rr.org[1], rr.org[2]), v3(rr.dir[0], rr.dir[1], rr.dir[2]), rr.tmin, rr.tmax};
+    xb_hit out;
+    memset(&out, 0, sizeof(out));
+    out.t = kInf; out.prim_id = -1; out.instance_id = -1; out.mat_id = -1;
+    if (mode == XB_TRACE_CLOSEST) {
+      HitState h;
+      if (scene_closest<true>(sc, r, h, tstack, bstack, tc, overflow)) {
+        FullHit f;
+        complete_hit(sc, r, h, f);
+        out.t = h.t; out.u = f.u; out.v = f.v;
+        out.prim_id = f.prim_id; out.instance_id = f.instance_id; out.mat_id = f.mat_id;
+        out.front_face = f.front_face ? 1 : 0;
+        out.pos[0] = f.pos.x; out.pos[1] = f.pos.y; out.pos[2] = f.pos.z;
+        out.normal[0] = f.normal.x; out.normal[1] = f.normal.y; out.normal[2] = f.normal.z;
+        out.geo_normal[0] = f.geo_normal.x; out.geo_normal[1] = f.geo_normal.y;
+        out.geo_normal[2] = f.geo_normal.z;
+      }
+    } else {
+      if (scene_any<true>(sc, r, tstack, bstack, tc, overflow)) out.t = 0.f;
+    }
+    hits[i] = out;
+  }
+  if (overflow) atomicAdd(stats + STAT_OVERFLOW, 1ull);
+  flush_counters(stats + (mode == XB_TRACE_CLOSEST ? STAT_EXT_WORK : STAT_SH_WORK), tc);
+}
+
+// ── BSDF queries (xb_bsdf_eval / xb_bsdf_sample) ───────────────────────────────
+__global__ void bsdf_eval_kernel(DevMaterial m, int64_t n, const float* wo, const float* wi,
+                                 float* f, float* pdf) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    V3 o = v3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
+    V3 w = v3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+    V3 fv = bsdf_eval(o, w, m);
+    f[3 * i] = fv.x; f[3 * i + 1] = fv.y; f[3 * i + 2] = fv.z;
+    pdf[i] = bsdf_pdf(o, w, m);
+  }
+}
+
+__global__ void bsdf_sample_kernel(DevMaterial m, int64_t n, const float* wo, uint64_t* st,
+                                   float* wi, float* f, float* pdf, int32_t* flags) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Pcg g{st[i]};
+    V3 o = v3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
+    BsdfSample s;
+    bool ok = bsdf_sample(o, m, g, s);
+    st[i] = g.state;
+    wi[3 * i] = s.wi.x; wi[3 * i + 1] = s.wi.y; wi[3 * i + 2] = s.wi.z;
+    f[3 * i] = s.f.x; f[3 * i + 1] = s.f.y; f[3 * i + 2] = s.f.z;
+    pdf[i] = s.pdf;
+    flags[i] = (ok ? 1 : 0) | (s.delta ? 2 : 0);
+  }
+}
+
+DevMaterial to_dev_material(const xb_material& m) {
+  xb_material_derived d = xb::prepare_material(m);
+  DevMaterial o{};
+  for (int i = 0; i < 3; ++i) {
+    o.base[i] = m.base_color[i];
+    o.f0[i] = d.f0[i];
+    o.ss_color[i] = m.subsurface_color[i];
+  }
+  o.metallic = m.metallic;
+  o.ior = m.ior;
+  o.alpha = d.alpha; o.alpha_x = d.alpha_x; o.alpha_y = d.alpha_y;
+  o.subsurface = m.subsurface;
+  o.flags = d.flags;
+  return o;
+}
+
+void free_scene(xb_renderer* r) {
+  for (void* p : r->scene_mem) cudaFree(p);
+  r->scene_mem.clear();
+  r->has_scene = false;
+  std::memset(&r->scene, 0, sizeof(r->scene));
+}
+
+void free_wave(xb_renderer* r) {
+  WaveBuffers& w = r->wb;
+  void* ptrs[] = {w.ray_o[0], w.ray_o[1], w.ray_d[0], w.ray_d[1], w.tp[0], w.tp[1], w.rng[0],
+                  w.rng[1], w.path[0], w.path[1], w.hit, w.hit_inst, w.sh_o[0], w.sh_o[1],
+                  w.sh_d[0], w.sh_d[1], w.sh_c[0], w.sh_c[1], w.L, w.cnt};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  w = WaveBuffers();
+}
+
+template <class T>
+int dev_upload(xb_renderer* r, const std::vector<T>& v, const T** out) {
+  *out = nullptr;
+  if (v.empty()) return XB_OK;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, v.size() * sizeof(T));
+  if (e != cudaSuccess) return set_err(r, XB_E_OOM, "cudaMalloc(%zu) failed: %s", v.size() * sizeof(T), cudaGetErrorString(e));
+  r->scene_mem.push_back(p);
+  e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return set_err(r, XB_E_CUDA, "cudaMemcpy failed: %s", cudaGetErrorString(e));
+  *out = static_cast<const T*>(p);
+  return XB_OK;
+}
+
+float4 node_lo(const xb_bvh_node& n) { return make_float4(n.mn[0], n.mn[1], n.mn[2], n.mx[0]); }
+float4 node_hi(const xb_bvh_node& n, uint32_t child) {
+  return make_float4(n.mx[1], n.mx[2], u32_bits_to_f(child), u32_bits_to_f(n.count));
+}
+
+int alloc_wave(xb_renderer* r, int64_t cap) {
+  free_wave(r);
+  WaveBuffers& w = r->wb;
+  w.capacity = cap;
+  auto A = [&](auto** p, size_t bytes) -> bool {
+    return cudaMalloc((void**)p, bytes) == cudaSuccess;
+  };
+  bool ok = true;
+  for (int q = 0; q < 2; ++q) {
+    ok &= A(&w.ray_o[q], cap * sizeof(float4));
+    ok &= A(&w.ray_d[q], cap * sizeof(float4));
+    ok &= A(&w.tp[q], cap * sizeof(float4));
+    ok &= A(&w.rng[q], cap * sizeof(uint64_t));
+    ok &= A(&w.path[q], cap * sizeof(int32_t));
+    ok &= A(&w.sh_o[q], cap * sizeof(float4));
+    ok &= A(&w.sh_d[q], cap * sizeof(float4));
+    ok &= A(&w.sh_c[q], cap * sizeof(float4));
+  }
+  ok &= A(&w.hit, cap * sizeof(float4));
+  ok &= A(&w.hit_inst, cap * sizeof(int32_t));
+  ok &= A(&w.L, cap * sizeof(float4));
+  ok &= A(&w.cnt, (kMaxDepth + 1) * kCntStride * sizeof(int32_t));
+  if (!ok) {
+    free_wave(r);
+    return set_err(r, XB_E_OOM, "cannot allocate wave buffers for %lld paths", (long long)cap);
+  }
+  return XB_OK;
+}
+
+int check_ready(xb_renderer* r) {
+  if (!r) return xb::fail(XB_E_INVALID, "null renderer");
+  cudaError_t e = cudaSetDevice(r->cfg.device);
+  if (e != cudaSuccess) return set_err(r, XB_E_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return XB_OK;
+}
+
+enum { STAGE_RAYGEN = 0, STAGE_EXTEND = 1, STAGE_SHADE = 2, STAGE_SHADOW = 3, STAGE_ACCUM = 4 };
+
+// Stage timing: a pair of events around a launch, read back after the call's final sync.
+struct StageTimer {
+  xb_renderer* r;
+  int stage;
+  cudaEvent_t end = nullptr;
+  StageTimer(xb_renderer* rr, int st) : r(rr), stage(st) {
+    if (!(r->prof_flags & XB_PROFILE_STAGE_TIMES)) return;
+    if (r->ev_used + 2 > r->ev_pool.size()) {
+      for (int k = 0; k < 64; ++k) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        r->ev_pool.push_back(e);
+      }
+      r->ev_stage.resize(r->ev_pool.size() / 2);
+    }
+    cudaEventRecord(r->ev_pool[r->ev_used], r->stream);
+    end = r->ev_pool[r->ev_used + 1];
+    r->ev_stage[r->ev_used / 2] = stage;
+    r->ev_used += 2;
+  }
+  ~StageTimer() {
+    if (end) cudaEventRecord(end, r->stream);
+  }
+};
+
+void collect_stage_times(xb_renderer* r) {
+  for (size_t i = 0; i + 1 < r->ev_used; i += 2) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r->ev_pool[i], r->ev_pool[i + 1]) == cudaSuccess) {
+      const int st = r->ev_stage[i / 2];
+      r->stage_ms[st] += ms;
+      r->stage_launches[st] += 1;
+    }
+  }
+  r->ev_used = 0;
+}
+
+int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count) {
+  const int W = r->cfg.width, H = r->cfg.height;
+  const int64_t npix = (int64_t)W * H;
+  CamDev cd{v3(cam->eye[0], cam->eye[1], cam->eye[2]),
+            v3(cam->lower_left[0], cam->lower_left[1], cam->lower_left[2]),
+            v3(cam->horizontal[0], cam->horizontal[1], cam->horizontal[2]),
+            v3(cam->vertical[0], cam->vertical[1], cam->vertical[2])};
+  WaveBuffers& w = r->wb;
+  const int depth_max = std::min(r->max_bounces, kMaxDepth);
+  int done = 0;
+  while (done < spp_count) {
+    const int spw = std::min(r->spp_per_wave, spp_count - done);
+    const int64_t paths = npix * spw;
+    CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), r->stream));
+    const int g_rg = (int)std::min<int64_t>((paths + 255) / 256, (int64_t)r->num_sms * 16);
+    const bool count = (r->prof_flags & XB_PROFILE_COUNT_TRAVERSAL) != 0;
+    {
+      StageTimer t(r, STAGE_RAYGEN);
+      raygen_kernel<<<g_rg, 256, 0, r->stream>>>(cd, W, H, spp_first + done, paths, w.ray_o[0],
+                                                 w.ray_d[0], w.tp[0], w.rng[0], w.path[0], w.L, w.cnt);
+    }
+    for (int d = 0; d < depth_max; ++d) {
+      const int q = d & 1, nq = q ^ 1;
+      int32_t* cd_ = w.cnt + d * kCntStride;
+      {
+        StageTimer t(r, STAGE_EXTEND);
+        if (r->thread_per_ray) {
+          auto kern = count ? extend_kernel<true> : extend_kernel<false>;
+          kern<<<r->grid_ext, 128, 0, r->stream>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_,
+                                                   r->stats);
+        } else {
+          TraceQueue tq{w.ray_o[q], w.ray_d[q], cd_ + CNT_RAYS, cd_ + CNT_FETCH_EXT, w.hit, w.hit_inst,
+                        nullptr, nullptr, r->stats};
+          auto kern = count ? extend_persistent_kernel<true> : extend_persistent_kernel<false>;
+          kern<<<r->grid_pext, 128, 0, r->stream>>>(r->scene, tq, r->refill);
+        }
+      }
+      ShadeArgs sa;
+      sa.sc = r->scene;
+      sa.ray_o = w.ray_o[q]; sa.ray_d = w.ray_d[q]; sa.tp = w.tp[q]; sa.rng = w.rng[q]; sa.path = w.path[q];
+      sa.nray_o = w.ray_o[nq]; sa.nray_d = w.ray_d[nq]; sa.ntp = w.tp[nq]; sa.nrng = w.rng[nq];
+      sa.npath = w.path[nq];
+      sa.hit = w.hit; sa.hit_inst = w.hit_inst;
+      for (int k = 0; k < 2; ++k) { sa.sh_o[k] = w.sh_o[k]; sa.sh_d[k] = w.sh_d[k]; sa.sh_c[k] = w.sh_c[k]; }
+      sa.L = w.L;
+      sa.cnt = cd_;
+      sa.cnt_next = w.cnt + (d + 1) * kCntStride;
+      sa.depth = d; sa.min_bounces = r->min_bounces; sa.max_bounces = depth_max;
+      sa.capacity = (int)w.capacity;
+      sa.stats = r->stats;
+      {
+        StageTimer t(r, STAGE_SHADE);
+        shade_kernel<<<r->grid_shade, 128, 0, r->stream>>>(sa);
+      }
+      for (int k = 0; k < 2; ++k) {
+        if (k == 0 && r->scene.num_lights == 0) continue;
+        if (k == 1 && r->scene.num_suns == 0) continue;
+        StageTimer t(r, STAGE_SHADOW);
+        if (r->thread_per_ray) {
+          auto kern = count ? shadow_kernel<true> : shadow_kernel<false>;
+          kern<<<r->grid_shadow, 128, 0, r->stream>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
+                                                      cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
+                                                      cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats);
+        } else {
+          TraceQueue tq{w.sh_o[k], w.sh_d[k], cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
+                        cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), nullptr, nullptr, w.sh_c[k], w.L,
+                        r->stats};
+          auto kern = count ? shadow_persistent_kernel<true> : shadow_persistent_kernel<false>;
+          kern<<<r->grid_pshadow, 128, 0, r->stream>>>(r->scene, tq, r->refill);
+        }
+      }
+    }
+    const int g_acc = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)r->num_sms * 16);
+    {
+      StageTimer t(r, STAGE_ACCUM);
+      accumulate_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, npix, spw, r->spp + done, r->accum, r->sum64,
+                                                      r->m2_64, r->mean64, w.cnt, depth_max, paths, r->stats);
+    }
+    CK(cudaGetLastError());
+    done += spw;
+  }
+  return XB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xb_create(const xb_config* cfg, xb_renderer** out) {
+  if (!cfg || !out) return xb::fail(XB_E_INVALID, "xb_create: null argument");
+  *out = nullptr;
+  if (cfg->width <= 0 || cfg->height <= 0 || cfg->max_bounces < 0 || cfg->min_bounces < 0)
+    return xb::fail(XB_E_INVALID, "xb_create: bad size or bounces");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return xb::fail(XB_E_CUDA, "xb_create: no CUDA device");
+  if (cfg->device < 0 || cfg->device >= ndev) return xb::fail(XB_E_INVALID, "xb_create: bad device %d", cfg->device);
+  auto* r = new (std::nothrow) xb_renderer();
+  if (!r) return xb::fail(XB_E_OOM, "xb_create: out of memory");
+  r->cfg = *cfg;
+  r->min_bounces = cfg->min_bounces;
+  r->max_bounces = std::min(cfg->max_bounces, kMaxDepth);
+  auto bail = [&](int code) { xb_destroy(r); return code; };
+  if (cudaSetDevice(cfg->device) != cudaSuccess) return bail(xb::fail(XB_E_CUDA, "cudaSetDevice failed"));
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return bail(xb::fail(XB_E_CUDA, "cudaGetDeviceProperties failed"));
+  r->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess)
+    return bail(xb::fail(XB_E_CUDA, "stream/event creation failed"));
+  const int64_t npix = (int64_t)cfg->width * cfg->height;
+  if (cudaMalloc(&r->accum, npix * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&r->resolve_buf, npix * 3 * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&r->stats, STAT_COUNT * sizeof(unsigned long long)) != cudaSuccess)
+    return bail(xb::fail(XB_E_OOM, "framebuffer allocation failed"));
+  if (cfg->flags & XB_FLAG_FP64_ACCUM) {
+    if (cudaMalloc(&r->sum64, npix * 3 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&r->m2_64, npix * 3 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&r->mean64, npix * 3 * sizeof(double)) != cudaSuccess)
+      return bail(xb::fail(XB_E_OOM, "FP64 accumulation allocation failed"));
+  }
+  // Paths per wave: whole samples of every pixel, about 2^21 paths in flight by default.
+  int64_t target = cfg->wave_paths > 0 ? cfg->wave_paths : (int64_t)1 << 21;
+  r->spp_per_wave = (int)std::max<int64_t>(1, target / npix);
+  r->spp_per_wave = std::min(r->spp_per_wave, 1024);
+  int rc = alloc_wave(r, npix * r->spp_per_wave);
+  if (rc != XB_OK) return bail(rc);
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_kernel<false>, 128, 0);
+  r->grid_ext = r->num_sms * std::max(occ, 1);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_kernel<false>, 128, 0);
+  r->grid_shadow = r->num_sms * std::max(occ, 1);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel, 128, 0);
+  r->grid_shade = r->num_sms * std::max(occ, 1);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_persistent_kernel<false>, 128, 0);
+  r->grid_pext = r->num_sms * std::max(occ, 1);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_persistent_kernel<false>, 128, 0);
+  r->grid_pshadow = r->num_sms * std::max(occ, 1);
+  r->thread_per_ray = (cfg->flags & XB_FLAG_THREAD_PER_RAY) != 0;
+  rc = xb_reset(r);
+  if (rc != XB_OK) return bail(rc);
+  if (cudaMemset(r->stats, 0, STAT_COUNT * sizeof(unsigned long long)) != cudaSuccess)
+    return bail(xb::fail(XB_E_CUDA, "cudaMemset failed"));
+  *out = r;
+  return XB_OK;
+}
+
+void xb_destroy(xb_renderer* r) {
+  if (!r) return;
+  cudaSetDevice(r->cfg.device);
+  if (r->stream) cudaStreamSynchronize(r->stream);
+  free_scene(r);
+  free_wave(r);
+  void* ptrs[] = {r->accum, r->sum64, r->m2_64, r->mean64, r->resolve_buf, r->stats, r->scratch};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  for (cudaEvent_t e : r->ev_pool) cudaEventDestroy(e);
+  if (r->ev0) cudaEventDestroy(r->ev0);
+  if (r->ev1) cudaEventDestroy(r->ev1);
+  if (r->stream) cudaStreamDestroy(r->stream);
+  delete r;
+}
+
+int xb_last_error(const xb_renderer* r, char* buf, size_t len) {
+  if (!buf || !len) return XB_E_INVALID;
+  const std::string& s = (r && !r->err.empty()) ? r->err : xb::g_last_error;
+  std::snprintf(buf, len, "%s", s.c_str());
+  return XB_OK;
+}
+
+int xb_set_bounces(xb_renderer* r, int32_t min_b, int32_t max_b) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (min_b < 0 || max_b < 0 || max_b > kMaxDepth) return set_err(r, XB_E_INVALID, "bad bounces %d..%d", min_b, max_b);
+  r->min_bounces = min_b;
+  r->max_bounces = max_b;
+  return XB_OK;
+}
+
+int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!v) return set_err(r, XB_E_INVALID, "xb_upload_scene: null view");
+  CK(cudaStreamSynchronize(r->stream));
+  free_scene(r);
+  // ── meshes: BLAS nodes (odd-aligned per mesh), slot-ordered triangles ──
+  std::vector<float4> blas, tris;
+  std::vector<int32_t> tri_index, tri_mat, root_of(v->num_meshes, -1);
+  std::vector<float> nx, ny, nz;
+  std::vector<DevMesh> meshes(v->num_meshes);
+  int64_t slot_base = 0, tri_base = 0, vtx_base = 0;
+  for (int m = 0; m < v->num_meshes; ++m) {
+    const xb_mesh_view& mv = v->meshes[m];
+    if (mv.num_triangles > 0 && (!mv.blas_nodes || mv.num_blas_nodes <= 0 || !mv.blas_prims))
+      return set_err(r, XB_E_INVALID, "mesh %d has no BLAS", m);
+    if ((blas.size() / 2) % 2 == 0) { blas.push_back(make_float4(0, 0, 0, 0)); blas.push_back(make_float4(0, 0, 0, 0)); }
+    const int64_t node_base = (int64_t)blas.size() / 2;
+    if (mv.num_blas_nodes > 0) root_of[m] = (int32_t)node_base;
+    for (int i = 0; i < mv.num_blas_nodes; ++i) {
+      const xb_bvh_node& nd = mv.blas_nodes[i];
+      uint32_t child;
+      if (nd.count > 0) {
+        if ((int64_t)nd.child + nd.count > mv.num_triangles) return set_err(r, XB_E_INVALID, "mesh %d BLAS leaf out of range", m);
+        child = (uint32_t)(slot_base + nd.child);
+      } else {
+        if ((int64_t)nd.child + 1 >= mv.num_blas_nodes) return set_err(r, XB_E_INVALID, "mesh %d BLAS child out of range", m);
+        child = (uint32_t)(node_base + nd.child);
+      }
+      blas.push_back(node_lo(nd));
+      blas.push_back(node_hi(nd, child));
+    }
+    for (int s = 0; s < mv.num_triangles; ++s) {
+      const uint32_t t = mv.blas_prims[s];
+      if ((int)t >= mv.num_triangles) return set_err(r, XB_E_INVALID, "mesh %d prim index out of range", m);
+      const int i0 = mv.indices[3 * t], i1 = mv.indices[3 * t + 1], i2 = mv.indices[3 * t + 2];
+      tris.push_back(make_float4(mv.vx[i0], mv.vy[i0], mv.vz[i0], i32_bits_to_f((int)t)));
+      tris.push_back(make_float4(mv.vx[i1], mv.vy[i1], mv.vz[i1], i32_bits_to_f((int)(tri_base + t))));
+      tris.push_back(make_float4(mv.vx[i2], mv.vy[i2], mv.vz[i2], 0.f));
+    }
+    for (int t = 0; t < mv.num_triangles; ++t) {
+      for (int k = 0; k < 3; ++k) {
+        const int vi = mv.indices[3 * t + k];
+        if (vi < 0 || vi >= mv.num_vertices) return set_err(r, XB_E_INVALID, "mesh %d vertex index out of range", m);
+        tri_index.push_back((int32_t)(vtx_base + vi));
+      }
+      const int mid = mv.mat_ids ? mv.mat_ids[t] : 0;
+      if (mid < 0 || mid >= v->num_materials) return set_err(r, XB_E_INVALID, "mesh %d triangle %d material %d out of range", m, t, mid);
+      tri_mat.push_back(mid);
+    }
+    meshes[m].tri_offset = (int32_t)tri_base;
+    meshes[m].vtx_offset = (int32_t)vtx_base;
+    meshes[m].has_normals = mv.nx != nullptr;
+    for (int i = 0; i < mv.num_vertices; ++i) {
+      nx.push_back(mv.nx ? mv.nx[i] : 0.f);
+      ny.push_back(mv.ny ? mv.ny[i] : 0.f);
+      nz.push_back(mv.nz ? mv.nz[i] : 0.f);
+    }
+    slot_base += mv.num_triangles;
+    tri_base += mv.num_triangles;
+    vtx_base += mv.num_vertices;
+  }
+  // ── analytic prims in PrimBLAS slot order ──
+  std::vector<float4> pnodes, prims;
+  for (int i = 0; i < v->num_prim_nodes; ++i) {
+    const xb_bvh_node& nd = v->prim_nodes[i];
+    pnodes.push_back(node_lo(nd));
+    pnodes.push_back(node_hi(nd, nd.child));
+  }
+  for (int s = 0; s < v->num_prims; ++s) {
+    const uint32_t pi = v->prim_indices ? v->prim_indices[s] : (uint32_t)s;
+    if ((int)pi >= v->num_prims) return set_err(r, XB_E_INVALID, "prim index out of range");
+    const xb_prim& q = v->prims[pi];
+    if (q.mat_id < 0 || q.mat_id >= v->num_materials) return set_err(r, XB_E_INVALID, "prim %u material out of range", pi);
+    prims.push_back(make_float4(i32_bits_to_f(q.type), i32_bits_to_f(q.mat_id), i32_bits_to_f((int)pi), 0.f));
+    prims.push_back(make_float4(q.p[0], q.p[1], q.p[2], q.p[3]));
+    prims.push_back(make_float4(q.p[4], q.p[5], q.p[6], q.p[7]));
+    prims.push_back(make_float4(q.p[8], q.p[9], 0.f, 0.f));
+  }
+  // ── TLAS and instances ──
+  std::vector<float4> tlas;
+  for (int i = 0; i < v->num_tlas_nodes; ++i) {
+    tlas.push_back(node_lo(v->tlas_nodes[i]));
+    tlas.push_back(node_hi(v->tlas_nodes[i], v->tlas_nodes[i].child));
+  }
+  std::vector<uint32_t> tinst(v->tlas_inst_indices, v->tlas_inst_indices + v->num_instances);
+  std::vector<DevInstance> insts(v->num_instances);
+  for (int i = 0; i < v->num_instances; ++i) {
+    const xb_instance_view& iv = v->instances[i];
+    DevInstance& d = insts[i];
+    std::memcpy(d.w2l, iv.world_to_local, sizeof(d.w2l));
+    d.instance_id = iv.instance_id;
+    if (iv.geom == XB_GEOM_PRIMS) {
+      d.kind = 1; d.root = 0; d.mesh = -1;
+      if (v->num_prim_nodes == 0) return set_err(r, XB_E_INVALID, "instance %d uses the empty prim group", i);
+    } else {
+      if (iv.geom < 0 || iv.geom >= v->num_meshes) return set_err(r, XB_E_INVALID, "instance %d: bad mesh %d", i, iv.geom);
+      d.kind = 0; d.root = root_of[iv.geom]; d.mesh = iv.geom;
+      if (d.root < 0) return set_err(r, XB_E_INVALID, "instance %d uses an empty mesh", i);
+    }
+  }
+  // ── materials, emitters, sky ──
+  std::vector<DevMaterial> mats;
+  for (int i = 0; i < v->num_materials; ++i) mats.push_back(to_dev_material(v->materials[i]));
+  std::vector<DevLight> lights;
+  for (int i = 0; i < v->num_lights; ++i) {
+    const xb_light& l = v->lights[i];
+    xb::LightGeom g;
+    if (!xb::light_geometry(*v, l, &g)) return set_err(r, XB_E_INVALID, "light %d refers to a missing triangle", i);
+    DevLight d;
+    d.p0 = make_float4(g.p0[0], g.p0[1], g.p0[2], l.area);
+    d.p1 = make_float4(g.p1[0], g.p1[1], g.p1[2], i32_bits_to_f((int)l.mesh_id));
+    d.p2 = make_float4(g.p2[0], g.p2[1], g.p2[2], i32_bits_to_f((int)l.tri_idx));
+    d.n = make_float4(g.n[0], g.n[1], g.n[2], 0.f);
+    d.emission = make_float4(l.emission[0], l.emission[1], l.emission[2], 0.f);
+    lights.push_back(d);
+  }
+  std::vector<DevSun> suns;
+  for (int i = 0; i < v->num_suns; ++i) {
+    DevSun s;
+    std::memcpy(s.dir, v->suns[i].direction, sizeof(s.dir));
+    xb::sun_emission(v->suns[i], s.emission);
+    suns.push_back(s);
+  }
+  DevScene& sc = r->scene;
+  std::memset(&sc, 0, sizeof(sc));
+  const float4* cp4;
+  if ((rc = dev_upload(r, blas, &sc.blas))) return rc;
+  if ((rc = dev_upload(r, tris, &sc.tris))) return rc;
+  if ((rc = dev_upload(r, pnodes, &sc.pnodes))) return rc;
+  if ((rc = dev_upload(r, prims, &sc.prims))) return rc;
+  if ((rc = dev_upload(r, tlas, &cp4))) return rc;
+  sc.tlas = cp4;
+  if ((rc = dev_upload(r, tinst, &sc.tlas_inst))) return rc;
+  if ((rc = dev_upload(r, insts, &sc.inst))) return rc;
+  if ((rc = dev_upload(r, meshes, &sc.meshes))) return rc;
+  if ((rc = dev_upload(r, tri_index, &sc.tri_index))) return rc;
+  if ((rc = dev_upload(r, tri_mat, &sc.tri_mat))) return rc;
+  if ((rc = dev_upload(r, nx, &sc.nx))) return rc;
+  if ((rc = dev_upload(r, ny, &sc.ny))) return rc;
+  if ((rc = dev_upload(r, nz, &sc.nz))) return rc;
+  if ((rc = dev_upload(r, mats, &sc.mats))) return rc;
+  if ((rc = dev_upload(r, lights, &sc.lights))) return rc;
+  if ((rc = dev_upload(r, suns, &sc.suns))) return rc;
+  sc.num_lights = v->num_lights;
+  sc.num_suns = v->num_suns;
+  sc.num_tlas_nodes = v->num_tlas_nodes;
+  sc.num_materials = v->num_materials;
+  std::memcpy(sc.sky_zenith, v->sky.zenith, sizeof(sc.sky_zenith));
+  std::memcpy(sc.sky_horizon, v->sky.horizon, sizeof(sc.sky_horizon));
+  std::memcpy(sc.sky_ground, v->sky.ground, sizeof(sc.sky_ground));
+  sc.sky_inv_sharpness = 1.0f / v->sky.sharpness;
+  sc.sky_intensity = v->sky.intensity;
+  r->has_scene = true;
+  return XB_OK;
+}
+
+int xb_reset(xb_renderer* r) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  const int64_t npix = (int64_t)r->cfg.width * r->cfg.height;
+  CK(cudaMemsetAsync(r->accum, 0, npix * sizeof(float4), r->stream));
+  if (r->sum64) {
+    CK(cudaMemsetAsync(r->sum64, 0, npix * 3 * sizeof(double), r->stream));
+    CK(cudaMemsetAsync(r->m2_64, 0, npix * 3 * sizeof(double), r->stream));
+    CK(cudaMemsetAsync(r->mean64, 0, npix * 3 * sizeof(double), r->stream));
+  }
+  r->spp = 0;
+  CK(cudaStreamSynchronize(r->stream));
+  return XB_OK;
+}
+
+int xb_render_range(xb_renderer* r, const xb_camera* cam, int32_t spp_first, int32_t spp_count) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!cam) return set_err(r, XB_E_INVALID, "xb_render: null camera");
+  if (!r->has_scene) return set_err(r, XB_E_STATE, "xb_render: no scene uploaded");
+  if (spp_count < 0 || spp_first < 1) return set_err(r, XB_E_INVALID, "xb_render: bad sample range");
+  if (spp_count == 0) return XB_OK;
+  unsigned long long ov_before = 0;
+  CK(cudaMemcpyAsync(&ov_before, r->stats + STAT_OVERFLOW, sizeof(ov_before), cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaEventRecord(r->ev0, r->stream));
+  rc = run_waves(r, cam, spp_first, spp_count);
+  if (rc) return rc;
+  CK(cudaEventRecord(r->ev1, r->stream));
+  r->spp += spp_count;
+  unsigned long long ov_after = 0;
+  CK(cudaMemcpyAsync(&ov_after, r->stats + STAT_OVERFLOW, sizeof(ov_after), cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  CK(cudaEventElapsedTime(&r->last_ms, r->ev0, r->ev1));
+  collect_stage_times(r);
+  if (ov_after != ov_before)
+    return set_err(r, XB_E_OVERFLOW, "%llu queue/stack overflows during render (work dropped)", ov_after - ov_before);
+  return XB_OK;
+}
+
+int xb_render(xb_renderer* r, const xb_camera* cam, int32_t spp_to_add) {
+  if (!r) return xb::fail(XB_E_INVALID, "null renderer");
+  return xb_render_range(r, cam, r->spp + 1, spp_to_add);
+}
+
+int xb_resolve(xb_renderer* r, float* out) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!out) return set_err(r, XB_E_INVALID, "xb_resolve: null output");
+  const int W = r->cfg.width, H = r->cfg.height;
+  const float inv = r->spp > 0 ? 1.0f / (float)r->spp : 0.f;
+  resolve_kernel<<<r->num_sms * 8, 256, 0, r->stream>>>(r->accum, W, H, inv, r->resolve_buf);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, r->resolve_buf, (size_t)W * H * 3 * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return XB_OK;
+}
+
+int xb_resolve_fp64(xb_renderer* r, double* sum, double* m2) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!r->sum64) return set_err(r, XB_E_STATE, "renderer was created without XB_FLAG_FP64_ACCUM");
+  // rows are flipped to the top-down order of xb_resolve (cpu_tiled.cpp:224-236)
+  const int W = r->cfg.width, H = r->cfg.height;
+  const size_t row = (size_t)W * 3;
+  std::vector<double> tmp((size_t)H * row);
+  double* outs[2] = {sum, m2};
+  const double* srcs[2] = {r->sum64, r->m2_64};
+  for (int k = 0; k < 2; ++k) {
+    if (!outs[k]) continue;
+    CK(cudaMemcpyAsync(tmp.data(), srcs[k], tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, r->stream));
+    CK(cudaStreamSynchronize(r->stream));
+    for (int y = 0; y < H; ++y) std::memcpy(outs[k] + (size_t)(H - 1 - y) * row, tmp.data() + (size_t)y * row, row * sizeof(double));
+  }
+  return XB_OK;
+}
+
+int xb_get_spp(const xb_renderer* r) { return r ? r->spp : XB_E_INVALID; }
+
+int xb_get_render_stats(const xb_renderer* r_, xb_render_stats* out) {
+  xb_renderer* r = const_cast<xb_renderer*>(r_);
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!out) return set_err(r, XB_E_INVALID, "null output");
+  unsigned long long s[STAT_COUNT];
+  CK(cudaMemcpyAsync(s, r->stats, sizeof(s), cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  out->rays_closest = (int64_t)s[STAT_RAYS];
+  out->rays_shadow = (int64_t)s[STAT_SHADOW];
+  out->paths = (int64_t)s[STAT_PATHS];
+  out->overflow = (int64_t)s[STAT_OVERFLOW];
+  out->last_ms = r->last_ms;
+  return XB_OK;
+}
+
+int xb_reset_render_stats(xb_renderer* r) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(r->stats, 0, STAT_COUNT * sizeof(unsigned long long), r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return XB_OK;
+}
+
+int xb_set_profiling(xb_renderer* r, int32_t flags) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (flags & ~(XB_PROFILE_STAGE_TIMES | XB_PROFILE_COUNT_TRAVERSAL)) return set_err(r, XB_E_INVALID, "bad profiling flags");
+  r->prof_flags = flags;
+  return XB_OK;
+}
+
+int xb_get_profile(const xb_renderer* r_, xb_profile* out) {
+  xb_renderer* r = const_cast<xb_renderer*>(r_);
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!out) return set_err(r, XB_E_INVALID, "null output");
+  unsigned long long s[STAT_COUNT];
+  CK(cudaMemcpyAsync(s, r->stats, sizeof(s), cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  std::memset(out, 0, sizeof(*out));
+  out->raygen_ms = r->stage_ms[STAGE_RAYGEN]; out->extend_ms = r->stage_ms[STAGE_EXTEND];
+  out->shade_ms = r->stage_ms[STAGE_SHADE]; out->shadow_ms = r->stage_ms[STAGE_SHADOW];
+  out->accumulate_ms = r->stage_ms[STAGE_ACCUM];
+  out->raygen_launches = r->stage_launches[STAGE_RAYGEN];
+  out->extend_launches = r->stage_launches[STAGE_EXTEND];
+  out->shade_launches = r->stage_launches[STAGE_SHADE];
+  out->shadow_launches = r->stage_launches[STAGE_SHADOW];
+  out->accumulate_launches = r->stage_launches[STAGE_ACCUM];
+  out->ext_blas_nodes = (int64_t)s[STAT_EXT_WORK]; out->ext_tris = (int64_t)s[STAT_EXT_WORK + 1];
+  out->ext_tlas_nodes = (int64_t)s[STAT_EXT_WORK + 2]; out->ext_instances = (int64_t)s[STAT_EXT_WORK + 3];
+  out->sh_blas_nodes = (int64_t)s[STAT_SH_WORK]; out->sh_tris = (int64_t)s[STAT_SH_WORK + 1];
+  out->sh_tlas_nodes = (int64_t)s[STAT_SH_WORK + 2]; out->sh_instances = (int64_t)s[STAT_SH_WORK + 3];
+  return XB_OK;
+}
+
+int xb_reset_profile(xb_renderer* r) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  for (int i = 0; i < 5; ++i) { r->stage_ms[i] = 0; r->stage_launches[i] = 0; }
+  unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  CK(cudaMemcpyAsync(r->stats + STAT_EXT_WORK, z, sizeof(z), cudaMemcpyHostToDevice, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return XB_OK;
+}
+
+int xb_trace_rays_device(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit* hits, int32_t mode,
+                         void* stream) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!r->has_scene) return set_err(r, XB_E_STATE, "xb_trace_rays: no scene uploaded");
+  if (n < 0 || (n > 0 && (!rays || !hits))) return set_err(r, XB_E_INVALID, "xb_trace_rays: bad arguments");
+  if (mode != XB_TRACE_CLOSEST && mode != XB_TRACE_ANY) return set_err(r, XB_E_INVALID, "bad trace mode %d", mode);
+  if (n == 0) return XB_OK;
+  cudaStream_t s = stream ? (cudaStream_t)stream : r->stream;
+  const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)r->num_sms * 16);
+  trace_full_kernel<<<grid, 128, 0, s>>>(r->scene, rays, n, hits, mode, r->stats);
+  CK(cudaGetLastError());
+  return XB_OK;
+}
+
+int xb_trace_rays(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit* hits, int32_t mode) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && (!rays || !hits))) return set_err(r, XB_E_INVALID, "xb_trace_rays: bad arguments");
+  if (n == 0) return XB_OK;
+  xb_ray* dr = nullptr;
+  xb_hit* dh = nullptr;
+  CK(cudaMalloc(&dr, n * sizeof(xb_ray)));
+  if (cudaMalloc(&dh, n * sizeof(xb_hit)) != cudaSuccess) {
+    cudaFree(dr);
+    return set_err(r, XB_E_OOM, "xb_trace_rays: out of device memory");
+  }
+  unsigned long long ov0 = 0, ov1 = 0;
+  cudaMemcpyAsync(&ov0, r->stats + STAT_OVERFLOW, sizeof(ov0), cudaMemcpyDeviceToHost, r->stream);
+  cudaMemcpyAsync(dr, rays, n * sizeof(xb_ray), cudaMemcpyHostToDevice, r->stream);
+  rc = xb_trace_rays_device(r, dr, n, dh, mode, r->stream);
+  if (rc == XB_OK) {
+    cudaMemcpyAsync(hits, dh, n * sizeof(xb_hit), cudaMemcpyDeviceToHost, r->stream);
+    cudaMemcpyAsync(&ov1, r->stats + STAT_OVERFLOW, sizeof(ov1), cudaMemcpyDeviceToHost, r->stream);
+    cudaError_t e = cudaStreamSynchronize(r->stream);
+    if (e != cudaSuccess) rc = set_err(r, XB_E_CUDA, "xb_trace_rays: %s", cudaGetErrorString(e));
+    else if (ov1 != ov0) rc = set_err(r, XB_E_OVERFLOW, "xb_trace_rays: traversal stack overflow");
+  }
+  cudaFree(dr);
+  cudaFree(dh);
+  return rc;
+}
+
+int xb_bsdf_eval(const xb_material* m, int64_t n, const float* wo, const float* wi, float* f, float* pdf) {
+  if (!m || n < 0 || (n > 0 && (!wo || !wi || !f || !pdf))) return xb::fail(XB_E_INVALID, "xb_bsdf_eval: bad arguments");
+  if (n == 0) return XB_OK;
+  float *d = nullptr;
+  const size_t bytes = (size_t)n * 10 * sizeof(float);
+  if (cudaMalloc(&d, bytes) != cudaSuccess) return xb::fail(XB_E_OOM, "xb_bsdf_eval: out of device memory");
+  float *dwo = d, *dwi = d + 3 * n, *df = d + 6 * n, *dp = d + 9 * n;
+  cudaMemcpy(dwo, wo, n * 3 * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(dwi, wi, n * 3 * sizeof(float), cudaMemcpyHostToDevice);
+  bsdf_eval_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256>>>(to_dev_material(*m), n, dwo, dwi, df, dp);
+  cudaMemcpy(f, df, n * 3 * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpy(pdf, dp, n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return xb::fail(XB_E_CUDA, "xb_bsdf_eval: %s", cudaGetErrorString(e));
+  return XB_OK;
+}
+
+int xb_bsdf_sample(const xb_material* m, int64_t n, const float* wo, uint64_t* st, float* wi, float* f,
+                   float* pdf, int32_t* flags) {
+  if (!m || n < 0 || (n > 0 && (!wo || !st || !wi || !f || !pdf || !flags)))
+    return xb::fail(XB_E_INVALID, "xb_bsdf_sample: bad arguments");
+  if (n == 0) return XB_OK;
+  char* d = nullptr;
+  const size_t bytes = (size_t)n * (3 + 3 + 3 + 1 + 1) * sizeof(float) + (size_t)n * sizeof(uint64_t);
+  if (cudaMalloc(&d, bytes) != cudaSuccess) return xb::fail(XB_E_OOM, "xb_bsdf_sample: out of device memory");
+  uint64_t* dst = reinterpret_cast<uint64_t*>(d);
+  float* dwo = reinterpret_cast<float*>(d + n * sizeof(uint64_t));
+  float *dwi = dwo + 3 * n, *df = dwo + 6 * n, *dp = dwo + 9 * n;
+  int32_t* dfl = reinterpret_cast<int32_t*>(dwo + 10 * n);
+  cudaMemcpy(dst, st, n * sizeof(uint64_t), cudaMemcpyHostToDevice);
+  cudaMemcpy(dwo, wo, n * 3 * sizeof(float), cudaMemcpyHostToDevice);
+  bsdf_sample_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256>>>(to_dev_material(*m), n, dwo, dst, dwi, df, dp, dfl);
+  cudaMemcpy(st, dst, n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+  cudaMemcpy(wi, dwi, n * 3 * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(f, df, n * 3 * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(pdf, dp, n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpy(flags, dfl, n * sizeof(int32_t), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return xb::fail(XB_E_CUDA, "xb_bsdf_sample: %s", cudaGetErrorString(e));
+  return XB_OK;
+}
+
+}  // extern "C"

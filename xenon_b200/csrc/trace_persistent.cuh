@@ -1,0 +1,228 @@
+// trace_persistent.cuh — persistent-warp traversal of a ray queue with per-lane refill.
+//
+// A warp holds 32 rays. Each outer iteration: lanes without a ray take new ones from the queue
+// (one atomic per warp for all idle lanes), then all lanes run "while-while" traversal:
+//   phase A  interior work (TLAS nodes, instance entry, BLAS interior nodes) until every lane
+//            has a leaf pending or has finished its ray;
+//   phase B  the pending leaves' triangle tests.
+// A lane that finishes writes its result and becomes idle, to be refilled on the next outer
+// iteration; so a long ray no longer holds 31 finished lanes hostage, which was the main loss of
+// the one-ray-per-thread kernel (7 of 32 lanes active on average).
+//
+// Per ray, nodes and triangles are visited in exactly the order of the reference's recursive
+// loops (tlas.cpp:172-245, blas.cpp:211-265): closest-hit results, including which of two
+// equal-t triangles wins, are the reference's. Any-hit rays (kAny) only need *whether* some
+// triangle lies in [tmin, tmax], which does not depend on order, so they descend nearest child
+// first to find occluders sooner.
+#pragma once
+
+#include "dev_scene.cuh"
+
+namespace xbd {
+
+struct TraceQueue {
+  const float4* ray_o;      // org xyz, w = tmin (closest) / tmax (any-hit shadow items)
+  const float4* ray_d;      // dir xyz, w = tmax (closest) / bits(path) (shadow items)
+  const int32_t* count;     // number of rays (device)
+  int32_t* fetch;           // work cursor (device, zeroed before launch)
+  // closest-hit outputs
+  float4* hit;              // t, u, v, bits(prim)
+  int32_t* hit_inst;
+  // any-hit (shadow) outputs: unoccluded items add contrib to L[path]
+  const float4* contrib;
+  float4* L;
+  unsigned long long* stats;
+};
+
+template <bool kAny, bool kCount>
+__device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const TraceQueue& q,
+                                                       int refill) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int n = *q.count;
+  uint32_t tstack[kStackSize];
+  uint32_t bstack[kStackSize];
+  TraversalCounters cnt{0, 0, 0, 0};
+  bool overflow = false;
+
+  int ray = -1;                   // queue index of this lane's ray, -1 = idle
+  bool exhausted = false;         // the queue has no more rays for this warp
+  V3 wo = v3s(0.f), wd = v3s(0.f), winv = v3s(0.f);
+  float tmin = 0.f, tmax = kInf;
+  int sign0 = 0, sign1 = 0, sign2 = 0;
+  V3 lo = v3s(0.f), ld = v3s(0.f), linv = v3s(0.f);
+  int tsp = 0, bsp = 0;
+  int cur_inst = -1;              // instance being traversed (-1: at TLAS level)
+  uint32_t tl_child = 0, tl_count = 0, tl_i = 0;   // instances of the current TLAS leaf
+  uint32_t leaf_child = 0, leaf_count = 0;         // pending BLAS leaf
+  HitState h{kInf, 0.f, 0.f, -1, -1};
+  bool occluded = false;
+
+  for (;;) {
+    // ── refill idle lanes ──
+    const unsigned idle = __ballot_sync(FULL, ray < 0);
+    if (!exhausted && __popc(idle) >= refill) {
+      int base = 0;
+      const int leader = __ffs(idle) - 1;
+      if (lane == leader) base = atomicAdd(q.fetch, __popc(idle));
+      base = __shfl_sync(FULL, base, leader);
+      if (base >= n) exhausted = true;
+      if (ray < 0) {
+        const int mine = base + __popc(idle & ((1u << lane) - 1u));
+        if (mine < n) {
+          ray = mine;
+          const float4 o = q.ray_o[ray], d = q.ray_d[ray];
+          wo = v3(o.x, o.y, o.z);
+          wd = v3(d.x, d.y, d.z);
+          if (kAny) { tmin = kShadowEps; tmax = o.w; }
+          else { tmin = o.w; tmax = d.w; }
+          winv = v3(1.f / wd.x, 1.f / wd.y, 1.f / wd.z);
+          sign0 = wd.x < 0.f; sign1 = wd.y < 0.f; sign2 = wd.z < 0.f;
+          tsp = 0; bsp = 0; cur_inst = -1; tl_count = 0; tl_i = 0; leaf_count = 0;
+          h = HitState{kInf, 0.f, 0.f, -1, -1};
+          occluded = false;
+          if (sc.num_tlas_nodes > 0) tstack[tsp++] = 0;
+        }
+      }
+    }
+    if (__ballot_sync(FULL, ray >= 0) == 0 && exhausted) break;
+
+    // ── phase A: interior work until a leaf is pending or the ray is finished ──
+    bool want = (ray >= 0);
+    while (__any_sync(FULL, want)) {
+      if (want) {
+        if (bsp > 0) {
+          // BLAS node (blas.cpp:222-263)
+          const uint32_t idx = bstack[--bsp];
+          const float4 nb = ldg4(sc.blas + 2 * idx + 1);
+          const uint32_t child = __float_as_uint(nb.z), count = __float_as_uint(nb.w);
+          if (count > 0) {
+            leaf_child = child;
+            leaf_count = count;
+            want = false;
+          } else {
+            if (kCount) cnt.nodes++;
+            const float4* pp = sc.blas + 2 * (size_t)child;
+            const float4 la = ldg4(pp), lb = ldg4(pp + 1), ra = ldg4(pp + 2), rb = ldg4(pp + 3);
+            float tl, tr;
+            const float tcull = kAny ? tmax : h.t;
+            const bool hl = slab_sse(la, lb, linv, lo, tmin, tcull, tl);
+            const bool hr = slab_sse(ra, rb, linv, lo, tmin, tcull, tr);
+            if (hl || hr) {
+              if (bsp + 2 > kStackSize) {
+                overflow = true;
+                bsp = 0; tsp = 0; tl_count = 0;   // abandon the ray (reported as overflow)
+              } else if (hl && hr) {
+                // closest: the reference order (nearer tn on top); any: same rule
+                if (tl < tr) { bstack[bsp++] = child + 1; bstack[bsp++] = child; }
+                else { bstack[bsp++] = child; bstack[bsp++] = child + 1; }
+              } else {
+                bstack[bsp++] = hl ? child : child + 1;
+              }
+            }
+          }
+        } else if (tl_i < tl_count) {
+          // enter the next instance of the current TLAS leaf (tlas.cpp:200-218)
+          const int ii = (int)__ldg(sc.tlas_inst + tl_child + tl_i);
+          ++tl_i;
+          const DevInstance& in = sc.inst[ii];
+          if (kCount) cnt.inst++;
+          const Ray wr{wo, wd, tmin, tmax};
+          const Ray lr = to_local(in, wr);
+          if (in.kind == 0) {
+            lo = lr.o; ld = lr.d;
+            linv = v3(1.f / ld.x, 1.f / ld.y, 1.f / ld.z);
+            cur_inst = ii;
+            bstack[bsp++] = (uint32_t)in.root;
+          } else {
+            // analytic prims: a short scalar walk, done in place
+            if (kAny) {
+              if (pblas_any(sc, lr, bstack, overflow)) { occluded = true; bsp = 0; tsp = 0; tl_count = 0; }
+            } else {
+              pblas_closest(sc, lr, h, ii, bstack, overflow);
+            }
+          }
+          if (kAny && occluded) want = false;
+        } else if (tsp > 0) {
+          // TLAS node (tlas.cpp:186-242)
+          const uint32_t idx = tstack[--tsp];
+          const float4 na = ldg4(sc.tlas + 2 * idx), nb = ldg4(sc.tlas + 2 * idx + 1);
+          if (kCount) cnt.tlas++;
+          const int sgn[3] = {sign0, sign1, sign2};
+          if (aabb_fast(na, nb, winv, wo, sgn, tmin, kAny ? tmax : h.t)) {
+            const uint32_t child = __float_as_uint(nb.z), count = __float_as_uint(nb.w);
+            if (count > 0) {
+              tl_child = child; tl_count = count; tl_i = 0;
+            } else if (tsp + 2 > kStackSize) {
+              overflow = true;
+              tsp = 0;
+            } else {
+              const float ex = na.w - na.x, ey = nb.x - na.y, ez = nb.y - na.z;
+              const int ax = (ex > ey && ex > ez) ? 0 : (ey > ez ? 1 : 2);
+              const float4 la = ldg4(sc.tlas + 2 * child), lb = ldg4(sc.tlas + 2 * child + 1);
+              const float4 ra = ldg4(sc.tlas + 2 * child + 2), rb = ldg4(sc.tlas + 2 * child + 3);
+              float cl, cr;
+              if (ax == 0) { cl = (la.x + la.w) * 0.5f; cr = (ra.x + ra.w) * 0.5f; }
+              else if (ax == 1) { cl = (la.y + lb.x) * 0.5f; cr = (ra.y + rb.x) * 0.5f; }
+              else { cl = (la.z + lb.y) * 0.5f; cr = (ra.z + rb.y) * 0.5f; }
+              const float tl = (cl - comp(wo, ax)) * comp(winv, ax);
+              const float tr = (cr - comp(wo, ax)) * comp(winv, ax);
+              if (tl < tr) { tstack[tsp++] = child + 1; tstack[tsp++] = child; }
+              else { tstack[tsp++] = child; tstack[tsp++] = child + 1; }
+            }
+          }
+        } else {
+          // ray finished
+          want = false;
+          if (kAny) {
+            if (!occluded) {
+              const float4 c = q.contrib[ray];
+              const int p = __float_as_int(q.ray_d[ray].w);
+              float4 l = q.L[p];
+              l.x = l.x + c.x; l.y = l.y + c.y; l.z = l.z + c.z;
+              q.L[p] = l;
+            }
+          } else {
+            q.hit[ray] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+            q.hit_inst[ray] = h.inst;
+          }
+          ray = -1;
+        }
+      }
+    }
+
+    // ── phase B: the pending leaf's triangles (blas.cpp:224-233 / 281-287) ──
+    if (leaf_count > 0) {
+      const float tlim = kAny ? tmax : h.t;
+      float tbest = tlim;
+      for (uint32_t i = 0; i < leaf_count; ++i) {
+        const float4* tp = sc.tris + 3 * (size_t)(leaf_child + i);
+        const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
+        if (kCount) cnt.tris++;
+        float t, u, v;
+        if (ray_triangle(lo, ld, tmin, ld3(a), ld3(b), ld3(c), kAny ? tmax : tbest, t, u, v)) {
+          if (kAny) {
+            occluded = true;
+            break;
+          }
+          tbest = t;
+          h.t = t; h.u = u; h.v = v;
+          h.prim = (int32_t)(leaf_child + i);
+          h.inst = cur_inst;
+        }
+      }
+      leaf_count = 0;
+      if (kAny && occluded) { bsp = 0; tsp = 0; tl_count = 0; }
+    }
+  }
+  if (overflow) atomicAdd(q.stats + 3, 1ull);
+  if (kCount) {
+    unsigned long long* dst = q.stats + (kAny ? 12 : 8);
+    atomicAdd(dst + 0, (unsigned long long)cnt.nodes);
+    atomicAdd(dst + 1, (unsigned long long)cnt.tris);
+    atomicAdd(dst + 2, (unsigned long long)cnt.tlas);
+    atomicAdd(dst + 3, (unsigned long long)cnt.inst);
+  }
+}
+
+}  // namespace xbd
