@@ -249,6 +249,10 @@ def main():
     r.upload_scene(hs)
     cam = xb.camera(desc.eye, desc.target, desc.fov, W / H)
     npix = W * H
+    from xenon_b200 import autotune
+    tuned = autotune.load_tuning("config2") if (W, H, args.level) == (1920, 1080, 8) else None
+    if tuned:
+        r.set_tuning(**tuned)
 
     # traversal work per ray (untimed pass with counters), for the roofline's algorithmic bytes
     r.set_profiling(abi.XB_PROFILE_COUNT_TRAVERSAL)
@@ -362,6 +366,7 @@ def main():
                 "config": {"workload": WORKLOAD, "paths_per_step": npix, "rays_per_path": rays_per_path,
                            "msamples_per_s": msamples, "l2": "flushed between timed steps (256 MiB write)",
                            "parallelism": f"sample-sharded x{ws}" if ws > 1 else "1 GPU",
+                           "tuning": r.tuning(), "tuning_source": "xenon_b200/tuning (autotuner)" if tuned else "defaults",
                            "stage_ms_per_step": {k: getattr(prof, k) / args.steps for k in
                                                  ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms")}},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),

@@ -291,6 +291,21 @@ typedef struct xb_render_stats {
 int  xb_get_render_stats(const xb_renderer *r, xb_render_stats *out);
 int  xb_reset_render_stats(xb_renderer *r);
 
+/* Launch tuning (picked per GPU and scene by xenon_b200/autotune.py). Zero fields keep the
+ * current value; negative fields restore the default. */
+typedef struct xb_tuning {
+  int32_t extend_persistent_from_depth; /* closest-hit rays of bounces >= this use persistent
+                                           warps, earlier bounces one ray per thread (64: never) */
+  int32_t shadow_persistent;            /* 1: persistent warps for shadow rays, 2: one per thread */
+  int32_t refill;                       /* persistent warps refill when this many lanes idle */
+  int32_t extend_blocks_per_sm;         /* resident blocks of 128 threads per SM for the trace */
+  int32_t shadow_blocks_per_sm;         /* kernels; bounded by the kernel's occupancy limit */
+  int32_t shade_blocks_per_sm;
+  int32_t wave_paths;                   /* paths in flight per wave (reallocates queues) */
+} xb_tuning;
+int  xb_set_tuning(xb_renderer *r, const xb_tuning *t);
+int  xb_get_tuning(const xb_renderer *r, xb_tuning *out);
+
 /* Profiling (tracing subsystem): per-stage device time from CUDA events recorded around every
  * stage launch on the renderer's stream, and per-ray traversal work counters. */
 #define XB_PROFILE_STAGE_TIMES     1

@@ -127,6 +127,7 @@ class RefScene:
         v = SceneView()
         if self.L.xr_scene_view(self.h, ctypes.byref(v)) != 0:
             raise RuntimeError("xr_scene_view failed")
+        v._owner = self
         return v
 
     def mesh_arrays(self, mesh: int, nv: int):

@@ -108,8 +108,10 @@ class HostScene:
         return s
 
     def view(self) -> abi.SceneView:
+        """The flattened arrays; they belong to this scene, which the view keeps alive."""
         v = abi.SceneView()
         check(lib().xb_scene_get_view(self.h, ctypes.byref(v)))
+        v._owner = self
         return v
 
 
@@ -177,6 +179,16 @@ class Renderer:
 
     def reset_stats(self) -> None:
         self._check(lib().xb_reset_render_stats(self.h))
+
+    def set_tuning(self, **kw) -> None:
+        """xb_set_tuning: fields of abi.Tuning; unnamed fields keep their value."""
+        t = abi.Tuning(**kw)
+        self._check(lib().xb_set_tuning(self.h, ctypes.byref(t)))
+
+    def tuning(self) -> dict:
+        t = abi.Tuning()
+        self._check(lib().xb_get_tuning(self.h, ctypes.byref(t)))
+        return t.as_dict()
 
     def set_profiling(self, flags: int) -> None:
         self._check(lib().xb_set_profiling(self.h, int(flags)))

@@ -149,6 +149,15 @@ class RenderStats(ctypes.Structure):
 XB_PROFILE_STAGE_TIMES, XB_PROFILE_COUNT_TRAVERSAL = 1, 2
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in ("extend_persistent_from_depth", "shadow_persistent", "refill",
+                                              "extend_blocks_per_sm", "shadow_blocks_per_sm",
+                                              "shade_blocks_per_sm", "wave_paths")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Profile(ctypes.Structure):
     _fields_ = [(k, ctypes.c_double) for k in ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms",
                                                "accumulate_ms")] + \

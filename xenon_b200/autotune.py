@@ -1,0 +1,126 @@
+"""Autotuner for the wavefront launch parameters (xb_tuning).
+
+For one scene and resolution it measures the device time per sample (CUDA events inside
+xb_render) while varying one parameter at a time around the current best (coordinate descent,
+two passes), and keeps the fastest setting:
+
+  extend_persistent_from_depth   which bounces trace closest hits with persistent warps
+  shadow_persistent              persistent warps or one ray per thread for shadow rays
+  refill                         idle lanes that trigger a warp refill
+  extend/shadow/shade_blocks_per_sm   resident blocks per SM (grid size)
+  wave_paths                     paths in flight per wave (queue capacity)
+
+Results are stored as JSON under xenon_b200/tuning/<gpu>/<workload>.json and loaded by
+load_tuning(); the renderer's image does not depend on any of these settings.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TUNING_DIR = os.path.join(HERE, "tuning")
+
+SPACE = {
+    "extend_persistent_from_depth": [0, 1, 2, 3, 64],
+    "shadow_persistent": [1, 2],
+    "refill": [2, 4, 8, 16, 24],
+    "extend_blocks_per_sm": [3, 4, 5, 6, 64],
+    "shadow_blocks_per_sm": [3, 4, 5, 6, 64],
+    "shade_blocks_per_sm": [2, 3, 4, 64],
+    "wave_paths": [1 << 20, 1 << 21, 1 << 22],
+}
+
+
+def gpu_name() -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(0).replace(" ", "_")
+    except Exception:
+        return "unknown_gpu"
+
+
+def tuning_path(workload: str, gpu: str | None = None) -> str:
+    return os.path.join(TUNING_DIR, gpu or gpu_name(), f"{workload}.json")
+
+
+def load_tuning(workload: str, gpu: str | None = None) -> dict | None:
+    p = tuning_path(workload, gpu)
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)["tuning"]
+    return None
+
+
+def measure(renderer, cam, spp: int, first: int) -> float:
+    """Device ms per sample over `spp` samples (after one warm-up sample)."""
+    renderer.render_range(cam, first, 1)
+    ms = 0.0
+    for k in range(spp):
+        renderer.render_range(cam, first + 1 + k, 1)
+        ms += renderer.stats().last_ms
+    return ms / spp
+
+
+def autotune(renderer, cam, workload: str, spp: int = 4, passes: int = 2, save: bool = True,
+             log=print) -> dict:
+    best = dict(renderer.tuning())
+    seq = [1000]
+
+    def run(t):
+        renderer.set_tuning(**t)
+        seq[0] += spp + 1
+        return measure(renderer, cam, spp, seq[0])
+
+    best_ms = run(best)
+    log(f"start {best_ms:.3f} ms/spp {best}")
+    for _ in range(passes):
+        for key, values in SPACE.items():
+            for v in values:
+                if best.get(key) == v:
+                    continue
+                cand = dict(best)
+                cand[key] = v
+                ms = run(cand)
+                if ms < best_ms * 0.995:
+                    best, best_ms = cand, ms
+                    log(f"  {key}={v}: {ms:.3f} ms/spp (new best)")
+    renderer.set_tuning(**best)
+    result = {"workload": workload, "gpu": gpu_name(), "ms_per_spp": best_ms, "tuning": best,
+              "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}
+    if save:
+        p = tuning_path(workload)
+        os.makedirs(os.path.dirname(p), exist_ok=True)
+        with open(p, "w") as f:
+            json.dump(result, f, indent=1)
+    return result
+
+
+if __name__ == "__main__":
+    import argparse
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    import xenon_b200 as xb
+    from xenon_b200 import scenes
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="config2")
+    ap.add_argument("--out", default=None, help="also write the result JSON here")
+    a = ap.parse_args()
+    if a.workload == "config2":
+        desc = scenes.icosphere_scene(level=8)
+    elif a.workload == "config1":
+        desc = scenes.cornell()
+    elif a.workload == "config4":
+        desc = scenes.guiding_room(level=8)
+    else:
+        desc = scenes.instanced_grid()
+    hs = xb.HostScene.from_desc(desc)
+    r = xb.Renderer(desc.width, desc.height, desc.max_bounces, desc.min_bounces)
+    r.upload_scene(hs)
+    cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
+    res = autotune(r, cam, a.workload)
+    print(json.dumps(res))
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(res, f, indent=1)

@@ -23,6 +23,7 @@ CXX_SRCS = ["scene_host.cpp", "loaders.cpp", "capi_scene.cpp"]
 CU_STRICT = ["renderer.cu"]
 CU_FAST: list[str] = []
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 
 def _nvcc() -> str:
@@ -62,7 +63,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILDDIR, src + ".o")
         if force or _stale(o, [s] + hdrs):
-            _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+            _run([CXX, "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
                   "-Wextra", "-I", INCLUDE, "-c", s, "-o", o])
         objs.append(o)
     for src, strict in [(s, True) for s in CU_STRICT] + [(s, False) for s in CU_FAST]:

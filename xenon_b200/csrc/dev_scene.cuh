@@ -114,6 +114,29 @@ struct TraversalCounters {
 
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
 
+// BLAS stack entries carry the node's own (child, count) — both already loaded with the
+// parent's 64 B child pair — so popping needs no further node load: count in the top 4 bits,
+// child (a node or triangle-slot index < 2^28) below. A count >= 15 (only degenerate leaves)
+// stores the node index instead, marked by 15, and the node is re-read when popped.
+constexpr uint32_t kEntryEscape = 15u;
+__device__ __forceinline__ uint32_t blas_entry(uint32_t child, uint32_t count, uint32_t node) {
+  return count < kEntryEscape ? ((count << 28) | child) : ((kEntryEscape << 28) | node);
+}
+__device__ __forceinline__ void blas_unpack(const DevScene& sc, uint32_t e, uint32_t& child,
+                                            uint32_t& count) {
+  count = e >> 28;
+  child = e & 0x0fffffffu;
+  if (count == kEntryEscape) {
+    const float4 nb = __ldg(sc.blas + 2 * (size_t)child + 1);
+    child = __float_as_uint(nb.z);
+    count = __float_as_uint(nb.w);
+  }
+}
+__device__ __forceinline__ uint32_t blas_root_entry(const DevScene& sc, int root) {
+  const float4 nb = __ldg(sc.blas + 2 * (size_t)root + 1);
+  return blas_entry(__float_as_uint(nb.z), __float_as_uint(nb.w), (uint32_t)root);
+}
+
 // ── world → local (AffineTransform::to_local, transform.h:44-51) ────────────────
 __device__ __forceinline__ Ray to_local(const DevInstance& in, const Ray& w) {
   const float* c = in.w2l;
@@ -303,12 +326,11 @@ __device__ __forceinline__ bool blas_closest(const DevScene& sc, int root, const
                                              TraversalCounters& cnt, bool& overflow) {
   const V3 inv = v3(1.f / r.d.x, 1.f / r.d.y, 1.f / r.d.z);
   int ptr = 0;
-  stack[ptr++] = (uint32_t)root;
+  stack[ptr++] = blas_root_entry(sc, root);
   bool hit = false;
   while (ptr > 0) {
-    const uint32_t idx = stack[--ptr];
-    const float4 nb = ldg4(sc.blas + 2 * idx + 1);
-    const uint32_t child = __float_as_uint(nb.z), count = __float_as_uint(nb.w);
+    uint32_t child, count;
+    blas_unpack(sc, stack[--ptr], child, count);
     if (count > 0) {
       for (uint32_t i = 0; i < count; ++i) {
         const float4* tp = sc.tris + 3 * (size_t)(child + i);
@@ -332,11 +354,13 @@ __device__ __forceinline__ bool blas_closest(const DevScene& sc, int root, const
     const bool hr = slab_sse(ra, rb, inv, r.o, r.tmin, h.t, tr);
     if (!hl && !hr) continue;
     if (ptr + 2 > kStackSize) { overflow = true; break; }
+    const uint32_t el = blas_entry(__float_as_uint(lb.z), __float_as_uint(lb.w), child);
+    const uint32_t er = blas_entry(__float_as_uint(rb.z), __float_as_uint(rb.w), child + 1);
     if (hl && hr) {
-      if (tl < tr) { stack[ptr++] = child + 1; stack[ptr++] = child; }
-      else { stack[ptr++] = child; stack[ptr++] = child + 1; }
+      if (tl < tr) { stack[ptr++] = er; stack[ptr++] = el; }
+      else { stack[ptr++] = el; stack[ptr++] = er; }
     } else {
-      stack[ptr++] = hl ? child : child + 1;
+      stack[ptr++] = hl ? el : er;
     }
   }
   return hit;
@@ -348,11 +372,10 @@ __device__ __forceinline__ bool blas_any(const DevScene& sc, int root, const Ray
                                          uint32_t* stack, TraversalCounters& cnt, bool& overflow) {
   const V3 inv = v3(1.f / r.d.x, 1.f / r.d.y, 1.f / r.d.z);
   int ptr = 0;
-  stack[ptr++] = (uint32_t)root;
+  stack[ptr++] = blas_root_entry(sc, root);
   while (ptr > 0) {
-    const uint32_t idx = stack[--ptr];
-    const float4 nb = ldg4(sc.blas + 2 * idx + 1);
-    const uint32_t child = __float_as_uint(nb.z), count = __float_as_uint(nb.w);
+    uint32_t child, count;
+    blas_unpack(sc, stack[--ptr], child, count);
     if (count > 0) {
       for (uint32_t i = 0; i < count; ++i) {
         const float4* tp = sc.tris + 3 * (size_t)(child + i);
@@ -370,8 +393,8 @@ __device__ __forceinline__ bool blas_any(const DevScene& sc, int root, const Ray
     const bool hl = slab_sse(la, lb, inv, r.o, r.tmin, r.tmax, tl);
     const bool hr = slab_sse(ra, rb, inv, r.o, r.tmin, r.tmax, tr);
     if (ptr + 2 > kStackSize) { overflow = true; return false; }
-    if (hr) stack[ptr++] = child + 1;
-    if (hl) stack[ptr++] = child;
+    if (hr) stack[ptr++] = blas_entry(__float_as_uint(rb.z), __float_as_uint(rb.w), child + 1);
+    if (hl) stack[ptr++] = blas_entry(__float_as_uint(lb.z), __float_as_uint(lb.w), child);
   }
   return false;
 }

@@ -118,6 +118,10 @@ struct xb_renderer {
   int grid_pext = 0, grid_pshadow = 0;
   bool thread_per_ray = false;   // XB_FLAG_THREAD_PER_RAY: one ray per thread traversal kernels
   int refill = 8;                // persistent traversal: refill a warp when this many lanes idle
+  int ext_persistent_from = 0;   // bounces >= this trace closest hits with persistent warps
+  bool shadow_persistent = true;
+  int occ_ext = 1, occ_pext = 1, occ_shadow = 1, occ_pshadow = 1, occ_shade = 1;  // limits
+  xb_tuning tune{};
   // profiling
   int prof_flags = 0;
   std::vector<cudaEvent_t> ev_pool;          // event pairs, reused each call
@@ -683,6 +687,34 @@ int check_ready(xb_renderer* r) {
   return XB_OK;
 }
 
+// Applies a tuning (0 keeps a field, negative restores its default) and recomputes grids.
+int apply_tuning(xb_renderer* r, const xb_tuning& t) {
+  xb_tuning& c = r->tune;
+  auto pick = [](int32_t v, int32_t cur, int32_t def) { return v == 0 ? cur : (v < 0 ? def : v); };
+  c.extend_persistent_from_depth = pick(t.extend_persistent_from_depth, c.extend_persistent_from_depth, 1);
+  c.shadow_persistent = pick(t.shadow_persistent, c.shadow_persistent, 1);
+  c.refill = std::min(32, pick(t.refill, c.refill, 8));
+  c.extend_blocks_per_sm = pick(t.extend_blocks_per_sm, c.extend_blocks_per_sm, 64);
+  c.shadow_blocks_per_sm = pick(t.shadow_blocks_per_sm, c.shadow_blocks_per_sm, 64);
+  c.shade_blocks_per_sm = pick(t.shade_blocks_per_sm, c.shade_blocks_per_sm, 64);
+  c.wave_paths = pick(t.wave_paths, c.wave_paths, 1 << 21);
+  r->ext_persistent_from = c.extend_persistent_from_depth;
+  r->shadow_persistent = c.shadow_persistent == 1;
+  r->refill = c.refill;
+  r->grid_ext = r->num_sms * std::min(r->occ_ext, c.extend_blocks_per_sm);
+  r->grid_pext = r->num_sms * std::min(r->occ_pext, c.extend_blocks_per_sm);
+  r->grid_shadow = r->num_sms * std::min(r->occ_shadow, c.shadow_blocks_per_sm);
+  r->grid_pshadow = r->num_sms * std::min(r->occ_pshadow, c.shadow_blocks_per_sm);
+  r->grid_shade = r->num_sms * std::min(r->occ_shade, c.shade_blocks_per_sm);
+  const int64_t npix = (int64_t)r->cfg.width * r->cfg.height;
+  const int spw = (int)std::min<int64_t>(1024, std::max<int64_t>(1, c.wave_paths / npix));
+  if (spw != r->spp_per_wave || r->wb.capacity == 0) {
+    r->spp_per_wave = spw;
+    return alloc_wave(r, npix * spw);
+  }
+  return XB_OK;
+}
+
 enum { STAGE_RAYGEN = 0, STAGE_EXTEND = 1, STAGE_SHADE = 2, STAGE_SHADOW = 3, STAGE_ACCUM = 4 };
 
 // Stage timing: a pair of events around a launch, read back after the call's final sync.
@@ -748,7 +780,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       int32_t* cd_ = w.cnt + d * kCntStride;
       {
         StageTimer t(r, STAGE_EXTEND);
-        if (r->thread_per_ray) {
+        if (r->thread_per_ray || d < r->ext_persistent_from) {
           auto kern = count ? extend_kernel<true> : extend_kernel<false>;
           kern<<<r->grid_ext, 128, 0, r->stream>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_,
                                                    r->stats);
@@ -780,7 +812,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
         if (k == 0 && r->scene.num_lights == 0) continue;
         if (k == 1 && r->scene.num_suns == 0) continue;
         StageTimer t(r, STAGE_SHADOW);
-        if (r->thread_per_ray) {
+        if (r->thread_per_ray || !r->shadow_persistent) {
           auto kern = count ? shadow_kernel<true> : shadow_kernel<false>;
           kern<<<r->grid_shadow, 128, 0, r->stream>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
                                                       cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
@@ -843,24 +875,27 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
         cudaMalloc(&r->mean64, npix * 3 * sizeof(double)) != cudaSuccess)
       return bail(xb::fail(XB_E_OOM, "FP64 accumulation allocation failed"));
   }
-  // Paths per wave: whole samples of every pixel, about 2^21 paths in flight by default.
-  int64_t target = cfg->wave_paths > 0 ? cfg->wave_paths : (int64_t)1 << 21;
-  r->spp_per_wave = (int)std::max<int64_t>(1, target / npix);
-  r->spp_per_wave = std::min(r->spp_per_wave, 1024);
-  int rc = alloc_wave(r, npix * r->spp_per_wave);
-  if (rc != XB_OK) return bail(rc);
+  int rc = XB_OK;
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_kernel<false>, 128, 0);
-  r->grid_ext = r->num_sms * std::max(occ, 1);
+  r->occ_ext = std::max(occ, 1);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_kernel<false>, 128, 0);
-  r->grid_shadow = r->num_sms * std::max(occ, 1);
+  r->occ_shadow = std::max(occ, 1);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel, 128, 0);
-  r->grid_shade = r->num_sms * std::max(occ, 1);
+  r->occ_shade = std::max(occ, 1);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_persistent_kernel<false>, 128, 0);
-  r->grid_pext = r->num_sms * std::max(occ, 1);
+  r->occ_pext = std::max(occ, 1);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_persistent_kernel<false>, 128, 0);
-  r->grid_pshadow = r->num_sms * std::max(occ, 1);
+  r->occ_pshadow = std::max(occ, 1);
   r->thread_per_ray = (cfg->flags & XB_FLAG_THREAD_PER_RAY) != 0;
+  {
+    // Paths per wave: whole samples of every pixel, about 2^21 paths in flight by default.
+    xb_tuning def;
+    std::memset(&def, 0xff, sizeof(def));   // every field negative: defaults
+    if (cfg->wave_paths > 0) def.wave_paths = cfg->wave_paths;
+    rc = apply_tuning(r, def);
+    if (rc != XB_OK) return bail(rc);
+  }
   rc = xb_reset(r);
   if (rc != XB_OK) return bail(rc);
   if (cudaMemset(r->stats, 0, STAT_COUNT * sizeof(unsigned long long)) != cudaSuccess)
@@ -962,6 +997,8 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
     tri_base += mv.num_triangles;
     vtx_base += mv.num_vertices;
   }
+  if (blas.size() / 2 >= (1u << 28) || slot_base >= (1 << 28))
+    return set_err(r, XB_E_UNSUPPORTED, "scene too large: more than 2^28 BLAS nodes or triangles");
   // ── analytic prims in PrimBLAS slot order ──
   std::vector<float4> pnodes, prims;
   for (int i = 0; i < v->num_prim_nodes; ++i) {
@@ -1156,6 +1193,21 @@ int xb_reset_render_stats(xb_renderer* r) {
   if (rc) return rc;
   CK(cudaMemsetAsync(r->stats, 0, STAT_COUNT * sizeof(unsigned long long), r->stream));
   CK(cudaStreamSynchronize(r->stream));
+  return XB_OK;
+}
+
+int xb_set_tuning(xb_renderer* r, const xb_tuning* t) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!t) return set_err(r, XB_E_INVALID, "xb_set_tuning: null tuning");
+  if (t->refill > 32 || t->shadow_persistent > 2) return set_err(r, XB_E_INVALID, "xb_set_tuning: bad value");
+  CK(cudaStreamSynchronize(r->stream));
+  return apply_tuning(r, *t);
+}
+
+int xb_get_tuning(const xb_renderer* r, xb_tuning* out) {
+  if (!r || !out) return xb::fail(XB_E_INVALID, "xb_get_tuning: null argument");
+  *out = r->tune;
   return XB_OK;
 }
 

@@ -93,9 +93,8 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
       if (want) {
         if (bsp > 0) {
           // BLAS node (blas.cpp:222-263)
-          const uint32_t idx = bstack[--bsp];
-          const float4 nb = ldg4(sc.blas + 2 * idx + 1);
-          const uint32_t child = __float_as_uint(nb.z), count = __float_as_uint(nb.w);
+          uint32_t child, count;
+          blas_unpack(sc, bstack[--bsp], child, count);
           if (count > 0) {
             leaf_child = child;
             leaf_count = count;
@@ -112,12 +111,16 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
               if (bsp + 2 > kStackSize) {
                 overflow = true;
                 bsp = 0; tsp = 0; tl_count = 0;   // abandon the ray (reported as overflow)
-              } else if (hl && hr) {
-                // closest: the reference order (nearer tn on top); any: same rule
-                if (tl < tr) { bstack[bsp++] = child + 1; bstack[bsp++] = child; }
-                else { bstack[bsp++] = child; bstack[bsp++] = child + 1; }
               } else {
-                bstack[bsp++] = hl ? child : child + 1;
+                const uint32_t el = blas_entry(__float_as_uint(lb.z), __float_as_uint(lb.w), child);
+                const uint32_t er = blas_entry(__float_as_uint(rb.z), __float_as_uint(rb.w), child + 1);
+                if (hl && hr) {
+                  // closest: the reference order (nearer tn on top); any: the same rule
+                  if (tl < tr) { bstack[bsp++] = er; bstack[bsp++] = el; }
+                  else { bstack[bsp++] = el; bstack[bsp++] = er; }
+                } else {
+                  bstack[bsp++] = hl ? el : er;
+                }
               }
             }
           }
@@ -133,7 +136,7 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
             lo = lr.o; ld = lr.d;
             linv = v3(1.f / ld.x, 1.f / ld.y, 1.f / ld.z);
             cur_inst = ii;
-            bstack[bsp++] = (uint32_t)in.root;
+            bstack[bsp++] = blas_root_entry(sc, in.root);
           } else {
             // analytic prims: a short scalar walk, done in place
             if (kAny) {
