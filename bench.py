@@ -155,6 +155,24 @@ def barrier(ws: int):
         dist.barrier()
 
 
+class quiet_stdout:
+    """Silences file descriptor 1 (the reference's C++ printf) so that stdout carries only the
+    JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 def cpu_reference_sample(desc, rays_per_path: float | None, budget_s: float, threads_note: bool = True) -> dict:
     """The reference CPU backend on a bounded sample of the same view (fewer pixels, same camera)."""
     from oracle import ref
@@ -188,16 +206,21 @@ def rays_per_path_port(desc, paths: int = 4096) -> float:
 
 def run_reference(args):
     """--impl reference: the reference's own CPU implementation of the path, host threads."""
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    with quiet_stdout():
+        line = reference_line(args)
+    print(json.dumps(line))
+    return 0
+
+
+def reference_line(args) -> dict:
     from oracle import ref
     from xenon_b200 import scenes
     desc = scenes.icosphere_scene(level=args.level, width=args.width, height=args.height)
     if not ref.available("fast"):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libxnref_fast.so was not built"}))
-        return 0
+        return {"impl": "reference", "unavailable": "oracle/_ref/libxnref_fast.so was not built"}
     try:
         rpp = rays_per_path_port(desc)
     except Exception as e:  # the restatement is missing: report samples only
@@ -227,8 +250,7 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "reference",
                              "sample": f"{w}x{h} px x {spp_per_step} spp per step, render_frame_tiled, Release flags, {cores} threads"},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def main():
@@ -353,7 +375,8 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference_sample(desc, rays_per_path, args.cpu_seconds)
+            with quiet_stdout():
+                cpu = cpu_reference_sample(desc, rays_per_path, args.cpu_seconds)
         except Exception as e:
             cpu = {"value": None, "unit": "Mrays/s", "cores": None, "kind": "reference",
                    "sample": f"failed: {e}"}
