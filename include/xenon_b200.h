@@ -330,6 +330,18 @@ int  xb_trace_rays(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit *hits, 
 int  xb_trace_rays_device(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit *hits,
                           int32_t mode, void *stream);
 
+/* Same as xb_trace_rays_device, but the call allocates nothing (no cudaMalloc, cudaFree or
+ * allocating library routine): for callers that cannot allocate device memory while they trace,
+ * e.g. code running while a stream is captured into a CUDA graph, or a plugin whose host
+ * application owns all device memory. Its scratch (ray cursor, count, overflow counter) is a
+ * fixed 256-byte device array inside the library, shared by every call: calls that overlap on
+ * the GPU race on it, so issue them on one stream or otherwise one at a time. The first call on a
+ * device looks up that array's address (cudaGetSymbolAddress, once per device, with the device
+ * current); make that first call before any stream capture. Batches above 2^31 - 65 rays are
+ * rejected with XB_E_INVALID. It has no counterpart in the reference. */
+int  xb_trace_rays_noalloc(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit *hits,
+                           int32_t mode, void *stream);
+
 /* BSDF on the device, host buffers: wo, wi float[n*3] in the shading frame (z = normal). */
 int  xb_bsdf_eval(const xb_material *m, int64_t n, const float *wo, const float *wi,
                   float *f_rgb, float *pdf);

@@ -1,0 +1,68 @@
+"""xb_trace_rays_noalloc: tracing for callers that cannot allocate device memory (code running
+while a stream is captured into a CUDA graph, or a plugin whose host owns all device memory).
+
+The entry point must give exactly the hit records of xb_trace_rays_device, on two calls in a
+row (its scratch is a fixed array shared by all calls, cleared at the start of each), and
+must leave the device's free memory unchanged. This file is collected last on purpose."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import xenon_b200 as xb
+from xenon_b200 import HostScene, Renderer, abi, scenes
+
+
+def _device_bytes(torch, arr: np.ndarray):
+    t = torch.empty(arr.nbytes, dtype=torch.uint8, device="cuda")
+    t.copy_(torch.from_numpy(arr.view(np.uint8).reshape(-1)))
+    return t
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [abi.XB_TRACE_CLOSEST, abi.XB_TRACE_ANY])
+def test_noalloc_trace_matches_trace_device(mode):
+    import torch
+    desc = scenes.instanced_grid(grid=3, levels=(3, 3, 4, 4), with_prims=True)
+    r = Renderer(16, 16)
+    r.upload_scene(HostScene.from_desc(desc))
+    lo, hi = scenes.scene_bounds(desc)
+    rays = scenes.random_rays((lo, hi), 50_000, seed=21)
+    n = len(rays)
+    d_rays = _device_bytes(torch, rays)
+    d_ref = torch.zeros(n * abi.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    d_a = torch.zeros_like(d_ref)
+    d_b = torch.zeros_like(d_ref)
+    stream = torch.cuda.current_stream().cuda_stream
+    L = xb.lib()
+    xb.native.check(L.xb_trace_rays_device(r.h, ctypes.c_void_p(d_rays.data_ptr()), n,
+                                           ctypes.c_void_p(d_ref.data_ptr()), mode, ctypes.c_void_p(stream)), r.h)
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for out in (d_a, d_b):     # two calls in a row share the scratch array
+        xb.native.check(L.xb_trace_rays_noalloc(r.h, ctypes.c_void_p(d_rays.data_ptr()), n,
+                                                ctypes.c_void_p(out.data_ptr()), mode, ctypes.c_void_p(stream)), r.h)
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    want = d_ref.cpu().numpy().view(abi.HIT_DTYPE)
+    for out in (d_a, d_b):
+        got = out.cpu().numpy().view(abi.HIT_DTYPE)
+        assert np.array_equal(got["prim_id"], want["prim_id"])
+        assert np.array_equal(got["instance_id"], want["instance_id"])
+        assert got.tobytes() == want.tobytes()
+    assert np.isfinite(want["t"]).sum() > n // 10
+    assert free_after == free_before
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_bad_requests():
+    desc = scenes.cornell()
+    r = Renderer(16, 16)
+    L = xb.lib()
+    # no scene yet
+    assert L.xb_trace_rays_noalloc(r.h, None, 0, None, 0, None) == abi.XB_E_STATE
+    r.upload_scene(HostScene.from_desc(desc))
+    assert L.xb_trace_rays_noalloc(r.h, ctypes.c_void_p(16), 1 << 31, ctypes.c_void_p(16), 0, None) == abi.XB_E_INVALID
+    assert "maximum batch" in xb.native.last_error(r.h)
+    assert L.xb_trace_rays_noalloc(r.h, ctypes.c_void_p(16), 4, ctypes.c_void_p(16), 7, None) == abi.XB_E_INVALID
+    assert L.xb_trace_rays_noalloc(r.h, None, 0, None, 0, None) == abi.XB_OK

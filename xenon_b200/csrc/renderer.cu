@@ -26,6 +26,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -598,6 +599,67 @@ __global__ void bsdf_sample_kernel(DevMaterial m, int64_t n, const float* wo, ui
     pdf[i] = s.pdf;
     flags[i] = (ok ? 1 : 0) | (s.delta ? 2 : 0);
   }
+}
+
+// ── trace without allocation (xb_trace_rays_noalloc) ─────────────────────────────
+// Some callers cannot call cudaMalloc while they trace: code that runs while a stream is being
+// captured into a CUDA graph, or a plugin whose host application owns every device allocation.
+// For them the work-stealing trace keeps its scratch (the ray cursor, the ray count and an
+// overflow counter) in this fixed file-scope array instead of renderer-allocated memory. It is
+// 256 bytes; every GPU that loads the library holds one copy until the process exits.
+constexpr int kNoAllocScratchWords = 32;
+constexpr int64_t kNoAllocMaxRays = (int64_t)0x7fffffff - 64;   // the cursor is a 32-bit int
+static __device__ __align__(256) int32_t g_noalloc_scratch[2 * kNoAllocScratchWords];
+
+__global__ void noalloc_begin_kernel(int32_t* scratch, int32_t n) {
+  // every call starts from a cleared cursor and counters: the array keeps the last call's values
+  if (threadIdx.x < 2 * kNoAllocScratchWords) scratch[threadIdx.x] = 0;
+  if (threadIdx.x == 0) scratch[1] = n;
+}
+
+// Work-stealing variant of trace_full_kernel: warps take 32 rays at a time from the cursor
+// in scratch[0] (count in scratch[1], stack overflows counted in scratch[2]).
+__global__ void __launch_bounds__(128) trace_stealing_kernel(DevScene sc, const xb_ray* rays,
+                                                             xb_hit* hits, int mode, int32_t* scratch) {
+  __shared__ int s_base[4];
+  const int n = scratch[1];
+  uint32_t tstack[kStackSize];
+  uint32_t bstack[kStackSize];
+  bool overflow = false;
+  TraversalCounters tc{0, 0, 0, 0};
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (;;) {
+    if (lane == 0) s_base[warp] = atomicAdd(scratch, 32);
+    __syncwarp();
+    const int base = s_base[warp];
+    __syncwarp();
+    if (base >= n) break;
+    const int i = base + lane;
+    if (i >= n) continue;
+    const xb_ray rr = rays[i];
+    Ray r{v3(rr.org[0], rr.org[1], rr.org[2]), v3(rr.dir[0], rr.dir[1], rr.dir[2]), rr.tmin, rr.tmax};
+    xb_hit out;
+    memset(&out, 0, sizeof(out));
+    out.t = kInf; out.prim_id = -1; out.instance_id = -1; out.mat_id = -1;
+    if (mode == XB_TRACE_CLOSEST) {
+      HitState h;
+      if (scene_closest<false>(sc, r, h, tstack, bstack, tc, overflow)) {
+        FullHit f;
+        complete_hit(sc, r, h, f);
+        out.t = h.t; out.u = f.u; out.v = f.v;
+        out.prim_id = f.prim_id; out.instance_id = f.instance_id; out.mat_id = f.mat_id;
+        out.front_face = f.front_face ? 1 : 0;
+        out.pos[0] = f.pos.x; out.pos[1] = f.pos.y; out.pos[2] = f.pos.z;
+        out.normal[0] = f.normal.x; out.normal[1] = f.normal.y; out.normal[2] = f.normal.z;
+        out.geo_normal[0] = f.geo_normal.x; out.geo_normal[1] = f.geo_normal.y;
+        out.geo_normal[2] = f.geo_normal.z;
+      }
+    } else if (scene_any<false>(sc, r, tstack, bstack, tc, overflow)) {
+      out.t = 0.f;
+    }
+    hits[i] = out;
+  }
+  if (overflow) atomicAdd(scratch + 2, 1);
 }
 
 DevMaterial to_dev_material(const xb_material& m) {
@@ -1264,6 +1326,44 @@ int xb_trace_rays_device(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit* 
   cudaStream_t s = stream ? (cudaStream_t)stream : r->stream;
   const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)r->num_sms * 16);
   trace_full_kernel<<<grid, 128, 0, s>>>(r->scene, rays, n, hits, mode, r->stats);
+  CK(cudaGetLastError());
+  return XB_OK;
+}
+
+// Device address of g_noalloc_scratch, looked up once per device (with that device current)
+// by the first call made on it; cudaGetSymbolAddress allocates nothing.
+static std::mutex g_noalloc_mu;
+static int32_t* g_noalloc_ptr[128] = {};
+
+int xb_trace_rays_noalloc(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit* hits, int32_t mode,
+                          void* stream) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!r->has_scene) return set_err(r, XB_E_STATE, "xb_trace_rays_noalloc: no scene uploaded");
+  if (n < 0 || (n > 0 && (!rays || !hits))) return set_err(r, XB_E_INVALID, "xb_trace_rays_noalloc: bad arguments");
+  if (n > kNoAllocMaxRays)
+    return set_err(r, XB_E_INVALID, "xb_trace_rays_noalloc: %lld rays exceed the maximum batch of %lld",
+                   (long long)n, (long long)kNoAllocMaxRays);
+  if (mode != XB_TRACE_CLOSEST && mode != XB_TRACE_ANY) return set_err(r, XB_E_INVALID, "bad trace mode %d", mode);
+  if (n == 0) return XB_OK;
+  const int dev = r->cfg.device;
+  if (dev < 0 || dev >= 128) return set_err(r, XB_E_UNSUPPORTED, "xb_trace_rays_noalloc: device %d", dev);
+  int32_t* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+        return set_err(r, XB_E_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s", cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = static_cast<int32_t*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  cudaStream_t s = stream ? (cudaStream_t)stream : r->stream;
+  noalloc_begin_kernel<<<1, 2 * kNoAllocScratchWords, 0, s>>>(scratch, (int32_t)n);
+  const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)r->num_sms * r->occ_ext);
+  trace_stealing_kernel<<<grid, 128, 0, s>>>(r->scene, rays, hits, mode, scratch);
   CK(cudaGetLastError());
   return XB_OK;
 }

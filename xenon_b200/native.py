@@ -51,6 +51,7 @@ SIGNATURES = {
     "xb_reset_render_stats": ([_P], _I),
     "xb_trace_rays": ([_P, _P, _I64, _P, _I32], _I),
     "xb_trace_rays_device": ([_P, _P, _I64, _P, _I32, _P], _I),
+    "xb_trace_rays_noalloc": ([_P, _P, _I64, _P, _I32, _P], _I),
     "xb_set_tuning": ([_P, _P], _I),
     "xb_get_tuning": ([_P, _P], _I),
     "xb_set_profiling": ([_P, _I32], _I),
