@@ -302,6 +302,8 @@ typedef struct xb_tuning {
   int32_t shadow_blocks_per_sm;         /* kernels; bounded by the kernel's occupancy limit */
   int32_t shade_blocks_per_sm;
   int32_t wave_paths;                   /* paths in flight per wave (reallocates queues) */
+  int32_t shadow_order;                 /* shadow rays: 1 nearer child first, 2 farther first
+                                           (the occlusion answer does not depend on it) */
 } xb_tuning;
 int  xb_set_tuning(xb_renderer *r, const xb_tuning *t);
 int  xb_get_tuning(const xb_renderer *r, xb_tuning *out);

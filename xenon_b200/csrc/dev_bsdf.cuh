@@ -115,22 +115,16 @@ __device__ __forceinline__ float vndf_pdf(V3 wo, V3 wh, float ax, float ay) {
   return d * g1 * smax(0.f, dot(wo, wh)) / co;
 }
 
-// Multiple-scattering compensation (bsdf.h:212-249)
-__device__ __forceinline__ float ggx_dir_albedo(float c, float a) {
-  float e = 1.0f - powf(1.0f - c, 5.0f * expf(-2.69f * a)) / (1.0f + 22.7f * powf(a, 1.5f));
+// Multiple-scattering compensation (bsdf.h:212-249). The direction-free terms (5 exp(-2.69 a),
+// 1 + 22.7 a^1.5 and F_avg^2 E_avg / denom) are per-material constants computed on the host.
+__device__ __forceinline__ float ggx_dir_albedo(float c, float k1, float k2) {
+  float e = 1.0f - powf(1.0f - c, k1) / k2;
   return sclamp(e, 0.f, 1.f);
 }
-__device__ __forceinline__ float ggx_avg_albedo(float a) {
-  return 1.0f / (1.0f + 0.3037f * a + 0.1218f * a * a);
-}
-__device__ __forceinline__ V3 multiscatter(V3 f0, float co, float ci, float alpha) {
-  float eo = ggx_dir_albedo(fabsf(co), alpha);
-  float ei = ggx_dir_albedo(fabsf(ci), alpha);
-  float eavg = ggx_avg_albedo(alpha);
-  V3 favg = (v3s(1.f) + f0 * 20.f) * (1.f / 21.f);
-  float denom = 1.f - favg.x * (1.f - eavg);
-  denom = smax(denom, 1e-4f);
-  V3 fms = favg * favg * eavg / v3s(denom);
+__device__ __forceinline__ V3 multiscatter(const DevMaterial& m, float co, float ci) {
+  float eo = ggx_dir_albedo(fabsf(co), m.ms_k1, m.ms_k2);
+  float ei = ggx_dir_albedo(fabsf(ci), m.ms_k1, m.ms_k2);
+  V3 fms = v3(m.ms_fms[0], m.ms_fms[1], m.ms_fms[2]);
   float comp_ = (1.f - eo) * (1.f - ei);
   return v3s(1.f) + fms * comp_ / v3s(smax(eo * ei, 1e-4f));
 }
@@ -163,7 +157,7 @@ __device__ __forceinline__ V3 mfr_eval(V3 wo, V3 wi, const DevMaterial& m) {
   float denom = 4.f * wo.z * wi.z;
   if (denom < 1e-8f) return v3s(0.f);
   V3 res = f * d * g / denom;
-  if (!(m.flags & kMatTransmissive)) res = res * multiscatter(mat_f0(m), wo.z, wi.z, m.alpha);
+  if (!(m.flags & kMatTransmissive)) res = res * multiscatter(m, wo.z, wi.z);
   return res;
 }
 __device__ __forceinline__ float mfr_pdf(V3 wo, V3 wi, const DevMaterial& m) {

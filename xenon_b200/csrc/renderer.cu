@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(128) shadow_kernel(DevScene sc, const float4* 
                                                      const float4* __restrict__ sd,
                                                      const float4* __restrict__ scn, float4* L,
                                                      const int32_t* count, int32_t* fetch,
-                                                     unsigned long long* stats) {
+                                                     unsigned long long* stats, int far_first) {
   __shared__ int s_base[4];
   const int n = *count;
   uint32_t tstack[kStackSize];
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(128) shadow_kernel(DevScene sc, const float4* 
     if (i < n) {
       const float4 o = so[i], d = sd[i];
       Ray r{v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), kShadowEps, o.w};
-      if (!scene_any<kCount>(sc, r, tstack, bstack, tc, overflow)) {
+      if (!scene_any<kCount>(sc, r, tstack, bstack, tc, overflow, far_first != 0)) {
         const float4 c = scn[i];
         const int p = __float_as_int(d.w);
         float4 l = L[p];
@@ -675,6 +675,7 @@ DevMaterial to_dev_material(const xb_material& m) {
   o.alpha = d.alpha; o.alpha_x = d.alpha_x; o.alpha_y = d.alpha_y;
   o.subsurface = m.subsurface;
   o.flags = d.flags;
+  xb::multiscatter_constants(d, &o.ms_k1, &o.ms_k2, o.ms_fms);
   return o;
 }
 
@@ -760,6 +761,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.shadow_blocks_per_sm = pick(t.shadow_blocks_per_sm, c.shadow_blocks_per_sm, 64);
   c.shade_blocks_per_sm = pick(t.shade_blocks_per_sm, c.shade_blocks_per_sm, 64);
   c.wave_paths = pick(t.wave_paths, c.wave_paths, 1 << 21);
+  c.shadow_order = pick(t.shadow_order, c.shadow_order, 1);
   r->ext_persistent_from = c.extend_persistent_from_depth;
   r->shadow_persistent = c.shadow_persistent == 1;
   r->refill = c.refill;
@@ -848,7 +850,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
                                                    r->stats);
         } else {
           TraceQueue tq{w.ray_o[q], w.ray_d[q], cd_ + CNT_RAYS, cd_ + CNT_FETCH_EXT, w.hit, w.hit_inst,
-                        nullptr, nullptr, r->stats};
+                        nullptr, nullptr, r->stats, 0};
           auto kern = count ? extend_persistent_kernel<true> : extend_persistent_kernel<false>;
           kern<<<r->grid_pext, 128, 0, r->stream>>>(r->scene, tq, r->refill);
         }
@@ -878,11 +880,12 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
           auto kern = count ? shadow_kernel<true> : shadow_kernel<false>;
           kern<<<r->grid_shadow, 128, 0, r->stream>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
                                                       cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
-                                                      cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats);
+                                                      cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats,
+                                                      r->tune.shadow_order == 2);
         } else {
           TraceQueue tq{w.sh_o[k], w.sh_d[k], cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
                         cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), nullptr, nullptr, w.sh_c[k], w.L,
-                        r->stats};
+                        r->stats, r->tune.shadow_order == 2};
           auto kern = count ? shadow_persistent_kernel<true> : shadow_persistent_kernel<false>;
           kern<<<r->grid_pshadow, 128, 0, r->stream>>>(r->scene, tq, r->refill);
         }
@@ -1262,7 +1265,8 @@ int xb_set_tuning(xb_renderer* r, const xb_tuning* t) {
   int rc = check_ready(r);
   if (rc) return rc;
   if (!t) return set_err(r, XB_E_INVALID, "xb_set_tuning: null tuning");
-  if (t->refill > 32 || t->shadow_persistent > 2) return set_err(r, XB_E_INVALID, "xb_set_tuning: bad value");
+  if (t->refill > 32 || t->shadow_persistent > 2 || t->shadow_order > 2)
+    return set_err(r, XB_E_INVALID, "xb_set_tuning: bad value");
   CK(cudaStreamSynchronize(r->stream));
   return apply_tuning(r, *t);
 }

@@ -430,6 +430,20 @@ bool light_geometry(const xb_scene_view& v, const xb_light& l, LightGeom* out) {
   return true;
 }
 
+void multiscatter_constants(const xb_material_derived& d, float* k1, float* k2, float fms[3]) {
+  const float a = d.alpha;
+  *k1 = 5.0f * std::exp(-2.69f * a);
+  *k2 = 1.0f + 22.7f * std::pow(a, 1.5f);
+  const float eavg = 1.0f / (1.0f + 0.3037f * a + 0.1218f * a * a);
+  const F3 f0(d.f0[0], d.f0[1], d.f0[2]);
+  const F3 favg = (F3::splat(1.f) + f0 * 20.f) * (1.f / 21.f);
+  float denom = 1.f - favg.x * (1.f - eavg);
+  denom = std::max(denom, 1e-4f);
+  // F_avg * F_avg * E_avg / Vec3(denom): component products, then component division
+  const F3 t = F3(favg.x * favg.x, favg.y * favg.y, favg.z * favg.z) * eavg;
+  fms[0] = t.x / denom; fms[1] = t.y / denom; fms[2] = t.z / denom;
+}
+
 void sun_emission(const xb_sun& s, float out[3]) {
   F3 e = F3(s.color[0], s.color[1], s.color[2]) * s.intensity;
   out[0] = e.x; out[1] = e.y; out[2] = e.z;

@@ -76,5 +76,9 @@ struct LightGeom {
   float p0[3], p1[3], p2[3], n[3];
 };
 bool light_geometry(const xb_scene_view& v, const xb_light& l, LightGeom* out);
+// Per-material terms of the multiple-scattering factor (src/material/bsdf.h:212-249) that do not
+// depend on directions: k1 = 5 exp(-2.69 a), k2 = 1 + 22.7 a^1.5 and F_ms = F_avg^2 E_avg / denom,
+// computed once with the host libm the reference itself uses.
+void multiscatter_constants(const xb_material_derived& d, float* k1, float* k2, float fms[3]);
 void sun_emission(const xb_sun& s, float out[3]);
 }  // namespace xb

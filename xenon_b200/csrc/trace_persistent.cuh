@@ -32,6 +32,7 @@ struct TraceQueue {
   const float4* contrib;
   float4* L;
   unsigned long long* stats;
+  int far_first;            // any-hit: descend into the farther child first
 };
 
 template <bool kAny, bool kCount>
@@ -52,6 +53,8 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
   int sign0 = 0, sign1 = 0, sign2 = 0;
   V3 lo = v3s(0.f), ld = v3s(0.f), linv = v3s(0.f);
   int tsp = 0, bsp = 0;
+  uint32_t bcur = 0;              // BLAS node being expanded (a stack entry), valid if bactive
+  bool bactive = false;
   int cur_inst = -1;              // instance being traversed (-1: at TLAS level)
   uint32_t tl_child = 0, tl_count = 0, tl_i = 0;   // instances of the current TLAS leaf
   uint32_t leaf_child = 0, leaf_count = 0;         // pending BLAS leaf
@@ -78,7 +81,7 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
           else { tmin = o.w; tmax = d.w; }
           winv = v3(1.f / wd.x, 1.f / wd.y, 1.f / wd.z);
           sign0 = wd.x < 0.f; sign1 = wd.y < 0.f; sign2 = wd.z < 0.f;
-          tsp = 0; bsp = 0; cur_inst = -1; tl_count = 0; tl_i = 0; leaf_count = 0;
+          tsp = 0; bsp = 0; bactive = false; cur_inst = -1; tl_count = 0; tl_i = 0; leaf_count = 0;
           h = HitState{kInf, 0.f, 0.f, -1, -1};
           occluded = false;
           if (sc.num_tlas_nodes > 0) tstack[tsp++] = 0;
@@ -91,13 +94,14 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
     bool want = (ray >= 0);
     while (__any_sync(FULL, want)) {
       if (want) {
-        if (bsp > 0) {
-          // BLAS node (blas.cpp:222-263)
+        if (bactive) {
+          // BLAS node (blas.cpp:222-263): the near child continues in bcur, the far one is pushed
           uint32_t child, count;
-          blas_unpack(sc, bstack[--bsp], child, count);
+          blas_unpack(sc, bcur, child, count);
           if (count > 0) {
             leaf_child = child;
             leaf_count = count;
+            bactive = false;      // the next entry is popped after the leaf's triangles
             want = false;
           } else {
             if (kCount) cnt.nodes++;
@@ -107,21 +111,23 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
             const float tcull = kAny ? tmax : h.t;
             const bool hl = slab_sse(la, lb, linv, lo, tmin, tcull, tl);
             const bool hr = slab_sse(ra, rb, linv, lo, tmin, tcull, tr);
-            if (hl || hr) {
-              if (bsp + 2 > kStackSize) {
+            const uint32_t el = blas_entry(__float_as_uint(lb.z), __float_as_uint(lb.w), child);
+            const uint32_t er = blas_entry(__float_as_uint(rb.z), __float_as_uint(rb.w), child + 1);
+            if (hl && hr) {
+              if (bsp + 1 > kStackSize) {
                 overflow = true;
-                bsp = 0; tsp = 0; tl_count = 0;   // abandon the ray (reported as overflow)
+                bactive = false; bsp = 0; tsp = 0; tl_count = 0;   // abandon (reported as overflow)
+              } else if ((tl < tr) != (kAny && q.far_first)) {
+                bstack[bsp++] = er; bcur = el;
               } else {
-                const uint32_t el = blas_entry(__float_as_uint(lb.z), __float_as_uint(lb.w), child);
-                const uint32_t er = blas_entry(__float_as_uint(rb.z), __float_as_uint(rb.w), child + 1);
-                if (hl && hr) {
-                  // closest: the reference order (nearer tn on top); any: the same rule
-                  if (tl < tr) { bstack[bsp++] = er; bstack[bsp++] = el; }
-                  else { bstack[bsp++] = el; bstack[bsp++] = er; }
-                } else {
-                  bstack[bsp++] = hl ? el : er;
-                }
+                bstack[bsp++] = el; bcur = er;
               }
+            } else if (hl || hr) {
+              bcur = hl ? el : er;
+            } else if (bsp > 0) {
+              bcur = bstack[--bsp];
+            } else {
+              bactive = false;
             }
           }
         } else if (tl_i < tl_count) {
@@ -136,11 +142,12 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
             lo = lr.o; ld = lr.d;
             linv = v3(1.f / ld.x, 1.f / ld.y, 1.f / ld.z);
             cur_inst = ii;
-            bstack[bsp++] = blas_root_entry(sc, in.root);
+            bcur = blas_root_entry(sc, in.root);
+            bactive = true;
           } else {
             // analytic prims: a short scalar walk, done in place
             if (kAny) {
-              if (pblas_any(sc, lr, bstack, overflow)) { occluded = true; bsp = 0; tsp = 0; tl_count = 0; }
+              if (pblas_any(sc, lr, bstack, overflow)) { occluded = true; bsp = 0; bactive = false; tsp = 0; tl_count = 0; }
             } else {
               pblas_closest(sc, lr, h, ii, bstack, overflow);
             }
@@ -215,7 +222,12 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
         }
       }
       leaf_count = 0;
-      if (kAny && occluded) { bsp = 0; tsp = 0; tl_count = 0; }
+      if (kAny && occluded) {
+        bsp = 0; tsp = 0; tl_count = 0;
+      } else if (bsp > 0) {
+        bcur = bstack[--bsp];
+        bactive = true;
+      }
     }
   }
   if (overflow) atomicAdd(q.stats + 3, 1ull);
