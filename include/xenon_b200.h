@@ -352,6 +352,14 @@ int  xb_bsdf_eval(const xb_material *m, int64_t n, const float *wo, const float 
 int  xb_bsdf_sample(const xb_material *m, int64_t n, const float *wo, uint64_t *rng_state,
                     float *wi, float *f_rgb, float *pdf, int32_t *flags);
 
+/* ── diagnostics ──────────────────────────────────────────────────────────── */
+
+/* D = A * B^T on the tensor cores (tcgen05, BF16 operands, FP32 accumulation in TMEM): the
+ * building block of the guiding network's layers, exposed so it can be checked on its own.
+ * A [rows x 64], B [n x 64] row-major bf16 bits, D [rows x n] f32; n in {16, 32, 48, 64}.
+ * Host buffers. No reference counterpart (the reference has no tensor-core code). */
+int  xb_tc_gemm_bf16(const uint16_t *A, const uint16_t *B, int64_t rows, int32_t n, float *D);
+
 #ifdef __cplusplus
 }
 #endif
