@@ -287,6 +287,7 @@ typedef struct xb_render_stats {
   int64_t paths;          /* paths started */
   int64_t overflow;       /* items dropped by a full queue or traversal stack (must be 0) */
   float   last_ms;        /* device time of the last xb_render / xb_render_range call */
+  int64_t nonfinite;      /* path samples with a NaN or infinite radiance (left out of the image) */
 } xb_render_stats;
 int  xb_get_render_stats(const xb_renderer *r, xb_render_stats *out);
 int  xb_reset_render_stats(xb_renderer *r);
@@ -318,6 +319,9 @@ typedef struct xb_profile {
   /* traversal work (XB_PROFILE_COUNT_TRAVERSAL): closest-hit (ext_*) and shadow (sh_*) rays */
   int64_t ext_blas_nodes, ext_tris, ext_tlas_nodes, ext_instances;
   int64_t sh_blas_nodes, sh_tris, sh_tlas_nodes, sh_instances;
+  /* guiding: record finalisation and network training after training waves */
+  double train_ms;
+  int64_t train_launches;
 } xb_profile;
 int  xb_set_profiling(xb_renderer *r, int32_t flags);
 int  xb_get_profile(const xb_renderer *r, xb_profile *out);
@@ -351,6 +355,73 @@ int  xb_bsdf_eval(const xb_material *m, int64_t n, const float *wo, const float 
  * bit1 = delta lobe. */
 int  xb_bsdf_sample(const xb_material *m, int64_t n, const float *wo, uint64_t *rng_state,
                     float *wi, float *f_rgb, float *pdf, int32_t *flags);
+
+/* ── learned path guiding (no reference counterpart: the reference has no learned part) ── */
+
+/* A small network maps a surface point (position in the scene bounds, shading normal, outgoing
+ * direction) to a mixture of 8 von Mises-Fisher lobes q over incoming directions. At every
+ * non-delta vertex seen from the front of its shading normal the next direction is drawn from
+ *     p(w) = guide_fraction * q(w) + (1 - guide_fraction) * p_bsdf(w)
+ * (p_bsdf: the density of bsdf_sample), the vertex keeps the lobe, f and pdf the plain sampler
+ * would have produced for w (so MIS weights, next-event estimation and Russian roulette are the
+ * plain tracer's), and the path's radiance is weighted by the product of p_bsdf(w) / p(w) over
+ * its guided vertices. The guided image therefore converges to the plain tracer's image for any
+ * network and any scene. The network is trained online, on the first train_spp samples per
+ * pixel, by Adam on the radiance-weighted negative log-likelihood of the sampled directions;
+ * the training samples are part of the image. BF16 tensor cores (tcgen05), FP32 accumulation
+ * and master weights. */
+typedef struct xb_guiding {
+  int32_t enabled;          /* 0: plain BSDF sampling (the reference's estimator) */
+  int32_t train_spp;        /* train on samples 1..train_spp of each pixel; default 64, -1 = never */
+  int32_t steps_per_spp;    /* Adam steps per training sample per pixel; default 32 */
+  int32_t batch;            /* records per Adam step (multiple of 128); default 16384 */
+  float learning_rate;      /* default 5e-3 */
+  float guide_fraction;     /* probability of sampling the network; default 0.5 */
+  int32_t max_records;      /* training records kept per wave; default 1 << 21 */
+  int32_t record_stride;    /* record the vertices of one path in this many; 0 = automatic */
+  uint64_t seed;            /* initial weights and batch windows */
+  float bounds_min[3];      /* box mapped to [0,1]^3 for the network's position input; */
+  float bounds_max[3];      /* an empty box selects the scene's bounds */
+} xb_guiding;
+
+/* Enables, disables or reconfigures guiding (0 fields take defaults). The first enabling, or a
+ * new seed or max_records, creates a freshly initialised network; otherwise the network is kept,
+ * across xb_reset too (samples 1..train_spp of every accumulation train it further). */
+int  xb_set_guiding(xb_renderer *r, const xb_guiding *g);
+int  xb_get_guiding(const xb_renderer *r, xb_guiding *out);
+
+typedef struct xb_guiding_stats {
+  int64_t adam_steps;       /* optimizer steps taken */
+  int64_t records;          /* training records collected */
+  int64_t records_dropped;  /* records beyond max_records */
+  float last_loss;          /* mean loss of the last step */
+  int32_t training;         /* 1 while spp < train_spp */
+} xb_guiding_stats;
+int  xb_get_guiding_stats(const xb_renderer *r, xb_guiding_stats *out);
+
+/* The network's parameters: XB_GUIDE_PARAMS floats, W0 b0 W1 b1 W2 b2 W3 b3 with every W
+ * row-major [out][in]; layers 64 -> 64 -> 64 -> 64 -> 48. */
+#define XB_GUIDE_PARAMS 15600
+int  xb_guide_get_params(xb_renderer *r, float *params);
+int  xb_guide_set_params(xb_renderer *r, const float *params);
+
+/* Standalone network calls on host buffers (parity tests and diagnostics).
+ *   feats: rows x 9 (position in [0,1]^3, normal, outgoing direction)
+ *   lobes: rows x 40, per lobe mean direction xyz, concentration kappa, weight
+ *   recs:  n x 20 training records: feats 9, direction 3, weight c, path, throughput 3, radiance 3
+ *          (the loss uses feats, direction and c). */
+int  xb_guide_init_params(uint64_t seed, float *params);
+int  xb_guide_forward(const float *params, const float *feats, int64_t rows, float *lobes);
+/* Loss sum(c * -log q(direction)) / sum(c) and its gradient with respect to the parameters. */
+int  xb_guide_loss_grad(const float *params, const float *recs, int64_t n, float *grad, float *loss);
+/* `steps` Adam steps (lr, beta 0.9 / 0.99, eps 1e-8) on batches of `batch` records (tiles of 128
+ * consecutive records at random starts; all records in order when n <= batch); params_out gets
+ * the result, losses[steps] (optional) each step's loss. */
+int  xb_guide_train(const float *params, const float *recs, int64_t n, int32_t steps, int32_t batch,
+                    float lr, uint64_t seed, float *params_out, float *losses);
+/* The device mixture pdf of one direction per row, and directions drawn from it by u (rows x 3). */
+int  xb_guide_mixture_pdf(const float *lobes, int64_t rows, const float *dirs, float *pdf);
+int  xb_guide_mixture_sample(const float *lobes, int64_t rows, const float *u, float *dirs, float *pdf);
 
 /* ── diagnostics ──────────────────────────────────────────────────────────── */
 

@@ -1,0 +1,117 @@
+"""Guided rendering (the learned proposal inside the wavefront bounce) against the plain tracer:
+the same converged image, lower variance once trained, and a plain path untouched by the feature.
+
+The room's glass sphere makes rare, very bright samples (delta lobes weighted F / cos): with it
+the per-pixel variance is dominated by a handful of pixels, so the image-wide mean comparison
+uses the room without the sphere, the room with it is compared through robust per-pixel
+statistics, and variance comparisons use the median over pixels."""
+import numpy as np
+import pytest
+
+import xenon_b200 as xb
+from xenon_b200 import scenes
+
+W, H = 96, 54
+
+
+def _room(sphere=True):
+    d = scenes.guiding_room(level=4, width=W, height=H)
+    if not sphere:
+        d.meshes = d.meshes[:-1]
+    sc = xb.HostScene.from_desc(d)
+    cam = xb.camera(d.eye, d.target, d.fov, W / H)
+    return d, sc, cam
+
+
+def _render(sc, cam, spp, guided, bounces=16, **kw):
+    r = xb.Renderer(W, H, max_bounces=bounces, min_bounces=3, fp64=True)
+    r.upload_scene(sc)
+    if guided:
+        r.set_guiding(True, **kw)
+    r.render_frame(cam, spp)
+    s, m2 = r.resolve_fp64()
+    stats = r.stats()
+    gst = r.guiding_stats() if guided else None
+    r.close()
+    return s / spp, m2 / max(spp - 1, 1), stats, gst
+
+
+def _agree(mp, vp, mg, vg, spp, heavy_tailed):
+    lg, lp = mg.mean(2), mp.mean(2)
+    z = (lg - lp) / (np.sqrt(vg.mean(2) / spp + vp.mean(2) / spp) + 1e-12)
+    if not heavy_tailed:
+        d = mg.sum() - mp.sum()
+        se = np.sqrt(vg.sum() / spp + vp.sum() / spp)
+        assert abs(d) < 4.5 * se, (mg.mean(), mp.mean(), d / se)
+        assert np.mean(np.abs(z) > 4) < 0.002
+    else:
+        # a few pixels see rare, very bright samples (sample variances there are unreliable):
+        # the bulk of the per-pixel differences must still be centred and of unit scale
+        assert np.mean(np.abs(z) > 4) < 0.02, np.mean(np.abs(z) > 4)
+        assert abs(np.median(z)) < 0.1, np.median(z)
+        assert 0.8 < np.median(np.abs(z)) / 0.6745 < 1.25, np.median(np.abs(z)) / 0.6745
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sphere,bounces", [(False, 16), (True, 2), (True, 16)])
+def test_guided_converges_to_the_plain_image(sphere, bounces):
+    _, sc, cam = _room(sphere)
+    spp = 2048
+    mp, vp, stp, _ = _render(sc, cam, spp, False, bounces)
+    for kw in (dict(train_spp=-1), dict(train_spp=64, steps_per_spp=8, batch=4096)):
+        mg, vg, stg, gst = _render(sc, cam, spp, True, bounces, **kw)
+        assert stp.nonfinite == 0 and stg.nonfinite == 0
+        if kw["train_spp"] > 0:
+            assert gst["adam_steps"] == 64 * 8 and gst["records"] > 0 and np.isfinite(gst["last_loss"])
+        _agree(mp, vp, mg, vg, spp, heavy_tailed=sphere)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sphere", [False, True])
+def test_guided_training_lowers_the_variance(sphere):
+    """Equal sample count after training: the light sits above a baffle, so most of the room is
+    lit indirectly; the learned proposal must lower the typical per-pixel variance."""
+    _, sc, cam = _room(sphere)
+    spp = 512
+    _, vp, _, _ = _render(sc, cam, spp, False)
+    _, vg, _, gst = _render(sc, cam, spp, True, train_spp=64, steps_per_spp=16, batch=8192)
+    ratio = np.median(vg.mean(2) / (vp.mean(2) + 1e-12))
+    assert ratio < 0.8, (ratio, gst)
+
+
+@pytest.mark.gpu
+def test_guiding_off_leaves_the_plain_path_bit_exact():
+    _, sc, cam = _room()
+    a = xb.Renderer(W, H, max_bounces=16, min_bounces=3)
+    a.upload_scene(sc)
+    a.render_frame(cam, 4)
+    ia = a.resolve().copy()
+    b = xb.Renderer(W, H, max_bounces=16, min_bounces=3)
+    b.upload_scene(sc)
+    b.set_guiding(True)
+    b.set_guiding(False)
+    b.render_frame(cam, 4)
+    ib = b.resolve().copy()
+    assert np.array_equal(ia, ib)
+    a.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_guide_params_round_trip_and_stats():
+    _, sc, cam = _room()
+    r = xb.Renderer(W, H, max_bounces=16, min_bounces=3)
+    r.upload_scene(sc)
+    r.set_guiding(True, train_spp=2, steps_per_spp=3, batch=1024, seed=5)
+    p0 = r.guide_params()
+    assert np.allclose(p0, xb.guide_init_params(5))
+    r.render_frame(cam, 4)
+    st = r.guiding_stats()
+    assert st["adam_steps"] == 6 and st["training"] == 0
+    p1 = r.guide_params()
+    assert not np.array_equal(p0, p1)
+    r.set_guide_params(p0)
+    assert np.array_equal(r.guide_params(), p0)
+    g = r.guiding()
+    assert g["enabled"] == 1 and g["train_spp"] == 2 and abs(g["guide_fraction"] - 0.5) < 1e-7
+    r.close()

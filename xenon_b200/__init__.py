@@ -201,6 +201,37 @@ class Renderer:
     def reset_profile(self) -> None:
         self._check(lib().xb_reset_profile(self.h))
 
+    def set_guiding(self, enabled: bool = True, **kw) -> None:
+        """xb_set_guiding: learned path guiding; keyword fields of abi.Guiding (0 = default)."""
+        g = abi.Guiding()
+        g.enabled = 1 if enabled else 0
+        for k, v in kw.items():
+            if k in ("bounds_min", "bounds_max"):
+                getattr(g, k)[:] = [float(x) for x in v]
+            else:
+                setattr(g, k, v)
+        self._check(lib().xb_set_guiding(self.h, ctypes.byref(g)))
+
+    def guiding(self) -> dict:
+        g = abi.Guiding()
+        self._check(lib().xb_get_guiding(self.h, ctypes.byref(g)))
+        return g.as_dict()
+
+    def guiding_stats(self) -> dict:
+        st = abi.GuidingStats()
+        self._check(lib().xb_get_guiding_stats(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def guide_params(self) -> np.ndarray:
+        out = np.empty(abi.GUIDE_PARAMS, np.float32)
+        self._check(lib().xb_guide_get_params(self.h, _p(out)))
+        return out
+
+    def set_guide_params(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.shape == (abi.GUIDE_PARAMS,)
+        self._check(lib().xb_guide_set_params(self.h, _p(p)))
+
     def trace_rays(self, rays: np.ndarray, mode: int = abi.XB_TRACE_CLOSEST) -> np.ndarray:
         rays = np.ascontiguousarray(rays)
         assert rays.dtype == abi.RAY_DTYPE
@@ -237,3 +268,55 @@ def bsdf_sample(mat: np.ndarray, wo: np.ndarray, states):
     m = np.ascontiguousarray(mat, np.float32)
     check(lib().xb_bsdf_sample(_p(m), n, _p(wo), _p(st), _p(wi), _p(f), _p(pdf), _p(flags)))
     return wi, f, pdf, flags, st
+
+
+# ── the guiding network on its own (xb_guide_*) ────────────────────────────────────
+def guide_init_params(seed: int = 1) -> np.ndarray:
+    out = np.empty(abi.GUIDE_PARAMS, np.float32)
+    check(lib().xb_guide_init_params(int(seed), _p(out)))
+    return out
+
+
+def guide_forward(params: np.ndarray, feats: np.ndarray) -> np.ndarray:
+    """feats [rows, 9] (position in [0,1]^3, normal, outgoing direction) -> lobes [rows, 8, 5]."""
+    p = np.ascontiguousarray(params, np.float32)
+    f = np.ascontiguousarray(feats, np.float32)
+    out = np.empty((len(f), abi.GUIDE_LOBE_FLOATS), np.float32)
+    check(lib().xb_guide_forward(_p(p), _p(f), len(f), _p(out)))
+    return out.reshape(len(f), 8, 5)
+
+
+def guide_loss_grad(params: np.ndarray, recs: np.ndarray):
+    p = np.ascontiguousarray(params, np.float32)
+    r = np.ascontiguousarray(recs, np.float32)
+    g = np.empty(abi.GUIDE_PARAMS, np.float32)
+    loss = np.zeros(1, np.float32)
+    check(lib().xb_guide_loss_grad(_p(p), _p(r), len(r), _p(g), _p(loss)))
+    return float(loss[0]), g
+
+
+def guide_train(params: np.ndarray, recs: np.ndarray, steps: int, batch: int, lr: float = 5e-3, seed: int = 1):
+    p = np.ascontiguousarray(params, np.float32)
+    r = np.ascontiguousarray(recs, np.float32)
+    out = np.empty(abi.GUIDE_PARAMS, np.float32)
+    losses = np.empty(steps, np.float32)
+    check(lib().xb_guide_train(_p(p), _p(r), len(r), int(steps), int(batch), float(lr), int(seed), _p(out),
+                               _p(losses)))
+    return out, losses
+
+
+def guide_mixture_pdf(lobes: np.ndarray, dirs: np.ndarray) -> np.ndarray:
+    L = np.ascontiguousarray(lobes, np.float32).reshape(-1, abi.GUIDE_LOBE_FLOATS)
+    d = np.ascontiguousarray(dirs, np.float32)
+    out = np.empty(len(L), np.float32)
+    check(lib().xb_guide_mixture_pdf(_p(L), len(L), _p(d), _p(out)))
+    return out
+
+
+def guide_mixture_sample(lobes: np.ndarray, u: np.ndarray):
+    L = np.ascontiguousarray(lobes, np.float32).reshape(-1, abi.GUIDE_LOBE_FLOATS)
+    uu = np.ascontiguousarray(u, np.float32)
+    d = np.empty((len(L), 3), np.float32)
+    pdf = np.empty(len(L), np.float32)
+    check(lib().xb_guide_mixture_sample(_p(L), len(L), _p(uu), _p(d), _p(pdf)))
+    return d, pdf

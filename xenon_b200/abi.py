@@ -143,7 +143,8 @@ class Config(ctypes.Structure):
 
 class RenderStats(ctypes.Structure):
     _fields_ = [("rays_closest", ctypes.c_int64), ("rays_shadow", ctypes.c_int64),
-                ("paths", ctypes.c_int64), ("overflow", ctypes.c_int64), ("last_ms", ctypes.c_float)]
+                ("paths", ctypes.c_int64), ("overflow", ctypes.c_int64), ("last_ms", ctypes.c_float),
+                ("nonfinite", ctypes.c_int64)]
 
 
 XB_PROFILE_STAGE_TIMES, XB_PROFILE_COUNT_TRAVERSAL = 1, 2
@@ -164,7 +165,35 @@ class Profile(ctypes.Structure):
                [(k, ctypes.c_int64) for k in ("raygen_launches", "extend_launches", "shade_launches",
                                               "shadow_launches", "accumulate_launches",
                                               "ext_blas_nodes", "ext_tris", "ext_tlas_nodes", "ext_instances",
-                                              "sh_blas_nodes", "sh_tris", "sh_tlas_nodes", "sh_instances")]
+                                              "sh_blas_nodes", "sh_tris", "sh_tlas_nodes", "sh_instances")] + \
+               [("train_ms", ctypes.c_double), ("train_launches", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+GUIDE_PARAMS = 15600        # XB_GUIDE_PARAMS
+GUIDE_LOBE_FLOATS = 40
+GUIDE_RECORD_FLOATS = 20
+
+
+class Guiding(ctypes.Structure):
+    """xb_guiding: learned path guiding (0 fields take their defaults)."""
+    _fields_ = [("enabled", ctypes.c_int32), ("train_spp", ctypes.c_int32), ("steps_per_spp", ctypes.c_int32),
+                ("batch", ctypes.c_int32), ("learning_rate", ctypes.c_float), ("guide_fraction", ctypes.c_float),
+                ("max_records", ctypes.c_int32), ("record_stride", ctypes.c_int32), ("seed", ctypes.c_uint64),
+                ("bounds_min", ctypes.c_float * 3), ("bounds_max", ctypes.c_float * 3)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["bounds_min"] = list(self.bounds_min)
+        d["bounds_max"] = list(self.bounds_max)
+        return d
+
+
+class GuidingStats(ctypes.Structure):
+    _fields_ = [("adam_steps", ctypes.c_int64), ("records", ctypes.c_int64), ("records_dropped", ctypes.c_int64),
+                ("last_loss", ctypes.c_float), ("training", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -371,4 +371,47 @@ __device__ __forceinline__ bool bsdf_sample(V3 wo, const DevMaterial& m, Pcg& rn
   return true;
 }
 
+// ── the sampler's lobe values for a given direction (guided sampling; no reference counterpart)
+// For a non-delta material seen from its front side (wo.z > 0), bsdf_sample draws a lobe l with
+// probability P_l and a direction from that lobe's density pdf_l, and returns f_l and
+// P_l pdf_l. Given a direction wi drawn by another proposal, this returns what the sampler
+// would have returned had it produced wi: a lobe chosen with its posterior probability
+// P_l pdf_l(wi) / sum_k P_k pdf_k(wi) (u selects it), that lobe's f and P_l pdf_l, and the
+// sampler's marginal density sum_k P_k pdf_k(wi) (equal to bsdf_pdf for these materials).
+// Returns false where the sampler cannot produce wi.
+__device__ __forceinline__ bool bsdf_lobe_for_direction(V3 wo, V3 wi, const DevMaterial& m, float u, V3& f,
+                                                        float& pdf_sel, float& pdf_marg) {
+  if (m.flags & kMatConductor) {
+    pdf_sel = pdf_marg = mfr_pdf(wo, wi, m);
+    f = mfr_eval(wo, wi, m);
+  } else if (m.flags & kMatSubsurface) {
+    pdf_sel = pdf_marg = diffuse_pdf(wi);
+    f = (wi.z > 0.f) ? ss_color(m) * (1.f - m.metallic) * kInvPi : v3s(0.f);
+  } else if (m.flags & kMatTransmissive) {
+    const float fr = fresnel_dielectric(fabsf(wo.z), m.ior);
+    if (wi.z > 0.f) {
+      pdf_sel = fr * mfr_pdf(wo, wi, m);
+      f = mfr_eval(wo, wi, m);
+    } else {
+      pdf_sel = (1.f - fr) * mft_pdf(wo, wi, m);
+      f = mft_eval(wo, wi, m);
+    }
+    pdf_marg = pdf_sel;
+  } else {
+    const float spec = sclamp(m.f0[0], 0.f, 1.f), diff = 1.f - spec;
+    const float ps = spec * mfr_pdf(wo, wi, m), pd = diff * diffuse_pdf(wi);
+    pdf_marg = ps + pd;
+    if (!(pdf_marg > 0.f)) return false;
+    if (u * pdf_marg < ps) {
+      pdf_sel = ps;
+      f = mfr_eval(wo, wi, m);
+    } else {
+      pdf_sel = pd;
+      f = diffuse_eval(wi, m);
+    }
+  }
+  return pdf_sel >= 1e-8f && pdf_marg > 0.f;
+}
+
 }  // namespace xbd
+

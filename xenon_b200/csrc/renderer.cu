@@ -38,6 +38,8 @@
 #include "dev_scene.cuh"
 #include "scene_host.h"
 #include "trace_persistent.cuh"
+#include "guide.h"
+#include "guide_dev.cuh"
 
 using namespace xbd;
 
@@ -57,6 +59,8 @@ enum {
   CNT_FETCH_SH_SUN = 5,
 };
 enum { STAT_RAYS = 0, STAT_SHADOW = 1, STAT_PATHS = 2, STAT_OVERFLOW = 3, STAT_NONFINITE = 4,
+       STAT_REC_DROPPED = 5,  // guiding: training records beyond the per-wave capacity
+       STAT_REC_TOTAL = 6,    // guiding: training records collected
        STAT_EXT_WORK = 8,    // 4 counters: blas nodes, tris, tlas nodes, instances (closest hit)
        STAT_SH_WORK = 12,    // same for shadow rays
        STAT_COUNT = 16 };
@@ -89,6 +93,8 @@ struct WaveBuffers {
   float4* sh_c[2] = {nullptr, nullptr};   // contribution xyz
   float4* L = nullptr;                    // per path radiance
   int32_t* cnt = nullptr;                 // [kMaxDepth + 1][kCntStride]
+  int32_t* rec[2] = {nullptr, nullptr};   // guiding: training record of the emitting vertex
+  float* ratio[2] = {nullptr, nullptr};   // guiding: importance ratio of the path
 };
 
 }  // namespace
@@ -128,8 +134,16 @@ struct xb_renderer {
   std::vector<cudaEvent_t> ev_pool;          // event pairs, reused each call
   std::vector<int> ev_stage;                 // stage of each recorded pair
   size_t ev_used = 0;
-  double stage_ms[5] = {0, 0, 0, 0, 0};      // raygen, extend, shade, shadow, accumulate
-  int64_t stage_launches[5] = {0, 0, 0, 0, 0};
+  double stage_ms[6] = {0, 0, 0, 0, 0, 0};      // raygen, extend, shade, shadow, accumulate, train
+  int64_t stage_launches[6] = {0, 0, 0, 0, 0, 0};
+  // learned path guiding
+  xb_guiding gcfg{};
+  bool guiding = false;
+  xbg::Guide* guide = nullptr;
+  float gbmin[3] = {0, 0, 0}, gbinv[3] = {1, 1, 1};   // network position box
+  float scene_lo[3] = {0, 0, 0}, scene_hi[3] = {1, 1, 1};
+  int occ_gshade = 1, grid_gshade = 0;
+  int last_loss_index = -1;
   // generic scratch for trace/bsdf helpers
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -471,6 +485,291 @@ __global__ void __launch_bounds__(128) shade_kernel(ShadeArgs a) {
   }
 }
 
+// ── guided shade: one bounce with the learned proposal (no reference counterpart) ──────
+// Guiding here importance-samples the plain estimator: at a guided vertex the direction comes
+// from the mixture p = a q_guide + (1 - a) p_bsdf (p_bsdf the density of bsdf_sample) and the
+// vertex keeps everything the plain sampler would have produced for that direction (the lobe,
+// its f and pdf, hence the MIS weights and the Russian-roulette throughput), while the path
+// carries the importance ratio prod p_bsdf / p as a separate scalar. The expectation therefore
+// equals the plain tracer's exactly, whatever the scene, and the ratio never exceeds 1 / (1 - a).
+// The network runs inside the kernel: each CTA encodes its 128 vertices into shared memory,
+// runs the 4 layers on the tensor cores (tcgen05, TMEM accumulators) and keeps the lobes of its
+// rows in shared memory for the rest of the bounce.
+struct GuideShadeArgs {
+  const __nv_bfloat16* wf;   // forward weights (bf16)
+  const float* master;       // FP32 parameters (biases)
+  float alpha;               // probability of sampling the network
+  float bmin[3], binv[3];    // position -> [0,1]^3
+  const float* ratio_in;     // importance ratio of each incoming path (nullptr: 1)
+  float* ratio_out;
+  float* recs;               // training records (nullptr: not training)
+  int32_t* rec_count;
+  int rec_cap, rec_stride;
+  const int32_t* rec_in;     // record of the vertex that emitted each incoming ray (or nullptr)
+  int32_t* rec_out;          // same for the outgoing queue
+  int* err;
+};
+
+constexpr float kNaN = __builtin_nanf("");
+constexpr int kLobStride = xbg::kLobeFloats + 1;   // conflict-free per-thread rows
+constexpr size_t kGuidedShadeSmem =
+    xbg::kFwdWeightBytes + xbg::kTileBytes + (size_t)xbg::kTile * kLobStride * 4 + 1024;
+
+__global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideShadeArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* sW = smem;
+  uint8_t* sA = smem + xbg::kFwdWeightBytes;
+  float* sLob = reinterpret_cast<float*>(sA + xbg::kTileBytes);
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ float sBias[xbg::kBiasFloats];
+  const int n = a.cnt[CNT_RAYS];
+  if ((int)blockIdx.x * 128 >= n) return;
+  const DevScene& sc = a.sc;
+  const bool last = (a.depth + 1 >= a.max_bounces);
+  const bool training = g.recs != nullptr;
+  xbg::load_forward_weights(sW, sBias, g.wf, g.master);
+  xbg::mma_setup(&tmem_slot, &mbar);
+  xbg::Mma m{tmem_slot, &mbar, 0u, g.err, true};
+  float* lob = sLob + threadIdx.x * kLobStride;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int slot = base + threadIdx.x;
+    bool emit_next = false, emit_area = false, emit_sun = false, emit_rec = false;
+    float4 n_o, n_d, n_tp;
+    uint64_t n_rng = 0;
+    int32_t pid = 0;
+    float n_ratio = 1.f;
+    float4 a_o, a_d, a_c, s_o, s_d, s_c;
+    float4 rec[5];
+    // ── phase 1: emitter test and the network's input ──
+    bool alive = false, guided = false;
+    float feat[9] = {0.5f, 0.5f, 0.5f, 0.f, 0.f, 1.f, 0.f, 0.f, 1.f};
+    float4 ro = make_float4(0, 0, 0, 0), rd = ro, tpv = ro;
+    float ratio = 1.f;
+    Pcg rng{0};
+    FullHit fh;
+    fh.mat_id = 0;
+    if (slot < n) {
+      ro = a.ray_o[slot]; rd = a.ray_d[slot]; tpv = a.tp[slot];
+      pid = a.path[slot];
+      rng.state = a.rng[slot];
+      if (g.ratio_in) ratio = g.ratio_in[slot];
+      if (g.rec_in) {
+        const int ri = g.rec_in[slot];
+        if (ri >= 0) {   // path radiance before the continuation of the record's vertex
+          const float4 l = a.L[pid];
+          float* R = g.recs + (size_t)ri * xbg::kRecFloats;
+          R[17] = l.x; R[18] = l.y; R[19] = l.z;
+        }
+      }
+      const Ray ray{v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), ro.w, rd.w};
+      const V3 tpr = v3(tpv.x, tpv.y, tpv.z) * ratio;   // the path's actual throughput
+      const float4 hv = a.hit[slot];
+      const int hinst = a.hit_inst[slot];
+      if (hinst < 0) {
+        if (sc.sky_intensity > 0.f) add_L(a.L, pid, tpr * sky_eval(sc, ray.d));
+      } else {
+        HitState h{hv.x, hv.y, hv.z, __float_as_int(hv.w), hinst};
+        complete_hit(sc, ray, h, fh);
+        bool hit_light = false;
+        for (int li = 0; li < sc.num_lights; ++li) {
+          const DevLight& lt = sc.lights[li];
+          if (__float_as_int(lt.p2.w) == fh.prim_id && __float_as_int(lt.p1.w) == fh.instance_id) {
+            float mis = 1.0f;
+            const float cos_l = smax(0.0f, dot(fh.geo_normal, -ray.d));
+            if (cos_l > 1e-6f) {
+              if (a.depth > 0 && !(tpv.w < 0.f)) {
+                const float pdf_area = (1.0f / lt.p0.w) * (1.0f / (float)sc.num_lights);
+                const float pdf_sa = (pdf_area * (h.t * h.t)) / cos_l;
+                mis = mis_power2(tpv.w, pdf_sa);
+              }
+              add_L(a.L, pid, tpr * v3(lt.emission.x, lt.emission.y, lt.emission.z) * mis);
+            }
+            hit_light = true;
+            break;
+          }
+        }
+        if (!hit_light) {
+          alive = true;
+          // The network proposes at non-delta vertices seen from the front of the shading
+          // normal, where the sampler's density is bsdf_pdf; elsewhere the plain sampler runs.
+          guided = (sc.mats[fh.mat_id].flags & kMatDelta) == 0 && dot(fh.normal, -ray.d) > 0.f;
+          for (int k = 0; k < 3; ++k) {
+            const float pk = (k == 0 ? fh.pos.x : k == 1 ? fh.pos.y : fh.pos.z);
+            feat[k] = fminf(fmaxf((pk - g.bmin[k]) * g.binv[k], 0.f), 1.f);
+          }
+          feat[3] = fh.normal.x; feat[4] = fh.normal.y; feat[5] = fh.normal.z;
+          feat[6] = -ray.d.x; feat[7] = -ray.d.y; feat[8] = -ray.d.z;
+        }
+      }
+    }
+    // ── the network on this CTA's 128 vertices ──
+    xbg::encode_row(feat, sA, threadIdx.x);
+    {
+      float raw[xbg::kOut];
+      xbg::forward_tile(m, sA, sW, sBias, raw);
+      if (!m.ok) break;   // uniform: every thread saw the same failed wait
+      float lo[xbg::kLobeFloats];
+      xbg::raw_to_lobes(raw, lo);
+#pragma unroll
+      for (int i = 0; i < xbg::kLobeFloats; ++i) lob[i] = lo[i];
+    }
+    // ── phase 2: NEE, roulette, the next direction (cpu_tiled.cpp:89-216) ──
+    if (alive) do {
+      const Ray ray{v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), ro.w, rd.w};
+      V3 tp = v3(tpv.x, tpv.y, tpv.z);   // the plain estimator's throughput
+      const DevMaterial& mat = sc.mats[fh.mat_id];
+      const bool is_delta = (mat.flags & kMatDelta) != 0;
+      if (sc.num_lights > 0 && !is_delta) {
+        const float upick = rng.next_float();
+        int li = (int)(upick * (float)sc.num_lights);
+        li = li < 0 ? 0 : (li > sc.num_lights - 1 ? sc.num_lights - 1 : li);
+        const float pick_pdf = 1.f / (float)sc.num_lights;
+        const DevLight& lt = sc.lights[li];
+        const float u1 = rng.next_float();
+        const float u2 = rng.next_float();
+        const float su1 = sqrtf(u1);
+        const float b0 = 1.0f - su1;
+        const float b1 = u2 * su1;
+        const float b2 = 1.0f - b0 - b1;
+        const V3 lp = ld3(lt.p0) * b0 + ld3(lt.p1) * b1 + ld3(lt.p2) * b2;
+        const V3 sdir = lp - fh.pos;
+        const float dsq = length_sq(sdir);
+        const float dist = sqrtf(dsq);
+        if (dist > 1e-6f) {
+          const V3 wi = sdir / dist;
+          const float cos_l = smax(0.0f, dot(ld3(lt.n), -wi));
+          const Onb onb(fh.geo_normal);
+          const V3 wo_l = onb.to_local(-ray.d);
+          const V3 wi_l = onb.to_local(wi);
+          if (cos_l > 1e-6f && wi_l.z > 1e-6f) {
+            const V3 f = bsdf_eval(wo_l, wi_l, mat);
+            const float bp = bsdf_pdf(wo_l, wi_l, mat);
+            const float lpdf = ((1.0f / lt.p0.w) * pick_pdf) * (dsq / cos_l);
+            const float mis = mis_power2(lpdf, bp);
+            if (mis > 0.0f && lpdf > 1e-12f) {
+              const V3 org = offset_origin(fh.pos, fh.geo_normal, wi, kShadowEps);
+              const V3 c = (tp * ratio) * f * wi_l.z * (v3(lt.emission.x, lt.emission.y, lt.emission.z) / lpdf) * mis;
+              a_o = make_float4(org.x, org.y, org.z, dist - kShadowEps);
+              a_d = make_float4(wi.x, wi.y, wi.z, __int_as_float(pid));
+              a_c = make_float4(c.x, c.y, c.z, 0.f);
+              emit_area = true;
+            }
+          }
+        }
+      }
+      if (sc.num_suns > 0 && !is_delta) {
+        const float upick = rng.next_float();
+        int di = (int)(upick * (float)sc.num_suns);
+        di = di < 0 ? 0 : (di > sc.num_suns - 1 ? sc.num_suns - 1 : di);
+        const float dpick = 1.f / (float)sc.num_suns;
+        const DevSun& sun = sc.suns[di];
+        const V3 sdir = v3(sun.dir[0], sun.dir[1], sun.dir[2]);
+        const Onb onb(fh.geo_normal);
+        const V3 wo_l = onb.to_local(-ray.d);
+        const V3 wi_l = onb.to_local(sdir);
+        if (wi_l.z > 1e-6f) {
+          const V3 f = bsdf_eval(wo_l, wi_l, mat);
+          const float bp = bsdf_pdf(wo_l, wi_l, mat);
+          const float lpdf = 1e8f * dpick;
+          const float mis = mis_power2(lpdf, bp);
+          const V3 org = offset_origin(fh.pos, fh.geo_normal, sdir, kShadowEps);
+          const V3 em = v3(sun.emission[0], sun.emission[1], sun.emission[2]);
+          const V3 c = (tp * ratio) * f * wi_l.z * (em / lpdf) * mis;
+          s_o = make_float4(org.x, org.y, org.z, kInf);
+          s_d = make_float4(sdir.x, sdir.y, sdir.z, __int_as_float(pid));
+          s_c = make_float4(c.x, c.y, c.z, 0.f);
+          emit_sun = true;
+        }
+      }
+      if (last) break;
+      if (a.depth >= a.min_bounces) {
+        // cpu_tiled.cpp:190-194 on the plain throughput: p = max(0.05, max(tp)), survive with
+        // min(1, p), divide by p. Its part above 1 is a deterministic rescale and stays as is;
+        // the survival draw is made with the probability the actual throughput (tp * ratio)
+        // asks for, and the ratio of the two survival probabilities joins the importance ratio.
+        const float p = smax(0.05f, max_component(tp));
+        const float surv = smin(1.f, p);
+        const float surv_g = sclamp(max_component(tp * ratio) / smax(1.f, p), 0.05f, 1.f);
+        if (rng.next_float() > surv_g) break;
+        tp = tp / p;
+        ratio = ratio * (surv / surv_g);
+      }
+      const Onb onb(fh.normal);
+      const V3 wo_l = onb.to_local(-ray.d);
+      BsdfSample s;
+      V3 wiw;
+      n_ratio = ratio;
+      if (!guided) {
+        if (!bsdf_sample(wo_l, mat, rng, s)) break;
+        wiw = onb.to_world(s.wi);
+      } else {
+        float pb;
+        if (rng.next_float() < g.alpha) {
+          const float u0 = rng.next_float(), u1 = rng.next_float(), u2 = rng.next_float();
+          float d[3];
+          xbg::mix_sample(lob, u0, u1, u2, d);
+          wiw = v3(d[0], d[1], d[2]);
+          s.wi = onb.to_local(wiw);
+          s.delta = false;
+          if (!bsdf_lobe_for_direction(wo_l, s.wi, mat, rng.next_float(), s.f, s.pdf, pb)) break;
+        } else {
+          if (!bsdf_sample(wo_l, mat, rng, s)) break;
+          wiw = onb.to_world(s.wi);
+          pb = bsdf_pdf(wo_l, s.wi, mat);
+        }
+        const float pm = g.alpha * xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) + (1.f - g.alpha) * pb;
+        if (!(pm > 0.f)) break;
+        n_ratio = ratio * (pb / pm);
+        if (training && (pid % g.rec_stride) == 0) {
+          const V3 tb = tp * ratio;   // actual throughput before the vertex's scattering
+          rec[0] = make_float4(feat[0], feat[1], feat[2], feat[3]);
+          rec[1] = make_float4(feat[4], feat[5], feat[6], feat[7]);
+          rec[2] = make_float4(feat[8], wiw.x, wiw.y, wiw.z);
+          rec[3] = make_float4(0.f, __int_as_float(pid), tb.x, tb.y);
+          rec[4] = make_float4(tb.z, kNaN, kNaN, kNaN);   // baseline: set by the next bounce
+          emit_rec = true;
+        }
+      }
+      // cpu_tiled.cpp:197-216
+      if (s.delta) {
+        tp = tp * s.f;
+      } else {
+        const float ci = fabsf(s.wi.z);
+        if (s.pdf < 1e-8f || ci < 1e-8f) { emit_rec = false; break; }
+        tp = tp * (s.f * ci / s.pdf);
+      }
+      const V3 org = offset_origin(fh.pos, fh.geo_normal, wiw, kRayEps);
+      n_o = make_float4(org.x, org.y, org.z, kRayEps);
+      n_d = make_float4(wiw.x, wiw.y, wiw.z, kInf);
+      n_tp = make_float4(tp.x, tp.y, tp.z, s.delta ? -1.f : s.pdf);
+      n_rng = rng.state;
+      emit_next = true;
+    } while (false);
+    if (!emit_next) emit_rec = false;
+    int ridx = -1;
+    if (training) {
+      ridx = warp_append(g.rec_count, emit_rec, g.rec_cap, a.stats + STAT_REC_DROPPED);
+      if (ridx >= 0) {
+        float4* R = reinterpret_cast<float4*>(g.recs + (size_t)ridx * xbg::kRecFloats);
+        for (int i = 0; i < 5; ++i) R[i] = rec[i];
+      }
+    }
+    int idx = warp_append(a.cnt_next + CNT_RAYS, emit_next, a.capacity, a.stats + STAT_OVERFLOW);
+    if (idx >= 0) {
+      a.nray_o[idx] = n_o; a.nray_d[idx] = n_d; a.ntp[idx] = n_tp; a.nrng[idx] = n_rng;
+      a.npath[idx] = pid;
+      g.ratio_out[idx] = n_ratio;
+      if (g.rec_out) g.rec_out[idx] = ridx;
+    }
+    idx = warp_append(a.cnt + CNT_SH_AREA, emit_area, a.capacity, a.stats + STAT_OVERFLOW);
+    if (idx >= 0) { a.sh_o[0][idx] = a_o; a.sh_d[0][idx] = a_d; a.sh_c[0][idx] = a_c; }
+    idx = warp_append(a.cnt + CNT_SH_SUN, emit_sun, a.capacity, a.stats + STAT_OVERFLOW);
+    if (idx >= 0) { a.sh_o[1][idx] = s_o; a.sh_d[1][idx] = s_d; a.sh_c[1][idx] = s_c; }
+  }
+  xbg::mma_teardown(m.tmem);
+}
+
 // ── accumulate the wave into the framebuffer, in sample order ──────────────────
 __global__ void accumulate_kernel(const float4* L, int64_t npix, int spw, int spp_before,
                                   float4* accum, double* sum64, double* m2_64, double* mean64,
@@ -690,7 +989,8 @@ void free_wave(xb_renderer* r) {
   WaveBuffers& w = r->wb;
   void* ptrs[] = {w.ray_o[0], w.ray_o[1], w.ray_d[0], w.ray_d[1], w.tp[0], w.tp[1], w.rng[0],
                   w.rng[1], w.path[0], w.path[1], w.hit, w.hit_inst, w.sh_o[0], w.sh_o[1],
-                  w.sh_d[0], w.sh_d[1], w.sh_c[0], w.sh_c[1], w.L, w.cnt};
+                  w.sh_d[0], w.sh_d[1], w.sh_c[0], w.sh_c[1], w.L, w.cnt, w.rec[0], w.rec[1],
+                  w.ratio[0], w.ratio[1]};
   for (void* p : ptrs) if (p) cudaFree(p);
   w = WaveBuffers();
 }
@@ -731,6 +1031,8 @@ int alloc_wave(xb_renderer* r, int64_t cap) {
     ok &= A(&w.sh_o[q], cap * sizeof(float4));
     ok &= A(&w.sh_d[q], cap * sizeof(float4));
     ok &= A(&w.sh_c[q], cap * sizeof(float4));
+    ok &= A(&w.rec[q], cap * sizeof(int32_t));
+    ok &= A(&w.ratio[q], cap * sizeof(float));
   }
   ok &= A(&w.hit, cap * sizeof(float4));
   ok &= A(&w.hit_inst, cap * sizeof(int32_t));
@@ -770,6 +1072,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   r->grid_shadow = r->num_sms * std::min(r->occ_shadow, c.shadow_blocks_per_sm);
   r->grid_pshadow = r->num_sms * std::min(r->occ_pshadow, c.shadow_blocks_per_sm);
   r->grid_shade = r->num_sms * std::min(r->occ_shade, c.shade_blocks_per_sm);
+  r->grid_gshade = r->num_sms * std::min(r->occ_gshade, c.shade_blocks_per_sm);
   const int64_t npix = (int64_t)r->cfg.width * r->cfg.height;
   const int spw = (int)std::min<int64_t>(1024, std::max<int64_t>(1, c.wave_paths / npix));
   if (spw != r->spp_per_wave || r->wb.capacity == 0) {
@@ -779,7 +1082,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   return XB_OK;
 }
 
-enum { STAGE_RAYGEN = 0, STAGE_EXTEND = 1, STAGE_SHADE = 2, STAGE_SHADOW = 3, STAGE_ACCUM = 4 };
+enum { STAGE_RAYGEN = 0, STAGE_EXTEND = 1, STAGE_SHADE = 2, STAGE_SHADOW = 3, STAGE_ACCUM = 4, STAGE_TRAIN = 5 };
 
 // Stage timing: a pair of events around a launch, read back after the call's final sync.
 struct StageTimer {
@@ -828,10 +1131,37 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
   WaveBuffers& w = r->wb;
   const int depth_max = std::min(r->max_bounces, kMaxDepth);
   int done = 0;
+  xbg::Guide* gd = r->guiding ? r->guide : nullptr;
+  if (gd) {
+    // position box of the network's input: the configured one, else the scene's bounds
+    const xb_guiding& gc = r->gcfg;
+    const bool boxed = gc.bounds_max[0] > gc.bounds_min[0] && gc.bounds_max[1] > gc.bounds_min[1] &&
+                       gc.bounds_max[2] > gc.bounds_min[2];
+    for (int k = 0; k < 3; ++k) {
+      const float lo = boxed ? gc.bounds_min[k] : r->scene_lo[k];
+      const float hi = boxed ? gc.bounds_max[k] : r->scene_hi[k];
+      r->gbmin[k] = lo;
+      r->gbinv[k] = hi > lo ? 1.f / (hi - lo) : 1.f;
+    }
+  }
   while (done < spp_count) {
-    const int spw = std::min(r->spp_per_wave, spp_count - done);
+    const int sample0 = spp_first + done;   // 1-based index of the wave's first sample
+    const bool train = gd && sample0 <= r->gcfg.train_spp;
+    int spw = std::min(r->spp_per_wave, spp_count - done);
+    if (train) {
+      // a training wave ends at train_spp and stays within one guide_train call's step budget
+      spw = std::min(spw, r->gcfg.train_spp - sample0 + 1);
+      spw = std::max(1, std::min(spw, xbg::kMaxTrainSteps / std::max(1, r->gcfg.steps_per_spp)));
+    }
     const int64_t paths = npix * spw;
     CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), r->stream));
+    int rec_stride = 1;
+    if (train) {
+      CK(cudaMemsetAsync(xbg::guide_record_count(gd), 0, sizeof(int32_t), r->stream));
+      const int64_t cap = xbg::guide_record_capacity(gd);
+      rec_stride = r->gcfg.record_stride > 0 ? r->gcfg.record_stride
+                                             : (int)std::max<int64_t>(1, (paths * 4 + cap - 1) / cap);
+    }
     const int g_rg = (int)std::min<int64_t>((paths + 255) / 256, (int64_t)r->num_sms * 16);
     const bool count = (r->prof_flags & XB_PROFILE_COUNT_TRAVERSAL) != 0;
     {
@@ -868,7 +1198,24 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       sa.depth = d; sa.min_bounces = r->min_bounces; sa.max_bounces = depth_max;
       sa.capacity = (int)w.capacity;
       sa.stats = r->stats;
-      {
+      if (gd) {
+        GuideShadeArgs ga;
+        ga.wf = xbg::guide_weights_bf16(gd);
+        ga.master = xbg::guide_master(gd);
+        ga.alpha = r->gcfg.guide_fraction;
+        ga.ratio_in = d > 0 ? w.ratio[q] : nullptr;
+        ga.ratio_out = w.ratio[nq];
+        for (int k = 0; k < 3; ++k) { ga.bmin[k] = r->gbmin[k]; ga.binv[k] = r->gbinv[k]; }
+        ga.recs = train ? xbg::guide_records(gd) : nullptr;
+        ga.rec_count = xbg::guide_record_count(gd);
+        ga.rec_cap = xbg::guide_record_capacity(gd);
+        ga.rec_stride = rec_stride;
+        ga.rec_in = (train && d > 0) ? w.rec[q] : nullptr;
+        ga.rec_out = train ? w.rec[nq] : nullptr;
+        ga.err = xbg::guide_error(gd);
+        StageTimer t(r, STAGE_SHADE);
+        guided_shade_kernel<<<r->grid_gshade, 128, kGuidedShadeSmem, r->stream>>>(sa, ga);
+      } else {
         StageTimer t(r, STAGE_SHADE);
         shade_kernel<<<r->grid_shade, 128, 0, r->stream>>>(sa);
       }
@@ -896,6 +1243,16 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       StageTimer t(r, STAGE_ACCUM);
       accumulate_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, npix, spw, r->spp + done, r->accum, r->sum64,
                                                       r->m2_64, r->mean64, w.cnt, depth_max, paths, r->stats);
+    }
+    if (train) {
+      StageTimer t(r, STAGE_TRAIN);
+      xbg::guide_finalize_records(gd, r->stream, w.L, r->num_sms * 8, r->stats + STAT_REC_TOTAL);
+      const int steps = r->gcfg.steps_per_spp * spw;
+      if (xbg::guide_train(gd, r->stream, xbg::guide_records(gd), xbg::guide_record_count(gd),
+                           xbg::guide_record_capacity(gd), steps, r->gcfg.batch, r->gcfg.learning_rate,
+                           r->gcfg.seed) != XB_OK)
+        return set_err(r, XB_E_CUDA, "guide training launch failed");
+      r->last_loss_index = steps - 1;
     }
     CK(cudaGetLastError());
     done += spw;
@@ -948,6 +1305,26 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   r->occ_shadow = std::max(occ, 1);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel, 128, 0);
   r->occ_shade = std::max(occ, 1);
+  // guided shade: dynamic shared memory for the weights, one activation tile and the lobes; at
+  // most 4 CTAs per SM so their TMEM (64 columns each) always fits the SM's 512 columns
+  if (cudaFuncSetAttribute(guided_shade_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kGuidedShadeSmem) != cudaSuccess)
+    return bail(xb::fail(XB_E_CUDA, "guided shade kernel attribute failed"));
+  {
+    // CTAs per SM from the kernel's own footprint (registers in 256-register warp units, shared
+    // memory with the per-CTA reservation), capped at 4 for TMEM
+    cudaFuncAttributes fa{};
+    int regs_sm = 65536, smem_sm = 0, smem_rsv = 0;
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, cfg->device);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, cfg->device);
+    cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, cfg->device);
+    if (cudaFuncGetAttributes(&fa, guided_shade_kernel) != cudaSuccess)
+      return bail(xb::fail(XB_E_CUDA, "guided shade kernel attributes failed"));
+    const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;
+    const int by_regs = regs_sm / std::max(1, warp_regs * 4);
+    const int by_smem = smem_sm / std::max<int>(1, (int)(kGuidedShadeSmem + fa.sharedSizeBytes) + smem_rsv);
+    r->occ_gshade = std::max(1, std::min(4, std::min(by_regs, by_smem)));
+  }
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_persistent_kernel<false>, 128, 0);
   r->occ_pext = std::max(occ, 1);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_persistent_kernel<false>, 128, 0);
@@ -975,6 +1352,7 @@ void xb_destroy(xb_renderer* r) {
   if (r->stream) cudaStreamSynchronize(r->stream);
   free_scene(r);
   free_wave(r);
+  xbg::guide_destroy(r->guide);
   void* ptrs[] = {r->accum, r->sum64, r->m2_64, r->mean64, r->resolve_buf, r->stats, r->scratch};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (cudaEvent_t e : r->ev_pool) cudaEventDestroy(e);
@@ -1146,6 +1524,12 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   if ((rc = dev_upload(r, mats, &sc.mats))) return rc;
   if ((rc = dev_upload(r, lights, &sc.lights))) return rc;
   if ((rc = dev_upload(r, suns, &sc.suns))) return rc;
+  if (v->num_tlas_nodes > 0) {
+    for (int k = 0; k < 3; ++k) {
+      r->scene_lo[k] = v->tlas_nodes[0].mn[k];
+      r->scene_hi[k] = v->tlas_nodes[0].mx[k];
+    }
+  }
   sc.num_lights = v->num_lights;
   sc.num_suns = v->num_suns;
   sc.num_tlas_nodes = v->num_tlas_nodes;
@@ -1250,6 +1634,7 @@ int xb_get_render_stats(const xb_renderer* r_, xb_render_stats* out) {
   out->paths = (int64_t)s[STAT_PATHS];
   out->overflow = (int64_t)s[STAT_OVERFLOW];
   out->last_ms = r->last_ms;
+  out->nonfinite = (int64_t)s[STAT_NONFINITE];
   return XB_OK;
 }
 
@@ -1274,6 +1659,98 @@ int xb_set_tuning(xb_renderer* r, const xb_tuning* t) {
 int xb_get_tuning(const xb_renderer* r, xb_tuning* out) {
   if (!r || !out) return xb::fail(XB_E_INVALID, "xb_get_tuning: null argument");
   *out = r->tune;
+  return XB_OK;
+}
+
+// ── learned path guiding ─────────────────────────────────────────────────────────
+int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!g) return set_err(r, XB_E_INVALID, "xb_set_guiding: null config");
+  xb_guiding c = *g;
+  if (c.train_spp == 0) c.train_spp = 64;
+  if (c.steps_per_spp == 0) c.steps_per_spp = 32;
+  if (c.batch == 0) c.batch = 16384;
+  if (c.learning_rate == 0.f) c.learning_rate = 5e-3f;
+  if (c.guide_fraction == 0.f) c.guide_fraction = 0.5f;
+  if (c.max_records == 0) c.max_records = 1 << 21;
+  if (c.seed == 0) c.seed = 1;
+  if (c.train_spp < -1 || c.steps_per_spp < 0 || c.steps_per_spp > xbg::kMaxTrainSteps || c.batch < 0 ||
+      c.batch % 128 != 0 || c.batch > (1 << 20) || !(c.learning_rate > 0.f) || !(c.guide_fraction > 0.f) ||
+      c.guide_fraction > 1.f || c.max_records < 128 || c.max_records > (1 << 24) || c.record_stride < 0)
+    return set_err(r, XB_E_INVALID, "xb_set_guiding: bad configuration");
+  if (!c.enabled) {
+    r->guiding = false;
+    r->gcfg = c;
+    return XB_OK;
+  }
+  CK(cudaStreamSynchronize(r->stream));
+  if (!r->guide || c.seed != r->gcfg.seed || c.max_records != r->gcfg.max_records) {
+    xbg::guide_destroy(r->guide);
+    r->guide = nullptr;
+    rc = xbg::guide_create(&r->guide, c.seed, c.max_records);
+    if (rc != XB_OK) return set_err(r, rc, "xb_set_guiding: cannot create the network (%d records)", c.max_records);
+    r->last_loss_index = -1;
+  }
+  r->gcfg = c;
+  r->guiding = true;
+  return XB_OK;
+}
+
+int xb_get_guiding(const xb_renderer* r, xb_guiding* out) {
+  if (!r || !out) return xb::fail(XB_E_INVALID, "xb_get_guiding: null argument");
+  *out = r->gcfg;
+  out->enabled = r->guiding ? 1 : 0;
+  return XB_OK;
+}
+
+int xb_get_guiding_stats(const xb_renderer* r_, xb_guiding_stats* out) {
+  xb_renderer* r = const_cast<xb_renderer*>(r_);
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!out) return set_err(r, XB_E_INVALID, "null output");
+  std::memset(out, 0, sizeof(*out));
+  unsigned long long s[STAT_COUNT];
+  CK(cudaMemcpyAsync(s, r->stats, sizeof(s), cudaMemcpyDeviceToHost, r->stream));
+  float loss = 0.f;
+  if (r->guide && r->last_loss_index >= 0)
+    CK(cudaMemcpyAsync(&loss, xbg::guide_losses(r->guide) + r->last_loss_index, sizeof(float),
+                       cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  out->adam_steps = r->guide ? xbg::guide_steps_taken(r->guide) : 0;
+  out->records = (int64_t)s[STAT_REC_TOTAL];
+  out->records_dropped = (int64_t)s[STAT_REC_DROPPED];
+  out->last_loss = loss;
+  out->training = (r->guiding && r->spp < r->gcfg.train_spp) ? 1 : 0;
+  if (r->guide) {
+    int herr = 0;
+    CK(cudaMemcpy(&herr, xbg::guide_error(r->guide), sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return set_err(r, XB_E_TIMEOUT, "guiding: a tensor-core completion wait ran out");
+  }
+  return XB_OK;
+}
+
+int xb_guide_get_params(xb_renderer* r, float* params) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!params) return set_err(r, XB_E_INVALID, "null output");
+  if (!r->guide) return set_err(r, XB_E_STATE, "guiding was never enabled");
+  CK(cudaMemcpyAsync(params, xbg::guide_master(r->guide), xbg::kParams * sizeof(float), cudaMemcpyDeviceToHost,
+                     r->stream));
+  CK(cudaStreamSynchronize(r->stream));
+  return XB_OK;
+}
+
+int xb_guide_set_params(xb_renderer* r, const float* params) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!params) return set_err(r, XB_E_INVALID, "null input");
+  if (!r->guide) return set_err(r, XB_E_STATE, "guiding was never enabled");
+  CK(cudaMemcpyAsync(xbg::guide_master(r->guide), params, xbg::kParams * sizeof(float), cudaMemcpyHostToDevice,
+                     r->stream));
+  xbg::guide_sync_bf16(r->guide, r->stream);
+  xbg::guide_reset_optimizer(r->guide, r->stream);
+  CK(cudaStreamSynchronize(r->stream));
   return XB_OK;
 }
 
@@ -1306,6 +1783,8 @@ int xb_get_profile(const xb_renderer* r_, xb_profile* out) {
   out->ext_tlas_nodes = (int64_t)s[STAT_EXT_WORK + 2]; out->ext_instances = (int64_t)s[STAT_EXT_WORK + 3];
   out->sh_blas_nodes = (int64_t)s[STAT_SH_WORK]; out->sh_tris = (int64_t)s[STAT_SH_WORK + 1];
   out->sh_tlas_nodes = (int64_t)s[STAT_SH_WORK + 2]; out->sh_instances = (int64_t)s[STAT_SH_WORK + 3];
+  out->train_ms = r->stage_ms[STAGE_TRAIN];
+  out->train_launches = r->stage_launches[STAGE_TRAIN];
   return XB_OK;
 }
 

@@ -60,6 +60,17 @@ SIGNATURES = {
     "xb_bsdf_eval": ([_P, _I64, _P, _P, _P, _P], _I),
     "xb_bsdf_sample": ([_P, _I64, _P, _P, _P, _P, _P, _P], _I),
     "xb_tc_gemm_bf16": ([_P, _P, _I64, _I32, _P], _I),
+    "xb_set_guiding": ([_P, _P], _I),
+    "xb_get_guiding": ([_P, _P], _I),
+    "xb_get_guiding_stats": ([_P, _P], _I),
+    "xb_guide_get_params": ([_P, _P], _I),
+    "xb_guide_set_params": ([_P, _P], _I),
+    "xb_guide_init_params": ([ctypes.c_uint64, _P], _I),
+    "xb_guide_forward": ([_P, _P, _I64, _P], _I),
+    "xb_guide_loss_grad": ([_P, _P, _I64, _P, _P], _I),
+    "xb_guide_train": ([_P, _P, _I64, _I32, _I32, _F, ctypes.c_uint64, _P, _P], _I),
+    "xb_guide_mixture_pdf": ([_P, _I64, _P, _P], _I),
+    "xb_guide_mixture_sample": ([_P, _I64, _P, _P, _P], _I),
 }
 
 _lib = None

@@ -132,11 +132,11 @@ def cornell(width: int = 256, height: int = 256, spp: int = 64, max_bounces: int
                                                   emission=(17.0, 12.0, 4.0)))
     L = 10.0
     # box spans x,z in [-5, 5], y in [0, 10]; normals point inward
-    d.add_mesh(quad_mesh((-5, 0, 5), (0, 0, -L), (L, 0, 0), white))       # floor   n=+y
-    d.add_mesh(quad_mesh((-5, L, -5), (0, 0, L), (L, 0, 0), white))       # ceiling n=-y
-    d.add_mesh(quad_mesh((-5, 0, -5), (0, L, 0), (L, 0, 0), white))       # back    n=+z
-    d.add_mesh(quad_mesh((-5, 0, 5), (0, L, 0), (0, 0, -L), red))         # left    n=+x
-    d.add_mesh(quad_mesh((5, 0, -5), (0, L, 0), (0, 0, L), green))        # right   n=-x
+    d.add_mesh(quad_mesh((-5, 0, 5), (L, 0, 0), (0, 0, -L), white))       # floor   n=+y
+    d.add_mesh(quad_mesh((-5, L, -5), (L, 0, 0), (0, 0, L), white))       # ceiling n=-y
+    d.add_mesh(quad_mesh((-5, 0, -5), (L, 0, 0), (0, L, 0), white))       # back    n=+z
+    d.add_mesh(quad_mesh((-5, 0, 5), (0, 0, -L), (0, L, 0), red))         # left    n=+x
+    d.add_mesh(quad_mesh((5, 0, -5), (0, 0, L), (0, L, 0), green))        # right   n=-x
     d.add_mesh(box_mesh((1.6, 1.5, 1.2), (3, 3, 3), 18.0, white))
     d.add_mesh(box_mesh((-1.7, 3.0, -1.5), (3, 6, 3), -15.0, white))
     s = 2.5
@@ -340,22 +340,24 @@ def guiding_room(level: int = 7, width: int = 1280, height: int = 720, max_bounc
                  spp: int = 64) -> SceneDesc:
     """Config 4: closed 10x10x10 diffuse room (albedo 0.7), the only light an emissive quad of
     0.5 units^2 (0.5 % of the ceiling) hidden above a diffuse baffle, and a smooth glass sphere
-    mesh (IOR 1.5, roughness 0 → delta). Level 7 = 327,680 tris; level 8 = 1.31 M."""
+    mesh (IOR 1.5, roughness 0 → delta). Level 7 = 327,680 tris; level 8 = 1.31 M.
+    The walls have IOR 1 (F0 = 0): a purely Lambertian BSDF whose sampled and evaluated forms
+    agree, so the guided and the plain estimator converge to the same image."""
     d = SceneDesc(name="guiding_room", width=width, height=height, spp=spp, max_bounces=max_bounces)
-    wall = d.add_material("wall", abi.material(base_color=(0.7, 0.7, 0.7), roughness=1.0))
+    wall = d.add_material("wall", abi.material(base_color=(0.7, 0.7, 0.7), roughness=1.0, ior=1.0))
     glass = d.add_material("glass", abi.material(base_color=(1.0, 1.0, 1.0), transmission=1.0, ior=1.5,
                                                  roughness=0.0))
     lightm = d.add_material("light", abi.material(base_color=(0.8, 0.8, 0.8), emission=(400.0, 380.0, 340.0)))
     L = 10.0
-    d.add_mesh(quad_mesh((-5, 0, 5), (0, 0, -L), (L, 0, 0), wall))       # floor
-    d.add_mesh(quad_mesh((-5, L, -5), (0, 0, L), (L, 0, 0), wall))       # ceiling
-    d.add_mesh(quad_mesh((-5, 0, -5), (0, L, 0), (L, 0, 0), wall))       # back
-    d.add_mesh(quad_mesh((-5, 0, 5), (0, L, 0), (0, 0, -L), wall))       # left
-    d.add_mesh(quad_mesh((5, 0, -5), (0, L, 0), (0, 0, L), wall))        # right
-    d.add_mesh(quad_mesh((5, 0, 5), (0, L, 0), (-L, 0, 0), wall))        # front (n=-z)
+    d.add_mesh(quad_mesh((-5, 0, 5), (L, 0, 0), (0, 0, -L), wall))       # floor   n=+y
+    d.add_mesh(quad_mesh((-5, L, -5), (L, 0, 0), (0, 0, L), wall))       # ceiling n=-y
+    d.add_mesh(quad_mesh((-5, 0, -5), (L, 0, 0), (0, L, 0), wall))       # back    n=+z
+    d.add_mesh(quad_mesh((-5, 0, 5), (0, 0, -L), (0, L, 0), wall))       # left    n=+x
+    d.add_mesh(quad_mesh((5, 0, -5), (0, 0, L), (0, L, 0), wall))        # right   n=-x
+    d.add_mesh(quad_mesh((5, 0, 5), (-L, 0, 0), (0, L, 0), wall))        # front   n=-z
     # baffle: horizontal panel under the light, both sides facing out
-    d.add_mesh(quad_mesh((2.0, 8.5, -4.0), (0, 0, 3.0), (2.8, 0, 0), wall))   # faces down
-    d.add_mesh(quad_mesh((2.0, 8.52, -4.0), (2.8, 0, 0), (0, 0, 3.0), wall))  # faces up
+    d.add_mesh(quad_mesh((2.0, 8.5, -4.0), (2.8, 0, 0), (0, 0, 3.0), wall))   # n=-y (faces the room)
+    d.add_mesh(quad_mesh((2.0, 8.52, -4.0), (0, 0, 3.0), (2.8, 0, 0), wall))  # n=+y (faces the light)
     s = 0.5 ** 0.5
     lm = d.add_mesh(quad_mesh((3.4 - s / 2, L - 0.01, -2.5 - s / 2), (s, 0, 0), (0, 0, s), lightm))
     for tri in (0, 1):
