@@ -56,6 +56,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--thread-per-ray", action="store_true", help="one-ray-per-thread traversal kernels")
+    ap.add_argument("--no-guiding-study", action="store_true", help="skip the config-4 guided vs plain study")
+    ap.add_argument("--guide-seconds", type=float, default=6.0, help="equal device-time budget per method")
+    ap.add_argument("--guide-ref-spp", type=int, default=2048, help="samples of the plain FP64 reference")
+    ap.add_argument("--guide-width", type=int, default=1280)
+    ap.add_argument("--guide-height", type=int, default=720)
     return ap.parse_args()
 
 
@@ -253,6 +258,82 @@ def reference_line(args) -> dict:
     return line
 
 
+def guiding_study(args, device: int) -> dict:
+    """Config 4: equal device-time relMSE of the guided and the plain wavefront against a plain
+    FP64 reference. Both methods render in chunks of samples until their summed device time
+    (CUDA events of each xb_render call) reaches the budget; the guided budget includes its
+    online training (the first train_spp samples, which are part of its image)."""
+    import xenon_b200 as xb
+    from xenon_b200 import scenes
+    W, H = args.guide_width, args.guide_height
+    desc = scenes.guiding_room(level=7, width=W, height=H)
+    hs = xb.HostScene.from_desc(desc)
+    cam = xb.camera(desc.eye, desc.target, desc.fov, W / H)
+    eps = 1e-2
+
+    def renderer(fp64=False):
+        r = xb.Renderer(W, H, desc.max_bounces, desc.min_bounces, device=device, fp64=fp64)
+        r.upload_scene(hs)
+        return r
+
+    t0 = time.perf_counter()
+    rr = renderer(fp64=True)
+    ref_ms = 0.0
+    done = 0
+    ref_first = 1 << 24            # sample indices disjoint from the compared renders (1, 2, ...)
+    while done < args.guide_ref_spp:
+        n = min(256, args.guide_ref_spp - done)
+        rr.render_range(cam, ref_first + done, n)
+        ref_ms += rr.stats().last_ms
+        done += n
+    s64, m2 = rr.resolve_fp64()
+    ref = s64 / done
+    ref_var = m2 / max(done - 1, 1)
+    rr.close()
+    denom = ref ** 2 + eps
+    ref_err = float(np.mean(ref_var / done / denom))   # the reference's own expected relMSE
+
+    def equal_time(guided: bool) -> dict:
+        r = renderer()
+        info = {}
+        if guided:
+            r.set_guiding(True, train_spp=64, steps_per_spp=32, batch=16384, guide_fraction=0.7)
+        ms, rendered, chunk = 0.0, 0, 8
+        while ms < args.guide_seconds * 1e3:
+            r.render_frame(cam, chunk)
+            ms += r.stats().last_ms
+            rendered += chunk
+            if guided and rendered == 64:
+                info["train_phase_ms"] = ms
+        spp = r.spp                              # image samples (training samples excluded)
+        img = r.resolve().astype(np.float64)
+        if guided:
+            info.update(r.guiding_stats())
+            info["config"] = {k: v for k, v in r.guiding().items() if k in
+                              ("train_spp", "steps_per_spp", "batch", "learning_rate", "guide_fraction")}
+        r.close()
+        e = (img - ref) ** 2 / denom
+        pix = e.mean(2).ravel()
+        trimmed = np.sort(pix)[: int(len(pix) * 0.999)]
+        return {"spp": spp, "samples_rendered": rendered, "device_ms": ms, "relmse": float(pix.mean()),
+                "relmse_minus_reference_noise": float(pix.mean()) - ref_err,
+                "relmse_trimmed_0.1pct": float(trimmed.mean()), "image_mean": float(img.mean()), **info}
+
+    plain = equal_time(False)
+    guided = equal_time(True)
+    return {"workload": "config4: closed room, light above a baffle, smooth glass icosphere L7 "
+                        f"(327,680 tris), {W}x{H}, depth 16",
+            "budget_device_s": args.guide_seconds, "reference": {"spp": done, "device_ms": ref_ms,
+                                                               "image_mean": float(ref.mean()),
+                                                               "expected_relmse": ref_err},
+            "plain": plain, "guided": guided,
+            "relmse_ratio_plain_over_guided": plain["relmse"] / max(guided["relmse"], 1e-30),
+            "relmse_ratio_reference_noise_removed": plain["relmse_minus_reference_noise"] /
+                max(guided["relmse_minus_reference_noise"], 1e-30),
+            "relmse_ratio_trimmed": plain["relmse_trimmed_0.1pct"] / max(guided["relmse_trimmed_0.1pct"], 1e-30),
+            "wall_s": time.perf_counter() - t0}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -381,6 +462,13 @@ def main():
             cpu = {"value": None, "unit": "Mrays/s", "cores": None, "kind": "reference",
                    "sample": f"failed: {e}"}
 
+    guiding = None
+    if rank == 0 and ws == 1 and not args.no_guiding_study:
+        try:
+            guiding = guiding_study(args, local)
+        except Exception as e:
+            guiding = {"error": f"{type(e).__name__}: {e}"}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
@@ -393,7 +481,7 @@ def main():
                            "stage_ms_per_step": {k: getattr(prof, k) / args.steps for k in
                                                  ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms")}},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary()}
+                "clocks": clk.summary(), "guiding": guiding}
         print(json.dumps(line))
     r.close()
     if ws > 1:

@@ -269,7 +269,9 @@ int  xb_last_error(const xb_renderer *r, char *buf, size_t len);
 int  xb_upload_scene(xb_renderer *r, const xb_scene_view *view);
 int  xb_set_bounces(xb_renderer *r, int32_t min_bounces, int32_t max_bounces);
 /* Adds spp_to_add samples per pixel; sample k of pixel p is seeded exactly as the CPU backend
- * seeds it (seed_pcg(p + k * 0xdeadbeef), src/render/cpu_tiled.cpp:22-23). */
+ * seeds it (seed_pcg(p + k * 0xdeadbeef), src/render/cpu_tiled.cpp:22-23). With guiding on, the
+ * samples that train the network are left out of the image unless keep_training_samples is set;
+ * xb_get_spp then counts the image's samples. */
 int  xb_render(xb_renderer *r, const xb_camera *cam, int32_t spp_to_add);
 /* Mean radiance, float[W*H*3], top-down rows. */
 int  xb_resolve(xb_renderer *r, float *out_rgb);
@@ -376,12 +378,14 @@ typedef struct xb_guiding {
   int32_t steps_per_spp;    /* Adam steps per training sample per pixel; default 32 */
   int32_t batch;            /* records per Adam step (multiple of 128); default 16384 */
   float learning_rate;      /* default 5e-3 */
-  float guide_fraction;     /* probability of sampling the network; default 0.5 */
+  float guide_fraction;     /* probability of sampling the network; default 0.7 */
   int32_t max_records;      /* training records kept per wave; default 1 << 21 */
   int32_t record_stride;    /* record the vertices of one path in this many; 0 = automatic */
   uint64_t seed;            /* initial weights and batch windows */
   float bounds_min[3];      /* box mapped to [0,1]^3 for the network's position input; */
   float bounds_max[3];      /* an empty box selects the scene's bounds */
+  int32_t keep_training_samples;  /* 0: samples 1..train_spp train the network only and stay out
+                                   * of the image (xb_get_spp counts image samples) */
 } xb_guiding;
 
 /* Enables, disables or reconfigures guiding (0 fields take defaults). The first enabling, or a

@@ -29,19 +29,21 @@ def _render(sc, cam, spp, guided, bounces=16, **kw):
     if guided:
         r.set_guiding(True, **kw)
     r.render_frame(cam, spp)
+    n = r.spp                     # samples in the image (training samples stay out of it)
     s, m2 = r.resolve_fp64()
     stats = r.stats()
     gst = r.guiding_stats() if guided else None
     r.close()
-    return s / spp, m2 / max(spp - 1, 1), stats, gst
+    return s / n, m2 / max(n - 1, 1), stats, gst
 
 
-def _agree(mp, vp, mg, vg, spp, heavy_tailed):
+def _agree(mp, vp, mg, vg, spp, heavy_tailed, spp_g=None):
+    spp_g = spp_g or spp
     lg, lp = mg.mean(2), mp.mean(2)
-    z = (lg - lp) / (np.sqrt(vg.mean(2) / spp + vp.mean(2) / spp) + 1e-12)
+    z = (lg - lp) / (np.sqrt(vg.mean(2) / spp_g + vp.mean(2) / spp) + 1e-12)
     if not heavy_tailed:
         d = mg.sum() - mp.sum()
-        se = np.sqrt(vg.sum() / spp + vp.sum() / spp)
+        se = np.sqrt(vg.sum() / spp_g + vp.sum() / spp)
         assert abs(d) < 4.5 * se, (mg.mean(), mp.mean(), d / se)
         assert np.mean(np.abs(z) > 4) < 0.002
     else:
@@ -63,7 +65,7 @@ def test_guided_converges_to_the_plain_image(sphere, bounces):
         assert stp.nonfinite == 0 and stg.nonfinite == 0
         if kw["train_spp"] > 0:
             assert gst["adam_steps"] == 64 * 8 and gst["records"] > 0 and np.isfinite(gst["last_loss"])
-        _agree(mp, vp, mg, vg, spp, heavy_tailed=sphere)
+        _agree(mp, vp, mg, vg, spp, heavy_tailed=sphere, spp_g=spp - max(kw["train_spp"], 0))
 
 
 @pytest.mark.gpu
@@ -108,10 +110,13 @@ def test_guide_params_round_trip_and_stats():
     r.render_frame(cam, 4)
     st = r.guiding_stats()
     assert st["adam_steps"] == 6 and st["training"] == 0
+    assert r.spp == 2                          # samples 1-2 trained the network only
+    r.render_frame(cam, 3)                     # continues with samples 5-7, no more training
+    assert r.spp == 5 and r.guiding_stats()["adam_steps"] == 6
     p1 = r.guide_params()
     assert not np.array_equal(p0, p1)
     r.set_guide_params(p0)
     assert np.array_equal(r.guide_params(), p0)
     g = r.guiding()
-    assert g["enabled"] == 1 and g["train_spp"] == 2 and abs(g["guide_fraction"] - 0.5) < 1e-7
+    assert g["enabled"] == 1 and g["train_spp"] == 2 and abs(g["guide_fraction"] - 0.7) < 1e-7
     r.close()

@@ -114,7 +114,8 @@ struct xb_renderer {
   double* sum64 = nullptr;                // FP64 sum (flag)
   double* m2_64 = nullptr;                // Welford M2 (flag)
   double* mean64 = nullptr;
-  int spp = 0;
+  int spp = 0;                            // samples in the image
+  int next_sample = 1;                    // index of the next sample xb_render renders
   float* resolve_buf = nullptr;
   WaveBuffers wb;
   int spp_per_wave = 1;
@@ -1121,7 +1122,11 @@ void collect_stage_times(xb_renderer* r) {
   r->ev_used = 0;
 }
 
-int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count) {
+// Renders samples [spp_first, spp_first + spp_count) and returns, in *kept_out, how many of
+// them went into the image.
+int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count, int* kept_out) {
+  int kept = 0;
+  *kept_out = 0;
   const int W = r->cfg.width, H = r->cfg.height;
   const int64_t npix = (int64_t)W * H;
   CamDev cd{v3(cam->eye[0], cam->eye[1], cam->eye[2]),
@@ -1241,8 +1246,13 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
     const int g_acc = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)r->num_sms * 16);
     {
       StageTimer t(r, STAGE_ACCUM);
-      accumulate_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, npix, spw, r->spp + done, r->accum, r->sum64,
-                                                      r->m2_64, r->mean64, w.cnt, depth_max, paths, r->stats);
+      // samples rendered while the guide trains stay out of the image unless asked for (their
+      // proposal is the still-untrained network); the kernel still counts the wave's rays
+      const bool keep = !train || r->gcfg.keep_training_samples != 0;
+      accumulate_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, npix, keep ? spw : 0, r->spp + kept, r->accum,
+                                                      r->sum64, r->m2_64, r->mean64, w.cnt, depth_max, paths,
+                                                      r->stats);
+      if (keep) kept += spw;
     }
     if (train) {
       StageTimer t(r, STAGE_TRAIN);
@@ -1257,6 +1267,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
     CK(cudaGetLastError());
     done += spw;
   }
+  *kept_out = kept;
   return XB_OK;
 }
 
@@ -1554,6 +1565,7 @@ int xb_reset(xb_renderer* r) {
     CK(cudaMemsetAsync(r->mean64, 0, npix * 3 * sizeof(double), r->stream));
   }
   r->spp = 0;
+  r->next_sample = 1;
   CK(cudaStreamSynchronize(r->stream));
   return XB_OK;
 }
@@ -1568,10 +1580,12 @@ int xb_render_range(xb_renderer* r, const xb_camera* cam, int32_t spp_first, int
   unsigned long long ov_before = 0;
   CK(cudaMemcpyAsync(&ov_before, r->stats + STAT_OVERFLOW, sizeof(ov_before), cudaMemcpyDeviceToHost, r->stream));
   CK(cudaEventRecord(r->ev0, r->stream));
-  rc = run_waves(r, cam, spp_first, spp_count);
+  int kept = 0;
+  rc = run_waves(r, cam, spp_first, spp_count, &kept);
   if (rc) return rc;
   CK(cudaEventRecord(r->ev1, r->stream));
-  r->spp += spp_count;
+  r->spp += kept;
+  r->next_sample = std::max(r->next_sample, spp_first + spp_count);
   unsigned long long ov_after = 0;
   CK(cudaMemcpyAsync(&ov_after, r->stats + STAT_OVERFLOW, sizeof(ov_after), cudaMemcpyDeviceToHost, r->stream));
   CK(cudaStreamSynchronize(r->stream));
@@ -1584,7 +1598,7 @@ int xb_render_range(xb_renderer* r, const xb_camera* cam, int32_t spp_first, int
 
 int xb_render(xb_renderer* r, const xb_camera* cam, int32_t spp_to_add) {
   if (!r) return xb::fail(XB_E_INVALID, "null renderer");
-  return xb_render_range(r, cam, r->spp + 1, spp_to_add);
+  return xb_render_range(r, cam, r->next_sample, spp_to_add);
 }
 
 int xb_resolve(xb_renderer* r, float* out) {
@@ -1672,7 +1686,7 @@ int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
   if (c.steps_per_spp == 0) c.steps_per_spp = 32;
   if (c.batch == 0) c.batch = 16384;
   if (c.learning_rate == 0.f) c.learning_rate = 5e-3f;
-  if (c.guide_fraction == 0.f) c.guide_fraction = 0.5f;
+  if (c.guide_fraction == 0.f) c.guide_fraction = 0.7f;
   if (c.max_records == 0) c.max_records = 1 << 21;
   if (c.seed == 0) c.seed = 1;
   if (c.train_spp < -1 || c.steps_per_spp < 0 || c.steps_per_spp > xbg::kMaxTrainSteps || c.batch < 0 ||
@@ -1721,7 +1735,7 @@ int xb_get_guiding_stats(const xb_renderer* r_, xb_guiding_stats* out) {
   out->records = (int64_t)s[STAT_REC_TOTAL];
   out->records_dropped = (int64_t)s[STAT_REC_DROPPED];
   out->last_loss = loss;
-  out->training = (r->guiding && r->spp < r->gcfg.train_spp) ? 1 : 0;
+  out->training = (r->guiding && r->next_sample <= r->gcfg.train_spp) ? 1 : 0;
   if (r->guide) {
     int herr = 0;
     CK(cudaMemcpy(&herr, xbg::guide_error(r->guide), sizeof(int), cudaMemcpyDeviceToHost));
