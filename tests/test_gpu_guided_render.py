@@ -62,7 +62,8 @@ def test_guided_converges_to_the_plain_image(sphere, bounces):
     mp, vp, stp, _ = _render(sc, cam, spp, False, bounces)
     for kw in (dict(train_spp=-1), dict(train_spp=64, steps_per_spp=8, batch=4096)):
         mg, vg, stg, gst = _render(sc, cam, spp, True, bounces, **kw)
-        assert stp.nonfinite == 0 and stg.nonfinite == 0
+        # non-finite samples are dropped from the image and counted; they must stay rare
+        assert stp.nonfinite <= 1e-6 * stp.paths and stg.nonfinite <= 1e-6 * stg.paths
         if kw["train_spp"] > 0:
             assert gst["adam_steps"] == 64 * 8 and gst["records"] > 0 and np.isfinite(gst["last_loss"])
         _agree(mp, vp, mg, vg, spp, heavy_tailed=sphere, spp_g=spp - max(kw["train_spp"], 0))

@@ -59,22 +59,25 @@ __device__ __forceinline__ void load_forward_weights(uint8_t* sW, float* sBias, 
 
 // The 64 input features of one row into the A tile: sin/cos(2^k pi x) of the position in
 // [0,1]^3 (k < 6), the normal (k < 2) and the outgoing direction (k < 2), then p xyz and 1.
-// f: p01 xyz, n xyz, wo xyz.
+// f: p01 xyz, n xyz, wo xyz. One sincospif per coordinate; the higher octaves follow from the
+// double-angle identities sin 2a = 2 sin a cos a, cos 2a = 1 - 2 sin^2 a (error doubling per
+// octave stays far below the bf16 rounding of the result).
 __device__ __forceinline__ void encode_row(const float* f, uint8_t* tile, int r) {
   float x[kIn];
-  int o = 0;
 #pragma unroll
-  for (int g = 0; g < 3; ++g) {
-    const int nf = g == 0 ? 6 : 2;
+  for (int c = 0; c < 9; ++c) {
+    const int nf = c < 3 ? 6 : 2;
+    const int o = c < 3 ? 12 * c : 36 + 4 * (c - 3);
+    float s, co;
+    sincospif(f[c], &s, &co);
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int k = 0; k < nf; ++k) {
-        float s, c;
-        sincospif((float)(1 << k) * f[3 * g + a], &s, &c);
-        x[o++] = s;
-        x[o++] = c;
-      }
+    for (int k = 0; k < nf; ++k) {
+      x[o + 2 * k] = s;
+      x[o + 2 * k + 1] = co;
+      const float s2 = 2.f * s * co;
+      co = 1.f - 2.f * s * s;
+      s = s2;
+    }
   }
   x[60] = f[0]; x[61] = f[1]; x[62] = f[2]; x[63] = 1.f;
 #pragma unroll
@@ -163,6 +166,7 @@ __device__ __forceinline__ void hidden_epilogue(const Mma& m, const float* bias,
 __device__ __forceinline__ void forward_tile(Mma& m, uint8_t* sA, const uint8_t* sW, const float* sBias,
                                              float* raw) {
   const uint32_t aA = xbd::smem_u32(sA);
+#pragma unroll 1
   for (int l = 0; l < 3; ++l) {
     m.sync_before();
     m.run(aA, xbd::smem_u32(sW + l * kWBytes), kK, kHid);
@@ -209,28 +213,44 @@ __device__ __forceinline__ float vmf_norm(float kappa) {
   return kappa / (2.f * kGuidePi * (-expm1f(-2.f * kappa)));
 }
 
-// Mixture pdf (per steradian) of the unit direction (x, y, z); lobes at stride 5.
-__device__ __forceinline__ float mix_pdf(const float* lob, float x, float y, float z) {
+// Lobes prepared for evaluation, kPrepFloats per lobe: mu xyz, kappa, weight, and
+// weight * vmf_norm(kappa) (the lobe's density at its mean direction, times its weight).
+constexpr int kPrepFloats = 6;
+constexpr int kPrepRow = kLobes * kPrepFloats;
+
+__device__ __forceinline__ void prepare_lobes(const float* lob5, float* out) {
+#pragma unroll
+  for (int k = 0; k < kLobes; ++k) {
+    const float* L = lob5 + 5 * k;
+    float* o = out + kPrepFloats * k;
+    o[0] = L[0]; o[1] = L[1]; o[2] = L[2]; o[3] = L[3]; o[4] = L[4];
+    o[5] = L[4] * vmf_norm(L[3]);
+  }
+}
+
+// Mixture pdf (per steradian) of the unit direction (x, y, z):
+//   q = sum_k w_k kappa_k / (2 pi (1 - e^{-2 kappa_k})) e^{kappa_k (mu_k . w - 1)}
+__device__ __forceinline__ float mix_pdf(const float* P, float x, float y, float z) {
   float q = 0.f;
 #pragma unroll
   for (int k = 0; k < kLobes; ++k) {
-    const float* L = lob + 5 * k;
+    const float* L = P + kPrepFloats * k;
     const float c = L[0] * x + L[1] * y + L[2] * z;
-    q += L[4] * vmf_norm(L[3]) * expf(L[3] * (c - 1.f));
+    q += L[5] * expf(L[3] * (c - 1.f));
   }
   return q;
 }
 
 // A direction from the mixture: u0 picks the lobe by its weight, u1 the angle to the mean
 // (inverse CDF of the vMF: cos = 1 + log(u1 + (1 - u1) e^{-2 kappa}) / kappa), u2 the azimuth.
-__device__ __forceinline__ void mix_sample(const float* lob, float u0, float u1, float u2, float* d) {
+__device__ __forceinline__ void mix_sample(const float* P, float u0, float u1, float u2, float* d) {
   int k = 0;
-  float cdf = lob[4];
+  float cdf = P[4];
   while (k < kLobes - 1 && u0 > cdf) {
     ++k;
-    cdf += lob[5 * k + 4];
+    cdf += P[kPrepFloats * k + 4];
   }
-  const float* L = lob + 5 * k;
+  const float* L = P + kPrepFloats * k;
   const float kp = L[3];
   float c = 1.f + logf(u1 + (1.f - u1) * expf(-2.f * kp)) / kp;
   c = fminf(fmaxf(c, -1.f), 1.f);

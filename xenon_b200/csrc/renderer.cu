@@ -512,7 +512,7 @@ struct GuideShadeArgs {
 };
 
 constexpr float kNaN = __builtin_nanf("");
-constexpr int kLobStride = xbg::kLobeFloats + 1;   // conflict-free per-thread rows
+constexpr int kLobStride = xbg::kPrepRow + 1;   // conflict-free per-thread rows
 constexpr size_t kGuidedShadeSmem =
     xbg::kFwdWeightBytes + xbg::kTileBytes + (size_t)xbg::kTile * kLobStride * 4 + 1024;
 
@@ -612,8 +612,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
       if (!m.ok) break;   // uniform: every thread saw the same failed wait
       float lo[xbg::kLobeFloats];
       xbg::raw_to_lobes(raw, lo);
-#pragma unroll
-      for (int i = 0; i < xbg::kLobeFloats; ++i) lob[i] = lo[i];
+      xbg::prepare_lobes(lo, lob);
     }
     // ── phase 2: NEE, roulette, the next direction (cpu_tiled.cpp:89-216) ──
     if (alive) do {
