@@ -273,6 +273,22 @@ int  xb_set_bounces(xb_renderer *r, int32_t min_bounces, int32_t max_bounces);
  * samples that train the network are left out of the image unless keep_training_samples is set;
  * xb_get_spp then counts the image's samples. */
 int  xb_render(xb_renderer *r, const xb_camera *cam, int32_t spp_to_add);
+/* Many views in one call (config 5: dozens of cameras, 256^2 to 1024^2 pixels, 16 to 1024
+ * samples): the views share the renderer's scene and bounce limits and are packed together into
+ * the same waves, so small views still fill the GPU. Each view renders samples 1..spp, seeded as
+ * a render of that view alone (seed_pcg(p + k * 0xdeadbeef)), so its image equals a
+ * single-view render of the same size; out_rgb receives the view's mean image (host memory,
+ * float[width*height*3], top-down rows). The renderer's own accumulation is untouched. With
+ * guiding on, views use the current network without training it. No reference counterpart:
+ * the reference renders one view per CudaRenderer. */
+typedef struct xb_view {
+  xb_camera camera;
+  int32_t width, height;
+  int32_t spp;
+  int32_t reserved;        /* 0 */
+  float *out_rgb;
+} xb_view;
+int  xb_render_views(xb_renderer *r, const xb_view *views, int32_t count);
 /* Mean radiance, float[W*H*3], top-down rows. */
 int  xb_resolve(xb_renderer *r, float *out_rgb);
 /* FP64 per-pixel sums and Welford M2 (needs XB_FLAG_FP64_ACCUM); each double[W*H*3]. */

@@ -153,6 +153,20 @@ class Renderer:
     def render_range(self, cam: abi.Camera, spp_first: int, spp_count: int) -> None:
         self._check(lib().xb_render_range(self.h, ctypes.byref(cam), int(spp_first), int(spp_count)))
 
+    def render_views(self, views) -> list:
+        """xb_render_views: views = [(camera, width, height, spp), ...] rendered together in shared
+        waves; returns each view's mean image (height, width, 3), top-down rows."""
+        arr = (abi.View * len(views))()
+        outs = []
+        for i, (cam, w, h, spp) in enumerate(views):
+            o = np.empty((h, w, 3), np.float32)
+            outs.append(o)
+            arr[i].camera = cam
+            arr[i].width, arr[i].height, arr[i].spp = int(w), int(h), int(spp)
+            arr[i].out_rgb = o.ctypes.data
+        self._check(lib().xb_render_views(self.h, arr, len(views)))
+        return outs
+
     def resolve(self, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:
             out = np.empty((self.height, self.width, 3), np.float32)

@@ -770,6 +770,99 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
   xbg::mma_teardown(m.tmem);
 }
 
+// ── many views: raygen and accumulation over a table of pieces ────────────────────
+constexpr int kMaxPieces = 64;
+struct ViewPiece {
+  CamDev cam;
+  int W, H;
+  int s_first, spp;        // 1-based first sample index, samples of every pixel in this wave
+  int64_t path_off;        // first path of the piece in the wave
+  int64_t pix_off;         // first pixel of the piece in the wave's pixel list
+  int64_t accum_off;       // first pixel of the view in the accumulation buffer
+};
+struct ViewPieces {
+  int n;
+  ViewPiece p[kMaxPieces];
+};
+
+__global__ void raygen_views_kernel(ViewPieces pk, int64_t paths, float4* ray_o, float4* ray_d, float4* tp,
+                                    uint64_t* rng, int32_t* path, float4* L, int32_t* cnt) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < paths;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    int i = 0;
+    while (i + 1 < pk.n && p >= pk.p[i + 1].path_off) ++i;
+    const ViewPiece& v = pk.p[i];
+    const int64_t npix = (int64_t)v.W * v.H;
+    const int64_t local = p - v.path_off;
+    const int64_t pixel = local % npix;
+    const int64_t s = v.s_first + local / npix;
+    const int x = (int)(pixel % v.W), y = (int)(pixel / v.W);
+    // cpu_tiled.cpp:20-32, as raygen_kernel
+    Pcg g{pcg_seed_state((uint64_t)pixel + (uint64_t)s * 0xdeadbeefULL)};
+    const float u = (float)x + g.next_float();
+    const float vv = (float)y + g.next_float();
+    const float su = u / (float)v.W, sv = vv / (float)v.H;
+    const V3 d = normalize(v.cam.ll + su * v.cam.hor + sv * v.cam.ver - v.cam.eye);
+    ray_o[p] = make_float4(v.cam.eye.x, v.cam.eye.y, v.cam.eye.z, kRayEps);
+    ray_d[p] = make_float4(d.x, d.y, d.z, kInf);
+    tp[p] = make_float4(1.f, 1.f, 1.f, -1.f);
+    rng[p] = g.state;
+    path[p] = (int32_t)p;
+    L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt[CNT_RAYS] = (int32_t)paths;
+}
+
+// Adds every piece's samples, in sample order, to its view's FP32 sums (NaN guard as the
+// single-view accumulation); counts the wave's rays.
+__global__ void accumulate_views_kernel(const float4* L, ViewPieces pk, int64_t pix_total, float4* accum,
+                                        const int32_t* cnt, int max_depth, int64_t paths,
+                                        unsigned long long* stats) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < pix_total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int i = 0;
+    while (i + 1 < pk.n && q >= pk.p[i + 1].pix_off) ++i;
+    const ViewPiece& v = pk.p[i];
+    const int64_t npix = (int64_t)v.W * v.H;
+    const int64_t pixel = q - v.pix_off;
+    float4 acc = accum[v.accum_off + pixel];
+    for (int k = 0; k < v.spp; ++k) {
+      const float4 l = L[v.path_off + (int64_t)k * npix + pixel];
+      if (!(isfinite(l.x) && isfinite(l.y) && isfinite(l.z))) {
+        atomicAdd(stats + STAT_NONFINITE, 1ull);
+        continue;
+      }
+      acc.x = acc.x + l.x; acc.y = acc.y + l.y; acc.z = acc.z + l.z;
+    }
+    accum[v.accum_off + pixel] = acc;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long rays = 0, sh = 0;
+    for (int d = 0; d < max_depth; ++d) {
+      rays += (unsigned long long)cnt[d * kCntStride + CNT_RAYS];
+      sh += (unsigned long long)cnt[d * kCntStride + CNT_SH_AREA] +
+            (unsigned long long)cnt[d * kCntStride + CNT_SH_SUN];
+    }
+    atomicAdd(stats + STAT_RAYS, rays);
+    atomicAdd(stats + STAT_SHADOW, sh);
+    atomicAdd(stats + STAT_PATHS, (unsigned long long)paths);
+  }
+}
+
+// Mean of one view's sums, top-down rows (cpu_tiled.cpp:224-236).
+__global__ void resolve_view_kernel(const float4* accum, int W, int H, float inv_spp, float* out) {
+  const int64_t npix = (int64_t)W * H;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npix;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % W), y = (int)(i / W);
+    const float4 a = accum[i];
+    const int64_t d = ((int64_t)(H - 1 - y) * W + x) * 3;
+    out[d] = a.x * inv_spp;
+    out[d + 1] = a.y * inv_spp;
+    out[d + 2] = a.z * inv_spp;
+  }
+}
+
 // ── accumulate the wave into the framebuffer, in sample order ──────────────────
 __global__ void accumulate_kernel(const float4* L, int64_t npix, int spw, int spp_before,
                                   float4* accum, double* sum64, double* m2_64, double* mean64,
@@ -1121,6 +1214,105 @@ void collect_stage_times(xb_renderer* r) {
   r->ev_used = 0;
 }
 
+// Position box of the network's input: the configured one, else the scene's bounds.
+void guide_box(xb_renderer* r) {
+  const xb_guiding& gc = r->gcfg;
+  const bool boxed = gc.bounds_max[0] > gc.bounds_min[0] && gc.bounds_max[1] > gc.bounds_min[1] &&
+                     gc.bounds_max[2] > gc.bounds_min[2];
+  for (int k = 0; k < 3; ++k) {
+    const float lo = boxed ? gc.bounds_min[k] : r->scene_lo[k];
+    const float hi = boxed ? gc.bounds_max[k] : r->scene_hi[k];
+    r->gbmin[k] = lo;
+    r->gbinv[k] = hi > lo ? 1.f / (hi - lo) : 1.f;
+  }
+}
+
+// The bounce loop of one wave whose camera rays are in queue 0: for every depth, closest hits,
+// shading (plain or guided), then the area-light and sun shadow rays (cpu_tiled.cpp:34-217).
+int trace_bounces(xb_renderer* r, bool train, int rec_stride) {
+  WaveBuffers& w = r->wb;
+  const int depth_max = std::min(r->max_bounces, kMaxDepth);
+  const bool count = (r->prof_flags & XB_PROFILE_COUNT_TRAVERSAL) != 0;
+  xbg::Guide* gd = r->guiding ? r->guide : nullptr;
+  for (int d = 0; d < depth_max; ++d) {
+    const int q = d & 1, nq = q ^ 1;
+    int32_t* cd_ = w.cnt + d * kCntStride;
+    {
+      StageTimer t(r, STAGE_EXTEND);
+      if (r->thread_per_ray || d < r->ext_persistent_from) {
+        auto kern = count ? extend_kernel<true> : extend_kernel<false>;
+        kern<<<r->grid_ext, 128, 0, r->stream>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_,
+                                                 r->stats);
+      } else {
+        TraceQueue tq{w.ray_o[q], w.ray_d[q], cd_ + CNT_RAYS, cd_ + CNT_FETCH_EXT, w.hit, w.hit_inst,
+                      nullptr, nullptr, r->stats, 0};
+        auto kern = count ? extend_persistent_kernel<true> : extend_persistent_kernel<false>;
+        kern<<<r->grid_pext, 128, 0, r->stream>>>(r->scene, tq, r->refill);
+      }
+    }
+    ShadeArgs sa;
+    sa.sc = r->scene;
+    sa.ray_o = w.ray_o[q]; sa.ray_d = w.ray_d[q]; sa.tp = w.tp[q]; sa.rng = w.rng[q]; sa.path = w.path[q];
+    sa.nray_o = w.ray_o[nq]; sa.nray_d = w.ray_d[nq]; sa.ntp = w.tp[nq]; sa.nrng = w.rng[nq];
+    sa.npath = w.path[nq];
+    sa.hit = w.hit; sa.hit_inst = w.hit_inst;
+    for (int k = 0; k < 2; ++k) { sa.sh_o[k] = w.sh_o[k]; sa.sh_d[k] = w.sh_d[k]; sa.sh_c[k] = w.sh_c[k]; }
+    sa.L = w.L;
+    sa.cnt = cd_;
+    sa.cnt_next = w.cnt + (d + 1) * kCntStride;
+    sa.depth = d; sa.min_bounces = r->min_bounces; sa.max_bounces = depth_max;
+    sa.capacity = (int)w.capacity;
+    sa.stats = r->stats;
+    if (gd) {
+      GuideShadeArgs ga;
+      ga.wf = xbg::guide_weights_bf16(gd);
+      ga.master = xbg::guide_master(gd);
+      ga.alpha = r->gcfg.guide_fraction;
+      ga.ratio_in = d > 0 ? w.ratio[q] : nullptr;
+      ga.ratio_out = w.ratio[nq];
+      for (int k = 0; k < 3; ++k) { ga.bmin[k] = r->gbmin[k]; ga.binv[k] = r->gbinv[k]; }
+      ga.recs = train ? xbg::guide_records(gd) : nullptr;
+      ga.rec_count = xbg::guide_record_count(gd);
+      ga.rec_cap = xbg::guide_record_capacity(gd);
+      ga.rec_stride = rec_stride;
+      ga.rec_in = (train && d > 0) ? w.rec[q] : nullptr;
+      ga.rec_out = train ? w.rec[nq] : nullptr;
+      ga.err = xbg::guide_error(gd);
+      StageTimer t(r, STAGE_SHADE);
+      guided_shade_kernel<<<r->grid_gshade, 128, kGuidedShadeSmem, r->stream>>>(sa, ga);
+    } else {
+      StageTimer t(r, STAGE_SHADE);
+      shade_kernel<<<r->grid_shade, 128, 0, r->stream>>>(sa);
+    }
+    for (int k = 0; k < 2; ++k) {
+      if (k == 0 && r->scene.num_lights == 0) continue;
+      if (k == 1 && r->scene.num_suns == 0) continue;
+      StageTimer t(r, STAGE_SHADOW);
+      if (r->thread_per_ray || !r->shadow_persistent) {
+        auto kern = count ? shadow_kernel<true> : shadow_kernel<false>;
+        kern<<<r->grid_shadow, 128, 0, r->stream>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
+                                                    cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
+                                                    cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats,
+                                                    r->tune.shadow_order == 2);
+      } else {
+        TraceQueue tq{w.sh_o[k], w.sh_d[k], cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
+                      cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), nullptr, nullptr, w.sh_c[k], w.L,
+                      r->stats, r->tune.shadow_order == 2};
+        auto kern = count ? shadow_persistent_kernel<true> : shadow_persistent_kernel<false>;
+        kern<<<r->grid_pshadow, 128, 0, r->stream>>>(r->scene, tq, r->refill);
+      }
+    }
+  }
+  CK(cudaGetLastError());
+  return XB_OK;
+}
+
+CamDev cam_dev(const xb_camera& c) {
+  return CamDev{v3(c.eye[0], c.eye[1], c.eye[2]), v3(c.lower_left[0], c.lower_left[1], c.lower_left[2]),
+                v3(c.horizontal[0], c.horizontal[1], c.horizontal[2]),
+                v3(c.vertical[0], c.vertical[1], c.vertical[2])};
+}
+
 // Renders samples [spp_first, spp_first + spp_count) and returns, in *kept_out, how many of
 // them went into the image.
 int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count, int* kept_out) {
@@ -1128,26 +1320,12 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
   *kept_out = 0;
   const int W = r->cfg.width, H = r->cfg.height;
   const int64_t npix = (int64_t)W * H;
-  CamDev cd{v3(cam->eye[0], cam->eye[1], cam->eye[2]),
-            v3(cam->lower_left[0], cam->lower_left[1], cam->lower_left[2]),
-            v3(cam->horizontal[0], cam->horizontal[1], cam->horizontal[2]),
-            v3(cam->vertical[0], cam->vertical[1], cam->vertical[2])};
+  const CamDev cd = cam_dev(*cam);
   WaveBuffers& w = r->wb;
   const int depth_max = std::min(r->max_bounces, kMaxDepth);
   int done = 0;
   xbg::Guide* gd = r->guiding ? r->guide : nullptr;
-  if (gd) {
-    // position box of the network's input: the configured one, else the scene's bounds
-    const xb_guiding& gc = r->gcfg;
-    const bool boxed = gc.bounds_max[0] > gc.bounds_min[0] && gc.bounds_max[1] > gc.bounds_min[1] &&
-                       gc.bounds_max[2] > gc.bounds_min[2];
-    for (int k = 0; k < 3; ++k) {
-      const float lo = boxed ? gc.bounds_min[k] : r->scene_lo[k];
-      const float hi = boxed ? gc.bounds_max[k] : r->scene_hi[k];
-      r->gbmin[k] = lo;
-      r->gbinv[k] = hi > lo ? 1.f / (hi - lo) : 1.f;
-    }
-  }
+  if (gd) guide_box(r);
   while (done < spp_count) {
     const int sample0 = spp_first + done;   // 1-based index of the wave's first sample
     const bool train = gd && sample0 <= r->gcfg.train_spp;
@@ -1167,81 +1345,13 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
                                              : (int)std::max<int64_t>(1, (paths * 4 + cap - 1) / cap);
     }
     const int g_rg = (int)std::min<int64_t>((paths + 255) / 256, (int64_t)r->num_sms * 16);
-    const bool count = (r->prof_flags & XB_PROFILE_COUNT_TRAVERSAL) != 0;
     {
       StageTimer t(r, STAGE_RAYGEN);
       raygen_kernel<<<g_rg, 256, 0, r->stream>>>(cd, W, H, spp_first + done, paths, w.ray_o[0],
                                                  w.ray_d[0], w.tp[0], w.rng[0], w.path[0], w.L, w.cnt);
     }
-    for (int d = 0; d < depth_max; ++d) {
-      const int q = d & 1, nq = q ^ 1;
-      int32_t* cd_ = w.cnt + d * kCntStride;
-      {
-        StageTimer t(r, STAGE_EXTEND);
-        if (r->thread_per_ray || d < r->ext_persistent_from) {
-          auto kern = count ? extend_kernel<true> : extend_kernel<false>;
-          kern<<<r->grid_ext, 128, 0, r->stream>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_,
-                                                   r->stats);
-        } else {
-          TraceQueue tq{w.ray_o[q], w.ray_d[q], cd_ + CNT_RAYS, cd_ + CNT_FETCH_EXT, w.hit, w.hit_inst,
-                        nullptr, nullptr, r->stats, 0};
-          auto kern = count ? extend_persistent_kernel<true> : extend_persistent_kernel<false>;
-          kern<<<r->grid_pext, 128, 0, r->stream>>>(r->scene, tq, r->refill);
-        }
-      }
-      ShadeArgs sa;
-      sa.sc = r->scene;
-      sa.ray_o = w.ray_o[q]; sa.ray_d = w.ray_d[q]; sa.tp = w.tp[q]; sa.rng = w.rng[q]; sa.path = w.path[q];
-      sa.nray_o = w.ray_o[nq]; sa.nray_d = w.ray_d[nq]; sa.ntp = w.tp[nq]; sa.nrng = w.rng[nq];
-      sa.npath = w.path[nq];
-      sa.hit = w.hit; sa.hit_inst = w.hit_inst;
-      for (int k = 0; k < 2; ++k) { sa.sh_o[k] = w.sh_o[k]; sa.sh_d[k] = w.sh_d[k]; sa.sh_c[k] = w.sh_c[k]; }
-      sa.L = w.L;
-      sa.cnt = cd_;
-      sa.cnt_next = w.cnt + (d + 1) * kCntStride;
-      sa.depth = d; sa.min_bounces = r->min_bounces; sa.max_bounces = depth_max;
-      sa.capacity = (int)w.capacity;
-      sa.stats = r->stats;
-      if (gd) {
-        GuideShadeArgs ga;
-        ga.wf = xbg::guide_weights_bf16(gd);
-        ga.master = xbg::guide_master(gd);
-        ga.alpha = r->gcfg.guide_fraction;
-        ga.ratio_in = d > 0 ? w.ratio[q] : nullptr;
-        ga.ratio_out = w.ratio[nq];
-        for (int k = 0; k < 3; ++k) { ga.bmin[k] = r->gbmin[k]; ga.binv[k] = r->gbinv[k]; }
-        ga.recs = train ? xbg::guide_records(gd) : nullptr;
-        ga.rec_count = xbg::guide_record_count(gd);
-        ga.rec_cap = xbg::guide_record_capacity(gd);
-        ga.rec_stride = rec_stride;
-        ga.rec_in = (train && d > 0) ? w.rec[q] : nullptr;
-        ga.rec_out = train ? w.rec[nq] : nullptr;
-        ga.err = xbg::guide_error(gd);
-        StageTimer t(r, STAGE_SHADE);
-        guided_shade_kernel<<<r->grid_gshade, 128, kGuidedShadeSmem, r->stream>>>(sa, ga);
-      } else {
-        StageTimer t(r, STAGE_SHADE);
-        shade_kernel<<<r->grid_shade, 128, 0, r->stream>>>(sa);
-      }
-      for (int k = 0; k < 2; ++k) {
-        if (k == 0 && r->scene.num_lights == 0) continue;
-        if (k == 1 && r->scene.num_suns == 0) continue;
-        StageTimer t(r, STAGE_SHADOW);
-        if (r->thread_per_ray || !r->shadow_persistent) {
-          auto kern = count ? shadow_kernel<true> : shadow_kernel<false>;
-          kern<<<r->grid_shadow, 128, 0, r->stream>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
-                                                      cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
-                                                      cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats,
-                                                      r->tune.shadow_order == 2);
-        } else {
-          TraceQueue tq{w.sh_o[k], w.sh_d[k], cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
-                        cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), nullptr, nullptr, w.sh_c[k], w.L,
-                        r->stats, r->tune.shadow_order == 2};
-          auto kern = count ? shadow_persistent_kernel<true> : shadow_persistent_kernel<false>;
-          kern<<<r->grid_pshadow, 128, 0, r->stream>>>(r->scene, tq, r->refill);
-        }
-      }
-    }
+    int rc = trace_bounces(r, train, rec_stride);
+    if (rc) return rc;
     const int g_acc = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)r->num_sms * 16);
     {
       StageTimer t(r, STAGE_ACCUM);
@@ -1267,6 +1377,64 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
     done += spw;
   }
   *kept_out = kept;
+  return XB_OK;
+}
+
+// ── many views in shared waves ───────────────────────────────────────────────────
+// A wave holds pieces: (view, a run of whole samples of every pixel of that view). Paths of a
+// piece are laid out sample-major like a single-view wave, so each path is seeded exactly as a
+// render of that view alone would seed it and the accumulation runs in sample order.
+int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accum, const int64_t* accum_off) {
+  WaveBuffers& w = r->wb;
+  const int depth_max = std::min(r->max_bounces, kMaxDepth);
+  xbg::Guide* gd = r->guiding ? r->guide : nullptr;
+  if (gd) guide_box(r);
+  std::vector<int> left(count);
+  for (int v = 0; v < count; ++v) left[v] = views[v].spp;
+  int v0 = 0;
+  while (v0 < count) {
+    ViewPieces pk{};
+    int64_t paths = 0;
+    int64_t pix_total = 0;
+    for (int v = v0; v < count && pk.n < kMaxPieces; ++v) {
+      if (left[v] == 0) { if (v == v0) ++v0; continue; }
+      const int64_t npix = (int64_t)views[v].width * views[v].height;
+      const int64_t room = (w.capacity - paths) / npix;
+      if (room <= 0) break;
+      const int n = (int)std::min<int64_t>(left[v], room);
+      ViewPiece& p = pk.p[pk.n++];
+      p.cam = cam_dev(views[v].camera);
+      p.W = views[v].width;
+      p.H = views[v].height;
+      p.s_first = views[v].spp - left[v] + 1;
+      p.spp = n;
+      p.path_off = paths;
+      p.pix_off = pix_total;
+      p.accum_off = accum_off[v];
+      paths += npix * n;
+      pix_total += npix;
+      left[v] -= n;
+      if (left[v] > 0) break;   // the next wave continues this view
+    }
+    while (v0 < count && left[v0] == 0) ++v0;
+    if (pk.n == 0) break;
+    CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), r->stream));
+    const int g_rg = (int)std::min<int64_t>((paths + 255) / 256, (int64_t)r->num_sms * 16);
+    {
+      StageTimer t(r, STAGE_RAYGEN);
+      raygen_views_kernel<<<g_rg, 256, 0, r->stream>>>(pk, paths, w.ray_o[0], w.ray_d[0], w.tp[0], w.rng[0],
+                                                       w.path[0], w.L, w.cnt);
+    }
+    int rc = trace_bounces(r, false, 1);
+    if (rc) return rc;
+    const int g_acc = (int)std::min<int64_t>((pix_total + 255) / 256, (int64_t)r->num_sms * 16);
+    {
+      StageTimer t(r, STAGE_ACCUM);
+      accumulate_views_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, pk, pix_total, accum, w.cnt, depth_max, paths,
+                                                            r->stats);
+    }
+    CK(cudaGetLastError());
+  }
   return XB_OK;
 }
 
@@ -1598,6 +1766,69 @@ int xb_render_range(xb_renderer* r, const xb_camera* cam, int32_t spp_first, int
 int xb_render(xb_renderer* r, const xb_camera* cam, int32_t spp_to_add) {
   if (!r) return xb::fail(XB_E_INVALID, "null renderer");
   return xb_render_range(r, cam, r->next_sample, spp_to_add);
+}
+
+int xb_render_views(xb_renderer* r, const xb_view* views, int32_t count) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!views || count <= 0 || count > 65536) return set_err(r, XB_E_INVALID, "xb_render_views: bad view list");
+  if (!r->has_scene) return set_err(r, XB_E_STATE, "xb_render_views: no scene uploaded");
+  std::vector<int64_t> off(count);
+  int64_t total = 0, max_npix = 0;
+  for (int v = 0; v < count; ++v) {
+    const xb_view& vw = views[v];
+    if (vw.width <= 0 || vw.height <= 0 || vw.spp < 0 || !vw.out_rgb ||
+        (int64_t)vw.width * vw.height > (1ll << 26))
+      return set_err(r, XB_E_INVALID, "xb_render_views: view %d has a bad size, sample count or output", v);
+    off[v] = total;
+    const int64_t npix = (int64_t)vw.width * vw.height;
+    total += npix;
+    max_npix = std::max(max_npix, npix);
+  }
+  if (max_npix > r->wb.capacity) {
+    rc = alloc_wave(r, max_npix);
+    if (rc) return rc;
+  }
+  float4* accum = nullptr;
+  float* out = nullptr;
+  if (cudaMalloc(&accum, total * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&out, max_npix * 3 * sizeof(float)) != cudaSuccess) {
+    cudaFree(accum);
+    return set_err(r, XB_E_OOM, "xb_render_views: cannot allocate %lld view pixels", (long long)total);
+  }
+  auto fail = [&](int code) { cudaStreamSynchronize(r->stream); cudaFree(accum); cudaFree(out); return code; };
+  unsigned long long ov_before = 0, ov_after = 0;
+  if (cudaMemsetAsync(accum, 0, total * sizeof(float4), r->stream) != cudaSuccess ||
+      cudaMemcpyAsync(&ov_before, r->stats + STAT_OVERFLOW, sizeof(ov_before), cudaMemcpyDeviceToHost,
+                      r->stream) != cudaSuccess ||
+      cudaEventRecord(r->ev0, r->stream) != cudaSuccess)
+    return fail(set_err(r, XB_E_CUDA, "xb_render_views: setup failed"));
+  rc = run_view_waves(r, views, count, accum, off.data());
+  if (rc) return fail(rc);
+  if (cudaEventRecord(r->ev1, r->stream) != cudaSuccess)
+    return fail(set_err(r, XB_E_CUDA, "xb_render_views: event record failed"));
+  for (int v = 0; v < count; ++v) {
+    const xb_view& vw = views[v];
+    const int64_t npix = (int64_t)vw.width * vw.height;
+    const int g = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)r->num_sms * 16);
+    resolve_view_kernel<<<g, 256, 0, r->stream>>>(accum + off[v], vw.width, vw.height,
+                                                  vw.spp > 0 ? 1.0f / (float)vw.spp : 0.f, out);
+    if (cudaMemcpyAsync(vw.out_rgb, out, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, r->stream) !=
+        cudaSuccess)
+      return fail(set_err(r, XB_E_CUDA, "xb_render_views: copy of view %d failed", v));
+  }
+  if (cudaMemcpyAsync(&ov_after, r->stats + STAT_OVERFLOW, sizeof(ov_after), cudaMemcpyDeviceToHost,
+                      r->stream) != cudaSuccess)
+    return fail(set_err(r, XB_E_CUDA, "xb_render_views: stats copy failed"));
+  cudaError_t e = cudaStreamSynchronize(r->stream);
+  if (e != cudaSuccess) return fail(set_err(r, XB_E_CUDA, "xb_render_views: %s", cudaGetErrorString(e)));
+  cudaEventElapsedTime(&r->last_ms, r->ev0, r->ev1);
+  collect_stage_times(r);
+  cudaFree(accum);
+  cudaFree(out);
+  if (ov_after != ov_before)
+    return set_err(r, XB_E_OVERFLOW, "%llu queue/stack overflows during render (work dropped)", ov_after - ov_before);
+  return XB_OK;
 }
 
 int xb_resolve(xb_renderer* r, float* out) {

@@ -383,3 +383,27 @@ def scene_bounds(desc: SceneDesc) -> tuple:
     pts = [m.positions for m in desc.meshes]
     allp = np.concatenate(pts) if pts else np.zeros((1, 3), np.float32)
     return allp.min(0), allp.max(0)
+
+
+# ── config 5 ────────────────────────────────────────────────────────────────────
+VIEW_SIZES = (256, 512, 768, 1024)
+VIEW_SPP = (16, 64, 256, 1024)
+
+
+def orbit_views(desc: SceneDesc, n: int = 32, seed: int = 1, sizes=VIEW_SIZES, spps=VIEW_SPP) -> list:
+    """Config 5: n cameras from the seed, looking at the scene's centre from random directions on
+    the upper hemisphere at 1.2-2.0 scene radii; square images of a size from `sizes` and a
+    sample count from `spps`. Returns [(eye, target, fov, width, height, spp), ...]."""
+    lo, hi = scene_bounds(desc)
+    c = (lo + hi) / 2
+    rad = float(np.linalg.norm(hi - lo)) / 2
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        d = rng.normal(size=3)
+        d[1] = abs(d[1]) + 0.2
+        d /= np.linalg.norm(d)
+        eye = c + d * rad * rng.uniform(1.2, 2.0)
+        s = int(rng.choice(sizes))
+        out.append((tuple(float(x) for x in eye), tuple(float(x) for x in c), 40.0, s, s, int(rng.choice(spps))))
+    return out
