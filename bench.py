@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--thread-per-ray", action="store_true", help="one-ray-per-thread traversal kernels")
     ap.add_argument("--no-guiding-study", action="store_true", help="skip the config-4 guided vs plain study")
+    ap.add_argument("--no-views-study", action="store_true", help="skip the config-5 batched-views comparison")
     ap.add_argument("--guide-seconds", type=float, default=6.0, help="equal device-time budget per method")
     ap.add_argument("--guide-ref-spp", type=int, default=2048, help="samples of the plain FP64 reference")
     ap.add_argument("--guide-width", type=int, default=1280)
@@ -334,6 +335,43 @@ def guiding_study(args, device: int) -> dict:
             "wall_s": time.perf_counter() - t0}
 
 
+def views_study(desc, hs, device: int) -> dict:
+    """Config 5 (reduced: 32 views of 256^2 or 512^2 pixels, 16 samples each): the same views
+    rendered by one xb_render_views call (shared waves) and one after the other (a renderer per
+    view size, one xb_render each), device time of the calls."""
+    import xenon_b200 as xb
+    from xenon_b200 import scenes
+    specs = scenes.orbit_views(desc, 32, seed=1, sizes=(256, 512), spps=(16,))
+    cams = [xb.camera(e, t, f, w / h) for (e, t, f, w, h, _) in specs]
+    views = [(c, w, h, spp) for c, (_, _, _, w, h, spp) in zip(cams, specs)]
+    paths = sum(w * h * spp for (_, w, h, spp) in views)
+    r = xb.Renderer(512, 512, desc.max_bounces, desc.min_bounces, device=device)
+    r.upload_scene(hs)
+    r.render_views(views[:2])                          # warm-up
+    r.reset_stats()
+    r.render_views(views)
+    batched_ms = r.stats().last_ms
+    r.close()
+    rs = {}
+    seq_ms = 0.0
+    for (c, w, h, spp) in views:
+        if (w, h) not in rs:
+            rr = xb.Renderer(w, h, desc.max_bounces, desc.min_bounces, device=device)
+            rr.upload_scene(hs)
+            rr.render_frame(c, 1)                      # warm-up
+            rs[(w, h)] = rr
+        rr = rs[(w, h)]
+        rr.reset()
+        rr.render_frame(c, spp)
+        seq_ms += rr.stats().last_ms
+    for rr in rs.values():
+        rr.close()
+    return {"workload": "config5 (reduced): 32 orbit views of the config-2 scene, 256^2 or 512^2 px, 16 spp",
+            "paths": paths, "batched_ms": batched_ms, "sequential_ms": seq_ms,
+            "batched_msamples_per_s": paths / batched_ms / 1e3, "sequential_msamples_per_s": paths / seq_ms / 1e3,
+            "speedup": seq_ms / max(batched_ms, 1e-9)}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -462,6 +500,12 @@ def main():
             cpu = {"value": None, "unit": "Mrays/s", "cores": None, "kind": "reference",
                    "sample": f"failed: {e}"}
 
+    views = None
+    if rank == 0 and ws == 1 and not args.no_views_study:
+        try:
+            views = views_study(desc, hs, local)
+        except Exception as e:
+            views = {"error": f"{type(e).__name__}: {e}"}
     guiding = None
     if rank == 0 and ws == 1 and not args.no_guiding_study:
         try:
@@ -481,7 +525,7 @@ def main():
                            "stage_ms_per_step": {k: getattr(prof, k) / args.steps for k in
                                                  ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms")}},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "guiding": guiding}
+                "clocks": clk.summary(), "guiding": guiding, "views": views}
         print(json.dumps(line))
     r.close()
     if ws > 1:

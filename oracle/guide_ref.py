@@ -1,5 +1,9 @@
-"""FP64 oracle for the path-guiding network (no reference counterpart: the reference has no
-learned component). Test infrastructure only.
+"""FP64 oracle for the path-guiding network. Test infrastructure only.
+
+Parity unpinned: the reference has no learned component, so nothing here restates reference code;
+this is the project's own specification of the network, checked against finite differences and
+quadrature (tests/test_guide_oracle.py) and used to check the GPU kernels. The reference-pinned
+quantity for guiding is the image (the guided estimator converges to the plain tracer's image).
 
 Network (the GPU kernels in xenon_b200/csrc/guide.cu follow this exactly, in BF16/FP32):
   input   64 features of a surface point: for position p in [0,1]^3 (scene bounds), shading
