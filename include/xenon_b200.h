@@ -323,6 +323,9 @@ typedef struct xb_tuning {
   int32_t wave_paths;                   /* paths in flight per wave (reallocates queues) */
   int32_t shadow_order;                 /* shadow rays: 1 nearer child first, 2 farther first
                                            (the occlusion answer does not depend on it) */
+  int32_t overlap;                      /* 1: a bounce's shadow rays run on a second stream,
+                                           concurrently with the next bounce's closest hits;
+                                           2: one stream */
 } xb_tuning;
 int  xb_set_tuning(xb_renderer *r, const xb_tuning *t);
 int  xb_get_tuning(const xb_renderer *r, xb_tuning *out);

@@ -84,12 +84,16 @@ def test_traversal_variants_render_identically(builder):
     from xenon_b200 import abi
     desc = builder()
     imgs = []
-    for flags in (0, abi.XB_FLAG_THREAD_PER_RAY):
+    for flags, tune in ((0, {}), (abi.XB_FLAG_THREAD_PER_RAY, {}), (0, {"overlap": 2}),
+                        (0, {"extend_persistent_from_depth": 1, "shadow_order": 2, "refill": 4})):
         r = Renderer(64, 48, desc.max_bounces, desc.min_bounces, flags=flags)
         r.upload_scene(HostScene.from_desc(desc))
+        if tune:
+            r.set_tuning(**tune)
         r.render_frame(camera(desc.eye, desc.target, desc.fov, 64 / 48), 3)
         imgs.append(r.resolve())
-    assert np.array_equal(imgs[0], imgs[1])
+    for img in imgs[1:]:
+        assert np.array_equal(imgs[0], img)
 
 
 @pytest.mark.gpu

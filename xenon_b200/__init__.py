@@ -56,9 +56,12 @@ class HostScene:
         self.camera_desc = None
 
     def __del__(self):
-        if getattr(self, "h", None) is not None and self.h.value:
-            lib().xb_scene_destroy(self.h)
-            self.h = None
+        try:
+            if getattr(self, "h", None) is not None and self.h.value:
+                lib().xb_scene_destroy(self.h)
+                self.h = None
+        except Exception:       # interpreter shutdown: the library handle may be gone already
+            pass
 
     @classmethod
     def from_desc(cls, desc) -> "HostScene":
@@ -134,7 +137,10 @@ class Renderer:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:   # interpreter shutdown: the library handle may be gone already
+            pass
 
     def _check(self, rc):
         return check(rc, self.h)

@@ -7,6 +7,7 @@ two passes), and keeps the fastest setting:
   extend_persistent_from_depth   which bounces trace closest hits with persistent warps
   shadow_persistent              persistent warps or one ray per thread for shadow rays
   shadow_order                   nearer or farther child first for shadow (any-hit) rays
+  overlap                        shadow rays of a bounce concurrent with the next bounce's closest hits
   refill                         idle lanes that trigger a warp refill
   extend/shadow/shade_blocks_per_sm   resident blocks per SM (grid size)
   wave_paths                     paths in flight per wave (queue capacity)
@@ -27,6 +28,7 @@ SPACE = {
     "extend_persistent_from_depth": [0, 1, 2, 3, 64],
     "shadow_persistent": [1, 2],
     "shadow_order": [1, 2],
+    "overlap": [1, 2],
     "refill": [2, 4, 8, 16, 24],
     "extend_blocks_per_sm": [3, 4, 5, 6, 64],
     "shadow_blocks_per_sm": [3, 4, 5, 6, 64],

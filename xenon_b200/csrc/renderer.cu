@@ -103,6 +103,9 @@ struct xb_renderer {
   xb_config cfg{};
   int min_bounces = 3, max_bounces = 8;
   cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;         // shadow rays, concurrent with the next bounce's hits
+  cudaEvent_t ev_shade[kMaxDepth] = {};   // bounce d's shading done (its shadow queues are full)
+  cudaEvent_t ev_shadow[kMaxDepth] = {};  // bounce d's shadow rays done (path radiance final)
   int num_sms = 0;
   std::string err;
   // scene
@@ -1157,6 +1160,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.shade_blocks_per_sm = pick(t.shade_blocks_per_sm, c.shade_blocks_per_sm, 64);
   c.wave_paths = pick(t.wave_paths, c.wave_paths, 1 << 21);
   c.shadow_order = pick(t.shadow_order, c.shadow_order, 1);
+  c.overlap = pick(t.overlap, c.overlap, 1);
   r->ext_persistent_from = c.extend_persistent_from_depth;
   r->shadow_persistent = c.shadow_persistent == 1;
   r->refill = c.refill;
@@ -1182,7 +1186,8 @@ struct StageTimer {
   xb_renderer* r;
   int stage;
   cudaEvent_t end = nullptr;
-  StageTimer(xb_renderer* rr, int st) : r(rr), stage(st) {
+  cudaStream_t s = nullptr;
+  StageTimer(xb_renderer* rr, int st, cudaStream_t ss = nullptr) : r(rr), stage(st), s(ss ? ss : rr->stream) {
     if (!(r->prof_flags & XB_PROFILE_STAGE_TIMES)) return;
     if (r->ev_used + 2 > r->ev_pool.size()) {
       for (int k = 0; k < 64; ++k) {
@@ -1192,13 +1197,13 @@ struct StageTimer {
       }
       r->ev_stage.resize(r->ev_pool.size() / 2);
     }
-    cudaEventRecord(r->ev_pool[r->ev_used], r->stream);
+    cudaEventRecord(r->ev_pool[r->ev_used], s);
     end = r->ev_pool[r->ev_used + 1];
     r->ev_stage[r->ev_used / 2] = stage;
     r->ev_used += 2;
   }
   ~StageTimer() {
-    if (end) cudaEventRecord(end, r->stream);
+    if (end) cudaEventRecord(end, s);
   }
 };
 
@@ -1229,27 +1234,61 @@ void guide_box(xb_renderer* r) {
 
 // The bounce loop of one wave whose camera rays are in queue 0: for every depth, closest hits,
 // shading (plain or guided), then the area-light and sun shadow rays (cpu_tiled.cpp:34-217).
+void launch_extend(xb_renderer* r, int d, bool count) {
+  WaveBuffers& w = r->wb;
+  const int q = d & 1;
+  int32_t* cd_ = w.cnt + d * kCntStride;
+  StageTimer t(r, STAGE_EXTEND);
+  if (r->thread_per_ray || d < r->ext_persistent_from) {
+    auto kern = count ? extend_kernel<true> : extend_kernel<false>;
+    kern<<<r->grid_ext, 128, 0, r->stream>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_, r->stats);
+  } else {
+    TraceQueue tq{w.ray_o[q], w.ray_d[q], cd_ + CNT_RAYS, cd_ + CNT_FETCH_EXT, w.hit, w.hit_inst,
+                  nullptr, nullptr, r->stats, 0};
+    auto kern = count ? extend_persistent_kernel<true> : extend_persistent_kernel<false>;
+    kern<<<r->grid_pext, 128, 0, r->stream>>>(r->scene, tq, r->refill);
+  }
+}
+
+void launch_shadows(xb_renderer* r, int d, bool count, cudaStream_t s) {
+  WaveBuffers& w = r->wb;
+  int32_t* cd_ = w.cnt + d * kCntStride;
+  for (int k = 0; k < 2; ++k) {
+    if (k == 0 && r->scene.num_lights == 0) continue;
+    if (k == 1 && r->scene.num_suns == 0) continue;
+    StageTimer t(r, STAGE_SHADOW, s);
+    if (r->thread_per_ray || !r->shadow_persistent) {
+      auto kern = count ? shadow_kernel<true> : shadow_kernel<false>;
+      kern<<<r->grid_shadow, 128, 0, s>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
+                                          cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
+                                          cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats,
+                                          r->tune.shadow_order == 2);
+    } else {
+      TraceQueue tq{w.sh_o[k], w.sh_d[k], cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
+                    cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), nullptr, nullptr, w.sh_c[k], w.L,
+                    r->stats, r->tune.shadow_order == 2};
+      auto kern = count ? shadow_persistent_kernel<true> : shadow_persistent_kernel<false>;
+      kern<<<r->grid_pshadow, 128, 0, s>>>(r->scene, tq, r->refill);
+    }
+  }
+}
+
+// The bounce loop of one wave whose camera rays are in queue 0: for every depth, closest hits,
+// shading (plain or guided), then the area-light and sun shadow rays (cpu_tiled.cpp:34-217).
+// With overlap, bounce d's shadow rays run on the second stream while bounce d+1's closest hits
+// run on the first: the two only share the scene (shadow rays add to the path radiance, closest
+// hits write the hit records), and shading d+1 waits for both. Each kernel's tail — a few warps
+// finishing long rays after the queue has drained — then runs beside the other kernel's bulk.
 int trace_bounces(xb_renderer* r, bool train, int rec_stride) {
   WaveBuffers& w = r->wb;
   const int depth_max = std::min(r->max_bounces, kMaxDepth);
   const bool count = (r->prof_flags & XB_PROFILE_COUNT_TRAVERSAL) != 0;
+  const bool ov = r->tune.overlap == 1 && r->stream2 != nullptr;
   xbg::Guide* gd = r->guiding ? r->guide : nullptr;
   for (int d = 0; d < depth_max; ++d) {
     const int q = d & 1, nq = q ^ 1;
     int32_t* cd_ = w.cnt + d * kCntStride;
-    {
-      StageTimer t(r, STAGE_EXTEND);
-      if (r->thread_per_ray || d < r->ext_persistent_from) {
-        auto kern = count ? extend_kernel<true> : extend_kernel<false>;
-        kern<<<r->grid_ext, 128, 0, r->stream>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_,
-                                                 r->stats);
-      } else {
-        TraceQueue tq{w.ray_o[q], w.ray_d[q], cd_ + CNT_RAYS, cd_ + CNT_FETCH_EXT, w.hit, w.hit_inst,
-                      nullptr, nullptr, r->stats, 0};
-        auto kern = count ? extend_persistent_kernel<true> : extend_persistent_kernel<false>;
-        kern<<<r->grid_pext, 128, 0, r->stream>>>(r->scene, tq, r->refill);
-      }
-    }
+    if (d == 0 || !ov) launch_extend(r, d, count);
     ShadeArgs sa;
     sa.sc = r->scene;
     sa.ray_o = w.ray_o[q]; sa.ray_d = w.ray_d[q]; sa.tp = w.tp[q]; sa.rng = w.rng[q]; sa.path = w.path[q];
@@ -1284,24 +1323,16 @@ int trace_bounces(xb_renderer* r, bool train, int rec_stride) {
       StageTimer t(r, STAGE_SHADE);
       shade_kernel<<<r->grid_shade, 128, 0, r->stream>>>(sa);
     }
-    for (int k = 0; k < 2; ++k) {
-      if (k == 0 && r->scene.num_lights == 0) continue;
-      if (k == 1 && r->scene.num_suns == 0) continue;
-      StageTimer t(r, STAGE_SHADOW);
-      if (r->thread_per_ray || !r->shadow_persistent) {
-        auto kern = count ? shadow_kernel<true> : shadow_kernel<false>;
-        kern<<<r->grid_shadow, 128, 0, r->stream>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
-                                                    cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
-                                                    cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats,
-                                                    r->tune.shadow_order == 2);
-      } else {
-        TraceQueue tq{w.sh_o[k], w.sh_d[k], cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
-                      cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), nullptr, nullptr, w.sh_c[k], w.L,
-                      r->stats, r->tune.shadow_order == 2};
-        auto kern = count ? shadow_persistent_kernel<true> : shadow_persistent_kernel<false>;
-        kern<<<r->grid_pshadow, 128, 0, r->stream>>>(r->scene, tq, r->refill);
-      }
+    if (!ov) {
+      launch_shadows(r, d, count, r->stream);
+      continue;
     }
+    CK(cudaEventRecord(r->ev_shade[d], r->stream));
+    CK(cudaStreamWaitEvent(r->stream2, r->ev_shade[d], 0));
+    launch_shadows(r, d, count, r->stream2);
+    CK(cudaEventRecord(r->ev_shadow[d], r->stream2));
+    if (d + 1 < depth_max) launch_extend(r, d + 1, count);
+    CK(cudaStreamWaitEvent(r->stream, r->ev_shadow[d], 0));
   }
   CK(cudaGetLastError());
   return XB_OK;
@@ -1461,6 +1492,12 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return bail(xb::fail(XB_E_CUDA, "cudaGetDeviceProperties failed"));
   r->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&r->stream2, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(xb::fail(XB_E_CUDA, "stream creation failed"));
+  for (int d = 0; d < kMaxDepth; ++d)
+    if (cudaEventCreateWithFlags(&r->ev_shade[d], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev_shadow[d], cudaEventDisableTiming) != cudaSuccess)
+      return bail(xb::fail(XB_E_CUDA, "event creation failed"));
   if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess)
     return bail(xb::fail(XB_E_CUDA, "stream/event creation failed"));
@@ -1536,6 +1573,12 @@ void xb_destroy(xb_renderer* r) {
   for (cudaEvent_t e : r->ev_pool) cudaEventDestroy(e);
   if (r->ev0) cudaEventDestroy(r->ev0);
   if (r->ev1) cudaEventDestroy(r->ev1);
+  if (r->stream2) cudaStreamSynchronize(r->stream2);
+  for (int d = 0; d < kMaxDepth; ++d) {
+    if (r->ev_shade[d]) cudaEventDestroy(r->ev_shade[d]);
+    if (r->ev_shadow[d]) cudaEventDestroy(r->ev_shadow[d]);
+  }
+  if (r->stream2) cudaStreamDestroy(r->stream2);
   if (r->stream) cudaStreamDestroy(r->stream);
   delete r;
 }
