@@ -110,6 +110,8 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="config2")
     ap.add_argument("--out", default=None, help="also write the result JSON here")
+    ap.add_argument("--spp", type=int, default=4, help="samples per measurement")
+    ap.add_argument("--from-saved", action="store_true", help="start from the stored tuning")
     a = ap.parse_args()
     if a.workload == "config2":
         desc = scenes.icosphere_scene(level=8)
@@ -123,7 +125,9 @@ if __name__ == "__main__":
     r = xb.Renderer(desc.width, desc.height, desc.max_bounces, desc.min_bounces)
     r.upload_scene(hs)
     cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
-    res = autotune(r, cam, a.workload)
+    if a.from_saved and load_tuning(a.workload):
+        r.set_tuning(**load_tuning(a.workload))
+    res = autotune(r, cam, a.workload, spp=a.spp)
     print(json.dumps(res))
     if a.out:
         with open(a.out, "w") as f:
