@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--no-views-study", action="store_true", help="skip the config-5 batched-views comparison")
     ap.add_argument("--guide-seconds", type=float, default=6.0, help="equal device-time budget per method")
     ap.add_argument("--guide-ref-spp", type=int, default=2048, help="samples of the plain FP64 reference")
+    ap.add_argument("--guide-train-spp", type=int, default=64)
+    ap.add_argument("--guide-steps-per-spp", type=int, default=32)
+    ap.add_argument("--guide-fraction", type=float, default=0.0,
+                    help="fixed probability of sampling the network (0: learned per vertex)")
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--guide-height", type=int, default=720)
     return ap.parse_args()
@@ -298,20 +302,24 @@ def guiding_study(args, device: int) -> dict:
         r = renderer()
         info = {}
         if guided:
-            r.set_guiding(True, train_spp=64, steps_per_spp=32, batch=16384, guide_fraction=0.7)
+            fixed = args.guide_fraction > 0
+            r.set_guiding(True, train_spp=args.guide_train_spp, steps_per_spp=args.guide_steps_per_spp,
+                          batch=16384, guide_fraction=args.guide_fraction if fixed else 0.7,
+                          fixed_fraction=1 if fixed else 0)
         ms, rendered, chunk = 0.0, 0, 8
         while ms < args.guide_seconds * 1e3:
             r.render_frame(cam, chunk)
             ms += r.stats().last_ms
             rendered += chunk
-            if guided and rendered == 64:
+            if guided and rendered == args.guide_train_spp:
                 info["train_phase_ms"] = ms
         spp = r.spp                              # image samples (training samples excluded)
         img = r.resolve().astype(np.float64)
         if guided:
             info.update(r.guiding_stats())
             info["config"] = {k: v for k, v in r.guiding().items() if k in
-                              ("train_spp", "steps_per_spp", "batch", "learning_rate", "guide_fraction")}
+                              ("train_spp", "steps_per_spp", "batch", "learning_rate", "guide_fraction",
+                               "fixed_fraction")}
         r.close()
         e = (img - ref) ** 2 / denom
         pix = e.mean(2).ravel()

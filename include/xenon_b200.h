@@ -380,15 +380,16 @@ int  xb_bsdf_sample(const xb_material *m, int64_t n, const float *wo, uint64_t *
 /* ── learned path guiding (no reference counterpart: the reference has no learned part) ── */
 
 /* A small network maps a surface point (position in the scene bounds, shading normal, outgoing
- * direction) to a mixture of 8 von Mises-Fisher lobes q over incoming directions. At every
- * non-delta vertex seen from the front of its shading normal the next direction is drawn from
- *     p(w) = guide_fraction * q(w) + (1 - guide_fraction) * p_bsdf(w)
+ * direction) to a mixture of 8 von Mises-Fisher lobes q over incoming directions and a selection
+ * probability a. At every non-delta vertex seen from the front of its shading normal the next
+ * direction is drawn from
+ *     p(w) = a * q(w) + (1 - a) * p_bsdf(w)
  * (p_bsdf: the density of bsdf_sample), the vertex keeps the lobe, f and pdf the plain sampler
  * would have produced for w (so MIS weights, next-event estimation and Russian roulette are the
  * plain tracer's), and the path's radiance is weighted by the product of p_bsdf(w) / p(w) over
  * its guided vertices. The guided image therefore converges to the plain tracer's image for any
  * network and any scene. The network is trained online, on the first train_spp samples per
- * pixel, by Adam on the radiance-weighted negative log-likelihood of the sampled directions;
+ * pixel, by Adam on the radiance-weighted negative log-likelihood of p at the sampled directions;
  * the training samples are part of the image. BF16 tensor cores (tcgen05), FP32 accumulation
  * and master weights. */
 typedef struct xb_guiding {
@@ -397,7 +398,8 @@ typedef struct xb_guiding {
   int32_t steps_per_spp;    /* Adam steps per training sample per pixel; default 32 */
   int32_t batch;            /* records per Adam step (multiple of 128); default 16384 */
   float learning_rate;      /* default 5e-3 */
-  float guide_fraction;     /* probability of sampling the network; default 0.7 */
+  float guide_fraction;     /* probability of sampling the network when fixed_fraction is set;
+                               default 0.7 */
   int32_t max_records;      /* training records kept per wave; default 1 << 21 */
   int32_t record_stride;    /* record the vertices of one path in this many; 0 = automatic */
   uint64_t seed;            /* initial weights and batch windows */
@@ -405,6 +407,9 @@ typedef struct xb_guiding {
   float bounds_max[3];      /* an empty box selects the scene's bounds */
   int32_t keep_training_samples;  /* 0: samples 1..train_spp train the network only and stay out
                                    * of the image (xb_get_spp counts image samples) */
+  int32_t fixed_fraction;   /* 0: the network also outputs the probability of sampling it at each
+                             * vertex (in [0.05, 0.95], trained with the mixture);
+                             * 1: guide_fraction everywhere */
 } xb_guiding;
 
 /* Enables, disables or reconfigures guiding (0 fields take defaults). The first enabling, or a
@@ -430,12 +435,15 @@ int  xb_guide_set_params(xb_renderer *r, const float *params);
 
 /* Standalone network calls on host buffers (parity tests and diagnostics).
  *   feats: rows x 9 (position in [0,1]^3, normal, outgoing direction)
- *   lobes: rows x 40, per lobe mean direction xyz, concentration kappa, weight
- *   recs:  n x 20 training records: feats 9, direction 3, weight c, path, throughput 3, radiance 3
- *          (the loss uses feats, direction and c). */
+ *   lobes: rows x 40, per lobe mean direction xyz, concentration kappa, weight; the forward call
+ *          writes rows x 41: the lobes, then the selection probability a
+ *   recs:  n x 24 training records: feats 9, direction 3, weight c, path, throughput 3,
+ *          radiance 3, p_bsdf at the direction (< 0: the loss is that of q alone), 3 unused
+ *          (the loss uses feats, direction, c and p_bsdf). */
 int  xb_guide_init_params(uint64_t seed, float *params);
 int  xb_guide_forward(const float *params, const float *feats, int64_t rows, float *lobes);
-/* Loss sum(c * -log q(direction)) / sum(c) and its gradient with respect to the parameters. */
+/* Loss sum(c * -log p(direction)) / sum(c), p = a q + (1 - a) p_bsdf, and its gradient with
+ * respect to the parameters. */
 int  xb_guide_loss_grad(const float *params, const float *recs, int64_t n, float *grad, float *loss);
 /* `steps` Adam steps (lr, beta 0.9 / 0.99, eps 1e-8) on batches of `batch` records (tiles of 128
  * consecutive records at random starts; all records in order when n <= batch); params_out gets

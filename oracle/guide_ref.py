@@ -17,8 +17,12 @@ Network (the GPU kernels in xenon_b200/csrc/guide.cu follow this exactly, in BF1
             mu_k    = m / sqrt(|m|^2 + 1e-8),  m = raw[5k:5k+3]
             kappa_k = exp(clamp(raw[5k+3], -4, 6))
             w       = softmax(raw[5k+4])
+  select  a = A_MIN + (A_MAX - A_MIN) sigmoid(raw[40]): the probability of sampling q at the vertex
   pdf     q(w) = sum_k w_k kappa_k / (2 pi (1 - exp(-2 kappa_k))) exp(kappa_k (mu_k . w - 1))
-  loss    sum_b c_b (-log q_b(omega_b)) / sum_b c_b   (c_b >= 0: radiance / sampling pdf)
+  mixture p(w) = a q(w) + (1 - a) p_bsdf(w), the density the renderer samples
+  loss    sum_b c_b (-log p_b(omega_b)) / sum_b c_b   (c_b >= 0: the integrand over the sampling
+          density; p_bsdf(omega_b) is recorded with the sample) — the weighted negative
+          log-likelihood of the mixture (Mueller et al., Neural Importance Sampling, 2019)
 """
 from __future__ import annotations
 
@@ -29,6 +33,8 @@ N_HID = 64
 N_OUT = 48
 N_LOBES = 8
 KAPPA_MIN, KAPPA_MAX = -4.0, 6.0
+A_MIN, A_MAX = 0.05, 0.95
+SELECT = 40                     # raw output holding the selection logit
 LAYERS = [(N_HID, N_IN), (N_HID, N_HID), (N_HID, N_HID), (N_OUT, N_HID)]  # (out, in)
 
 
@@ -114,6 +120,10 @@ def lobes(raw: np.ndarray):
     return mu, kappa, w, s, kraw
 
 
+def selection(raw: np.ndarray) -> np.ndarray:
+    return A_MIN + (A_MAX - A_MIN) / (1.0 + np.exp(-raw[:, SELECT]))
+
+
 def vmf_norm(kappa):
     return kappa / (2.0 * np.pi * (-np.expm1(-2.0 * kappa)))
 
@@ -125,25 +135,37 @@ def pdf(raw: np.ndarray, omega: np.ndarray) -> np.ndarray:
     return (w * v).sum(-1)
 
 
-def loss_grad_raw(raw: np.ndarray, omega: np.ndarray, c: np.ndarray):
-    """Loss and dLoss/draw for the weighted negative log-likelihood."""
+def loss_grad_raw(raw: np.ndarray, omega: np.ndarray, c: np.ndarray, pb: np.ndarray | None = None):
+    """Loss and dLoss/draw for the weighted negative log-likelihood of the mixture
+    p = a q + (1 - a) pb (pb = None: of q alone, a fixed at 1)."""
     mu, kappa, w, s, kraw = lobes(raw)
     cos = (mu * omega[:, None, :]).sum(-1)
     v = vmf_norm(kappa) * np.exp(kappa * (cos - 1.0))
     q = (w * v).sum(-1)
+    if pb is None:
+        a = np.ones(len(raw))
+        pm = q
+    else:
+        a = selection(raw)
+        pm = a * q + (1.0 - a) * pb
     csum = c.sum()
-    loss = float((c * -np.log(q)).sum() / csum)
-    cb = (c / csum)[:, None]
+    loss = float((c * -np.log(pm)).sum() / csum)
+    cb = (c / csum)
+    rho = a * q / pm                      # the share of the mixture density that q holds
+    cq = (cb * rho)[:, None]              # d(-log pm) = rho * d(-log q) for q's parameters
     r = w * v / q[:, None]
     g = np.zeros_like(raw)
     gl = g[:, :5 * N_LOBES].reshape(-1, N_LOBES, 5)
-    gl[..., 4] = cb * (w - r)
+    gl[..., 4] = cq * (w - r)
     dlogv_dk = 1.0 / kappa - 2.0 / np.expm1(2.0 * kappa) + (cos - 1.0)
     inside = (kraw > KAPPA_MIN) & (kraw < KAPPA_MAX)
-    gl[..., 3] = -cb * r * dlogv_dk * kappa * inside
-    dmu = -(cb * r * kappa)[..., None] * omega[:, None, :]
+    gl[..., 3] = -cq * r * dlogv_dk * kappa * inside
+    dmu = -(cq * r * kappa)[..., None] * omega[:, None, :]
     proj = (dmu * mu).sum(-1, keepdims=True)
     gl[..., 0:3] = (dmu - proj * mu) / s[..., None]
+    if pb is not None:
+        sig = (a - A_MIN) / (A_MAX - A_MIN)
+        g[:, SELECT] = cb * (-(q - pb) / pm) * (A_MAX - A_MIN) * sig * (1.0 - sig)
     return loss, g
 
 
@@ -159,9 +181,10 @@ def backward(P: dict, acts: list, graw: np.ndarray, emulate_bf16: bool = False) 
     return G
 
 
-def loss_and_grads(P: dict, X: np.ndarray, omega: np.ndarray, c: np.ndarray, emulate_bf16: bool = False):
+def loss_and_grads(P: dict, X: np.ndarray, omega: np.ndarray, c: np.ndarray, emulate_bf16: bool = False,
+                   pb: np.ndarray | None = None):
     acts, raw = forward(P, X, emulate_bf16)
-    loss, graw = loss_grad_raw(raw, omega, c)
+    loss, graw = loss_grad_raw(raw, omega, c, pb)
     return loss, backward(P, acts, graw, emulate_bf16), raw
 
 

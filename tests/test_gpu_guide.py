@@ -55,12 +55,24 @@ def _params(seed, out_scale=10.0):
     return G.flatten(P).astype(np.float32)
 
 
-def _records(rng, n):
-    R = np.zeros((n, 20), np.float32)
+def _records(rng, n, mixture=True):
+    R = np.zeros((n, 24), np.float32)
     R[:, 0:9] = _feats(rng, n)
     R[:, 9:12] = _unit(rng, n)
     R[:, 12] = rng.random(n) * 2.0
+    if mixture:
+        R[:, 20] = rng.random(n) * 0.5          # density of the BSDF sampler at the direction
+        R[::7, 20] = 0.0                        # directions the BSDF cannot produce
+    else:
+        R[:, 20] = -1.0                         # loss of q alone
     return R
+
+
+def _oracle_loss(params, R, emulate=True):
+    mixture = R[0, 20] >= 0
+    return G.loss_and_grads(G.unflatten(params), G.features(R[:, 0:9]), R[:, 9:12].astype(np.float64),
+                            R[:, 12].astype(np.float64), emulate_bf16=emulate,
+                            pb=R[:, 20].astype(np.float64) if mixture else None)
 
 
 def _oracle_lobes(params, f9):
@@ -75,8 +87,9 @@ def test_guide_forward_matches_oracle(rows):
     rng = np.random.default_rng(rows)
     params = _params(3)
     f9 = _feats(rng, rows)
-    got = xb.guide_forward(params, f9)
-    mu, kappa, w, _ = _oracle_lobes(params, f9)
+    got, sel = xb.guide_forward(params, f9, with_selection=True)
+    mu, kappa, w, raw = _oracle_lobes(params, f9)
+    assert np.abs(sel - G.selection(raw)).max() < 1e-2
     # BF16 operands on both sides; the remaining differences are FP32 vs FP64 accumulation and
     # activations that round to a neighbouring bf16 value
     assert np.abs(got[:, :, 0:3] - mu).max() < 2e-2
@@ -88,14 +101,13 @@ def test_guide_forward_matches_oracle(rows):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [128, 777])
-def test_guide_gradient_matches_oracle(n):
+@pytest.mark.parametrize("n,mixture", [(128, False), (777, False), (128, True), (777, True)])
+def test_guide_gradient_matches_oracle(n, mixture):
     rng = np.random.default_rng(n)
     params = _params(5)
-    R = _records(rng, n)
+    R = _records(rng, n, mixture)
     loss, grad = xb.guide_loss_grad(params, R)
-    want_loss, GW, _ = G.loss_and_grads(G.unflatten(params), G.features(R[:, 0:9]), R[:, 9:12].astype(np.float64),
-                                         R[:, 12].astype(np.float64), emulate_bf16=True)
+    want_loss, GW, _ = _oracle_loss(params, R)
     want = G.flatten(GW)
     assert abs(loss - want_loss) <= 1e-3 * abs(want_loss) + 1e-5, (loss, want_loss)
     # per layer: the backward MMAs take the error signal in BF16, so relative agreement ~1e-2
@@ -119,7 +131,8 @@ def test_guide_adam_steps_match_oracle():
     want_losses = []
     X = G.features(R[:, 0:9])
     for t in range(1, steps + 1):
-        l, GW, _ = G.loss_and_grads(P, X, R[:, 9:12].astype(np.float64), R[:, 12].astype(np.float64), True)
+        l, GW, _ = G.loss_and_grads(P, X, R[:, 9:12].astype(np.float64), R[:, 12].astype(np.float64), True,
+                                    pb=R[:, 20].astype(np.float64))
         want_losses.append(l)
         G.adam(P, GW, M, V, t, lr=1e-3)
     want = G.flatten(P)
@@ -135,7 +148,7 @@ def test_guide_training_learns_a_direction_field():
     the learned density there far above uniform (1 / 4 pi)."""
     rng = np.random.default_rng(2)
     n = 16384
-    R = _records(rng, n)
+    R = _records(rng, n, mixture=False)
     axis = np.stack([np.cos(2 * np.pi * R[:, 0]), np.sin(2 * np.pi * R[:, 0]), 0.3 * np.ones(n)], 1)
     axis /= np.linalg.norm(axis, axis=1, keepdims=True)
     om = axis + 0.15 * rng.normal(size=(n, 3))

@@ -1,6 +1,7 @@
 """The guiding network's FP64 oracle checked on its own: analytic gradients against finite
 differences, the vMF mixture normalised over the sphere, sampling consistent with the pdf."""
 import numpy as np
+import pytest
 
 from oracle import guide_ref as g
 
@@ -21,26 +22,32 @@ def test_encoding_shape_and_range():
     assert np.all(np.abs(X[:, :60]) <= 1.0) and np.all(X[:, 63] == 1.0)
 
 
-def test_gradients_match_finite_differences():
+@pytest.mark.parametrize("mixture", [False, True])
+def test_gradients_match_finite_differences(mixture):
     P = g.init_params(3)
     for k in P:          # larger output layer so every lobe matters
         if k == "W3":
             P[k] = P[k] * 10
+    P["b3"][g.SELECT] = 0.7
     X, om, c = _batch(16, 1)
-    loss, G, _ = g.loss_and_grads(P, X, om, c)
+    pb = np.random.default_rng(5).random(16) * 0.6 if mixture else None
+    if mixture:
+        pb[3] = 0.0                       # a direction the BSDF cannot sample
+    loss, G, _ = g.loss_and_grads(P, X, om, c, pb=pb)
     rng = np.random.default_rng(7)
-    for key in ("W0", "b0", "W1", "W2", "W3", "b3"):
-        for _ in range(6):
-            idx = tuple(rng.integers(0, s) for s in P[key].shape)
-            h = 1e-6
-            Pp = {k: v.copy() for k, v in P.items()}
-            Pm = {k: v.copy() for k, v in P.items()}
-            Pp[key][idx] += h
-            Pm[key][idx] -= h
-            lp, _, _ = g.loss_and_grads(Pp, X, om, c)
-            lm, _, _ = g.loss_and_grads(Pm, X, om, c)
-            fd = (lp - lm) / (2 * h)
-            assert abs(fd - G[key][idx]) <= 1e-6 + 1e-4 * abs(fd), (key, idx, fd, G[key][idx])
+    checks = [(key, tuple(rng.integers(0, s) for s in P[key].shape))
+              for key in ("W0", "b0", "W1", "W2", "W3", "b3") for _ in range(6)]
+    checks += [("b3", (g.SELECT,)), ("W3", (g.SELECT, 5)), ("W3", (g.SELECT, 17))]
+    for key, idx in checks:
+        h = 1e-6
+        Pp = {k: v.copy() for k, v in P.items()}
+        Pm = {k: v.copy() for k, v in P.items()}
+        Pp[key][idx] += h
+        Pm[key][idx] -= h
+        lp, _, _ = g.loss_and_grads(Pp, X, om, c, pb=pb)
+        lm, _, _ = g.loss_and_grads(Pm, X, om, c, pb=pb)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - G[key][idx]) <= 1e-6 + 1e-4 * abs(fd), (key, idx, fd, G[key][idx])
 
 
 def test_mixture_pdf_integrates_to_one():

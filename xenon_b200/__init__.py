@@ -297,13 +297,15 @@ def guide_init_params(seed: int = 1) -> np.ndarray:
     return out
 
 
-def guide_forward(params: np.ndarray, feats: np.ndarray) -> np.ndarray:
-    """feats [rows, 9] (position in [0,1]^3, normal, outgoing direction) -> lobes [rows, 8, 5]."""
+def guide_forward(params: np.ndarray, feats: np.ndarray, with_selection: bool = False):
+    """feats [rows, 9] (position in [0,1]^3, normal, outgoing direction) -> lobes [rows, 8, 5]
+    (and the selection probabilities [rows] with with_selection)."""
     p = np.ascontiguousarray(params, np.float32)
     f = np.ascontiguousarray(feats, np.float32)
-    out = np.empty((len(f), abi.GUIDE_LOBE_FLOATS), np.float32)
+    out = np.empty((len(f), abi.GUIDE_OUT_FLOATS), np.float32)
     check(lib().xb_guide_forward(_p(p), _p(f), len(f), _p(out)))
-    return out.reshape(len(f), 8, 5)
+    lobes = np.ascontiguousarray(out[:, :40]).reshape(len(f), 8, 5)
+    return (lobes, out[:, 40].copy()) if with_selection else lobes
 
 
 def guide_loss_grad(params: np.ndarray, recs: np.ndarray):

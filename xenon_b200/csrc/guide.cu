@@ -70,9 +70,9 @@ __global__ void __launch_bounds__(128) guide_infer_kernel(const float* __restric
     float lob[kLobeFloats];
     raw_to_lobes(raw, lob);
     if (row < n) {
-      float4* o = reinterpret_cast<float4*>(lobes + (size_t)row * kLobeFloats);
-      for (int i = 0; i < kLobeFloats / 4; ++i)
-        o[i] = make_float4(lob[4 * i], lob[4 * i + 1], lob[4 * i + 2], lob[4 * i + 3]);
+      float* o = lobes + (size_t)row * kOutRow;
+      for (int i = 0; i < kLobeFloats; ++i) o[i] = lob[i];
+      o[kLobeFloats] = selection(raw);
     }
   }
   mma_teardown(m.tmem);
@@ -112,6 +112,7 @@ struct TrainArgs {
   const int32_t* rec_count;
   int cap, batch;
   uint64_t seed, t;       // tile placement of this step
+  float alpha_fixed;      // selection probability the renderer uses (< 0: the network's own)
   const float* csum;      // sum of the batch's weights
   const __nv_bfloat16* wf;
   const __nv_bfloat16* wb;
@@ -121,8 +122,11 @@ struct TrainArgs {
   int* err;
 };
 
-// Gradient of c (-log q(omega)) / csum with respect to the 48 raw outputs (oracle: loss_grad_raw).
-__device__ __forceinline__ float output_gradient(const float* raw, const float* om, float cb, float* g) {
+// Gradient of c (-log p(omega)) / csum with respect to the 48 raw outputs, p = a q + (1 - a) pb
+// the mixture the renderer samples (a: the learned selection probability; pb < 0: p = q alone)
+// (oracle: loss_grad_raw).
+__device__ __forceinline__ float output_gradient(const float* raw, const float* om, float cb, float pb,
+                                                 float alpha_fixed, float* g) {
   float lob[kLobeFloats];
   raw_to_lobes(raw, lob);
   float v[kLobes], cosv[kLobes], q = 0.f;
@@ -134,28 +138,37 @@ __device__ __forceinline__ float output_gradient(const float* raw, const float* 
     q += L[4] * v[k];
   }
   q = fmaxf(q, 1e-30f);
-  const float loss = cb > 0.f ? -cb * logf(q) : 0.f;
+  const bool mix = pb >= 0.f;
+  const bool learned = mix && alpha_fixed < 0.f;
+  const float a = mix ? (learned ? selection(raw) : alpha_fixed) : 1.f;
+  const float pm = fmaxf(mix ? a * q + (1.f - a) * pb : q, 1e-30f);
+  const float loss = cb > 0.f ? -cb * logf(pm) : 0.f;
+  const float cq = cb * (a * q / pm);   // d(-log pm) = (a q / pm) d(-log q) for q's parameters
 #pragma unroll
   for (int i = 40; i < kOut; ++i) g[i] = 0.f;
+  if (learned) {
+    const float sg = (a - kAMin) / (kAMax - kAMin);
+    g[kSelect] = cb * (-(q - pb) / pm) * (kAMax - kAMin) * sg * (1.f - sg);
+  }
 #pragma unroll
   for (int k = 0; k < kLobes; ++k) {
     const float* L = lob + 5 * k;
     const float r = L[4] * v[k] / q;
-    g[5 * k + 4] = cb * (L[4] - r);
+    g[5 * k + 4] = cq * (L[4] - r);
     const float kp = L[3];
     const float dlogv = 1.f / kp - 2.f / expm1f(2.f * kp) + (cosv[k] - 1.f);
     const float kr = raw[5 * k + 3];
-    g[5 * k + 3] = (kr > -4.f && kr < 6.f) ? -cb * r * dlogv * kp : 0.f;
+    g[5 * k + 3] = (kr > -4.f && kr < 6.f) ? -cq * r * dlogv * kp : 0.f;
     const float* m = raw + 5 * k;
     const float s = sqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2] + 1e-8f);
     float dmu[3], proj = 0.f;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      dmu[a] = -cb * r * kp * om[a];
-      proj += dmu[a] * L[a];
+    for (int a3 = 0; a3 < 3; ++a3) {
+      dmu[a3] = -cq * r * kp * om[a3];
+      proj += dmu[a3] * L[a3];
     }
 #pragma unroll
-    for (int a = 0; a < 3; ++a) g[5 * k + a] = (dmu[a] - proj * L[a]) / s;
+    for (int a3 = 0; a3 < 3; ++a3) g[5 * k + a3] = (dmu[a3] - proj * L[a3]) / s;
   }
   return loss;
 }
@@ -209,12 +222,13 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(TrainArgs A) {
   mma_setup(&tmem_slot, &mbar);
   Mma m{tmem_slot, &mbar, 0u, A.err, true};
   const bool valid = start + (int)threadIdx.x < n;
-  float f[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, om[3] = {0, 0, 1}, c = 0.f;
+  float f[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, om[3] = {0, 0, 1}, c = 0.f, pb = -1.f;
   if (valid) {
     const float* R = A.recs + (size_t)(start + threadIdx.x) * kRecFloats;
     for (int i = 0; i < 9; ++i) f[i] = R[i];
     om[0] = R[9]; om[1] = R[10]; om[2] = R[11];
     c = R[12];
+    pb = R[20];
   }
   encode_row(f, sAct, threadIdx.x);
   for (int l = 0; l < 3 && m.ok; ++l) {
@@ -233,7 +247,7 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(TrainArgs A) {
     for (int i = 0; i < kOut; ++i) raw[i] += sBias[3 * kHid + i];
     const float cb = (valid && csum > 0.f) ? c / csum : 0.f;
     float g[kOut];
-    loss_part = output_gradient(raw, om, cb, g);
+    loss_part = output_gradient(raw, om, cb, pb, A.alpha_fixed, g);
     for (int i = 0; i < kOut; ++i) sDf[threadIdx.x * kHid + i] = g[i];
     for (int k0 = 0; k0 < kOut; k0 += 8) store8_bf16(sD, threadIdx.x, k0, kOut, g + k0);
   }
@@ -419,7 +433,7 @@ void guide_finalize_records(Guide* g, cudaStream_t s, const float4* L, int grid,
 }
 
 int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_count, int cap, int steps,
-                int batch, float lr, uint64_t seed) {
+                int batch, float lr, uint64_t seed, float alpha_fixed) {
   steps = std::min(steps, g->max_steps);
   batch = std::max(kTile, (batch + kTile - 1) / kTile * kTile);
   const int tiles = batch / kTile;
@@ -429,8 +443,8 @@ int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_
   for (int k = 0; k < steps; ++k) {
     const uint64_t t = (uint64_t)g->t;
     weight_sum_kernel<<<tiles, kTile, 0, s>>>(recs, rec_count, cap, batch, seed, t, g->csum + k);
-    TrainArgs a{recs, rec_count, cap, batch, seed, t, g->csum + k, g->wf, g->wb, g->master, g->grad, g->loss + k,
-                g->err};
+    TrainArgs a{recs, rec_count, cap, batch, seed, t, alpha_fixed, g->csum + k, g->wf, g->wb, g->master, g->grad,
+                g->loss + k, g->err};
     guide_train_kernel<<<tiles, kTile, kTrainSmem, s>>>(a);
     g->t += 1;
     const float c1 = 1.f - (float)std::pow((double)b1, (double)g->t);
@@ -448,7 +462,7 @@ int guide_gradient(Guide* g, cudaStream_t s, const float* recs, const int32_t* c
   weight_sum_kernel<<<batch / kTile, kTile, 0, s>>>(recs, count, n, batch, 0, 0, g->csum);
   cudaMemsetAsync(grad_dev, 0, kParams * 4, s);
   cudaMemsetAsync(loss_dev, 0, 4, s);
-  TrainArgs a{recs, count, n, batch, 0, 0, g->csum, g->wf, g->wb, g->master, grad_dev, loss_dev, g->err};
+  TrainArgs a{recs, count, n, batch, 0, 0, -1.f, g->csum, g->wf, g->wb, g->master, grad_dev, loss_dev, g->err};
   guide_train_kernel<<<batch / kTile, kTile, kTrainSmem, s>>>(a);
   return cudaGetLastError() == cudaSuccess ? XB_OK : XB_E_CUDA;
 }
@@ -654,12 +668,12 @@ int xb_guide_forward(const float* params, const float* feats, int64_t rows, floa
   const int32_t n = (int32_t)rows;
   float* dF = s.upload(feats, (size_t)rows * 9);
   int32_t* dN = s.upload(&n, 1);
-  float* dL = s.alloc<float>((size_t)rows * xbg::kLobeFloats);
+  float* dL = s.alloc<float>((size_t)rows * xbg::kOutRow);
   if (!dF || !dN || !dL) return xb::fail(XB_E_OOM, "xb_guide_forward: out of device memory");
   const int tiles = (int)((rows + 127) / 128);
   xbg::guide_infer(h.g, 0, dF, 9, dN, n, dL, std::min(tiles, sm_count() * 4));
   if ((rc = finish(h.g, "xb_guide_forward")) != XB_OK) return rc;
-  if (cudaMemcpy(lobes, dL, (size_t)rows * xbg::kLobeFloats * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (cudaMemcpy(lobes, dL, (size_t)rows * xbg::kOutRow * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
     return xb::fail(XB_E_CUDA, "xb_guide_forward: copy failed");
   return XB_OK;
 }
@@ -699,7 +713,7 @@ int xb_guide_train(const float* params, const float* recs, int64_t n, int32_t st
   float* dR = s.upload(recs, (size_t)n * xbg::kRecFloats);
   int32_t* dN = s.upload(&cnt, 1);
   if (!dR || !dN) return xb::fail(XB_E_OOM, "xb_guide_train: out of device memory");
-  if (xbg::guide_train(h.g, 0, dR, dN, cnt, steps, batch, lr, seed) != XB_OK)
+  if (xbg::guide_train(h.g, 0, dR, dN, cnt, steps, batch, lr, seed, -1.f) != XB_OK)
     return xb::fail(XB_E_CUDA, "xb_guide_train: launch failed");
   if ((rc = finish(h.g, "xb_guide_train")) != XB_OK) return rc;
   if (cudaMemcpy(params_out, xbg::guide_master(h.g), xbg::kParams * 4, cudaMemcpyDeviceToHost) != cudaSuccess)

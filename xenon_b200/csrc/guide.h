@@ -13,11 +13,15 @@
 namespace xbg {
 
 constexpr int kIn = 64, kHid = 64, kOut = 48, kLobes = 8;
-constexpr int kLobeFloats = 40;  // per row: 8 x (mu xyz, kappa, weight)
+constexpr int kLobeFloats = 40;  // 8 x (mu xyz, kappa, weight)
+constexpr int kSelect = 40;      // raw output holding the selection logit
+constexpr int kOutRow = 41;      // forward output per row: the lobes, then the selection probability
+constexpr float kAMin = 0.05f, kAMax = 0.95f;   // range of the learned selection probability
 // Training record (floats): 0-8 features (position in [0,1]^3, normal, outgoing direction),
 // 9-11 sampled direction omega, 12 weight c (set once the path has finished), 13 path index
-// (int bits), 14-16 throughput before the vertex, 17-19 path radiance before the continuation.
-constexpr int kRecFloats = 20;
+// (int bits), 14-16 throughput before the vertex, 17-19 path radiance before the continuation,
+// 20 density of the BSDF sampler at omega (< 0: the loss uses q alone), 21-23 unused.
+constexpr int kRecFloats = 24;
 // Parameter vector: W0 b0 W1 b1 W2 b2 W3 b3, each W row-major [out][in].
 __host__ __device__ constexpr int off_w(int l) { return 4160 * l; }
 __host__ __device__ constexpr int off_b(int l) { return 4160 * l + (l == 3 ? 3072 : 4096); }
@@ -29,15 +33,17 @@ struct Guide;
 // `rec_cap` training records are allocated with the network (0: none).
 int guide_create(Guide** out, uint64_t seed, int rec_cap);
 void guide_destroy(Guide* g);
-// Lobes (kLobeFloats per row) for rows [0, min(*count, max_rows)) of feats (9 floats used per row,
-// `feat_stride` apart). Device-side count: no host synchronisation.
+// Lobes and selection probability (kOutRow per row) for rows [0, min(*count, max_rows)) of feats
+// (9 floats used per row, `feat_stride` apart). Device-side count: no host synchronisation.
 void guide_infer(Guide* g, cudaStream_t s, const float* feats, int feat_stride, const int32_t* count, int max_rows,
                  float* lobes, int grid);
 // `steps` Adam steps on records [0, min(*rec_count, cap)): each step takes batch / 128 tiles of 128
 // consecutive records at random starts (the whole set, in order, when there are no more records
 // than the batch).
+// alpha_fixed: the selection probability the renderer samples with (< 0: the network's own output,
+// which is then trained too).
 int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_count, int cap, int steps,
-                int batch, float lr, uint64_t seed);
+                int batch, float lr, uint64_t seed, float alpha_fixed);
 // Loss and gradient (no update) over records [0, min(*count, n)) into grad_dev[kParams], loss_dev[1].
 int guide_gradient(Guide* g, cudaStream_t s, const float* recs, const int32_t* count, int n, float* grad_dev,
                    float* loss_dev);

@@ -208,6 +208,11 @@ __device__ __forceinline__ void raw_to_lobes(const float* raw, float* out) {
   }
 }
 
+// Probability of sampling the network at the vertex: kAMin + (kAMax - kAMin) sigmoid(raw[kSelect]).
+__device__ __forceinline__ float selection(const float* raw) {
+  return kAMin + (kAMax - kAMin) / (1.f + expf(-raw[kSelect]));
+}
+
 // kappa / (2 pi (1 - exp(-2 kappa))): the vMF density's normalisation on the unit sphere.
 __device__ __forceinline__ float vmf_norm(float kappa) {
   return kappa / (2.f * kGuidePi * (-expm1f(-2.f * kappa)));

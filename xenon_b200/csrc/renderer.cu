@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(128) shade_kernel(ShadeArgs a) {
 struct GuideShadeArgs {
   const __nv_bfloat16* wf;   // forward weights (bf16)
   const float* master;       // FP32 parameters (biases)
-  float alpha;               // probability of sampling the network
+  float alpha;               // probability of sampling the network (< 0: learned per vertex)
   float bmin[3], binv[3];    // position -> [0,1]^3
   const float* ratio_in;     // importance ratio of each incoming path (nullptr: 1)
   float* ratio_out;
@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
     int32_t pid = 0;
     float n_ratio = 1.f;
     float4 a_o, a_d, a_c, s_o, s_d, s_c;
-    float4 rec[5];
+    float4 rec[6];
     // ── phase 1: emitter test and the network's input ──
     bool alive = false, guided = false;
     float feat[9] = {0.5f, 0.5f, 0.5f, 0.f, 0.f, 1.f, 0.f, 0.f, 1.f};
@@ -616,6 +616,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
       float lo[xbg::kLobeFloats];
       xbg::raw_to_lobes(raw, lo);
       xbg::prepare_lobes(lo, lob);
+      lob[xbg::kPrepRow] = g.alpha >= 0.f ? g.alpha : xbg::selection(raw);
     }
     // ── phase 2: NEE, roulette, the next direction (cpu_tiled.cpp:89-216) ──
     if (alive) do {
@@ -708,7 +709,8 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
         wiw = onb.to_world(s.wi);
       } else {
         float pb;
-        if (rng.next_float() < g.alpha) {
+        const float alpha = lob[xbg::kPrepRow];
+        if (rng.next_float() < alpha) {
           const float u0 = rng.next_float(), u1 = rng.next_float(), u2 = rng.next_float();
           float d[3];
           xbg::mix_sample(lob, u0, u1, u2, d);
@@ -721,7 +723,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
           wiw = onb.to_world(s.wi);
           pb = bsdf_pdf(wo_l, s.wi, mat);
         }
-        const float pm = g.alpha * xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) + (1.f - g.alpha) * pb;
+        const float pm = alpha * xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) + (1.f - alpha) * pb;
         if (!(pm > 0.f)) break;
         n_ratio = ratio * (pb / pm);
         if (training && (pid % g.rec_stride) == 0) {
@@ -731,6 +733,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
           rec[2] = make_float4(feat[8], wiw.x, wiw.y, wiw.z);
           rec[3] = make_float4(0.f, __int_as_float(pid), tb.x, tb.y);
           rec[4] = make_float4(tb.z, kNaN, kNaN, kNaN);   // baseline: set by the next bounce
+          rec[5] = make_float4(pb, 0.f, 0.f, 0.f);
           emit_rec = true;
         }
       }
@@ -755,7 +758,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
       ridx = warp_append(g.rec_count, emit_rec, g.rec_cap, a.stats + STAT_REC_DROPPED);
       if (ridx >= 0) {
         float4* R = reinterpret_cast<float4*>(g.recs + (size_t)ridx * xbg::kRecFloats);
-        for (int i = 0; i < 5; ++i) R[i] = rec[i];
+        for (int i = 0; i < 6; ++i) R[i] = rec[i];
       }
     }
     int idx = warp_append(a.cnt_next + CNT_RAYS, emit_next, a.capacity, a.stats + STAT_OVERFLOW);
@@ -1306,7 +1309,7 @@ int trace_bounces(xb_renderer* r, bool train, int rec_stride) {
       GuideShadeArgs ga;
       ga.wf = xbg::guide_weights_bf16(gd);
       ga.master = xbg::guide_master(gd);
-      ga.alpha = r->gcfg.guide_fraction;
+      ga.alpha = r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f;
       ga.ratio_in = d > 0 ? w.ratio[q] : nullptr;
       ga.ratio_out = w.ratio[nq];
       for (int k = 0; k < 3; ++k) { ga.bmin[k] = r->gbmin[k]; ga.binv[k] = r->gbinv[k]; }
@@ -1400,7 +1403,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       const int steps = r->gcfg.steps_per_spp * spw;
       if (xbg::guide_train(gd, r->stream, xbg::guide_records(gd), xbg::guide_record_count(gd),
                            xbg::guide_record_capacity(gd), steps, r->gcfg.batch, r->gcfg.learning_rate,
-                           r->gcfg.seed) != XB_OK)
+                           r->gcfg.seed, r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f) != XB_OK)
         return set_err(r, XB_E_CUDA, "guide training launch failed");
       r->last_loss_index = steps - 1;
     }
@@ -1964,7 +1967,8 @@ int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
   if (c.seed == 0) c.seed = 1;
   if (c.train_spp < -1 || c.steps_per_spp < 0 || c.steps_per_spp > xbg::kMaxTrainSteps || c.batch < 0 ||
       c.batch % 128 != 0 || c.batch > (1 << 20) || !(c.learning_rate > 0.f) || !(c.guide_fraction > 0.f) ||
-      c.guide_fraction > 1.f || c.max_records < 128 || c.max_records > (1 << 24) || c.record_stride < 0)
+      c.guide_fraction > 1.f || c.max_records < 128 || c.max_records > (1 << 24) || c.record_stride < 0 ||
+      (c.fixed_fraction != 0 && c.fixed_fraction != 1) || (c.keep_training_samples != 0 && c.keep_training_samples != 1))
     return set_err(r, XB_E_INVALID, "xb_set_guiding: bad configuration");
   if (!c.enabled) {
     r->guiding = false;
