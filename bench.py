@@ -59,9 +59,9 @@ def parse():
     ap.add_argument("--no-guiding-study", action="store_true", help="skip the config-4 guided vs plain study")
     ap.add_argument("--no-views-study", action="store_true", help="skip the config-5 batched-views comparison")
     ap.add_argument("--guide-seconds", type=float, default=6.0, help="equal device-time budget per method")
-    ap.add_argument("--guide-ref-spp", type=int, default=2048, help="samples of the plain FP64 reference")
-    ap.add_argument("--guide-train-spp", type=int, default=64)
-    ap.add_argument("--guide-steps-per-spp", type=int, default=32)
+    ap.add_argument("--guide-ref-spp", type=int, default=16384, help="samples of the plain FP64 reference")
+    ap.add_argument("--guide-train-spp", type=int, default=32)
+    ap.add_argument("--guide-steps-per-spp", type=int, default=64)
     ap.add_argument("--guide-fraction", type=float, default=0.0,
                     help="fixed probability of sampling the network (0: learned per vertex)")
     ap.add_argument("--guide-width", type=int, default=1280)

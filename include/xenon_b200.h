@@ -394,10 +394,11 @@ int  xb_bsdf_sample(const xb_material *m, int64_t n, const float *wo, uint64_t *
  * and master weights. */
 typedef struct xb_guiding {
   int32_t enabled;          /* 0: plain BSDF sampling (the reference's estimator) */
-  int32_t train_spp;        /* train on samples 1..train_spp of each pixel; default 64, -1 = never */
-  int32_t steps_per_spp;    /* Adam steps per training sample per pixel; default 32 */
+  int32_t train_spp;        /* train on samples 1..train_spp of each pixel; default 32, -1 = never */
+  int32_t steps_per_spp;    /* Adam steps per training sample per pixel; default 64 */
   int32_t batch;            /* records per Adam step (multiple of 128); default 16384 */
-  float learning_rate;      /* default 5e-3 */
+  float learning_rate;      /* Adam step size at the start, decaying (cosine) to a tenth of it
+                               over train_spp * steps_per_spp steps; default 5e-3 */
   float guide_fraction;     /* probability of sampling the network when fixed_fraction is set;
                                default 0.7 */
   int32_t max_records;      /* training records kept per wave; default 1 << 21 */

@@ -433,7 +433,7 @@ void guide_finalize_records(Guide* g, cudaStream_t s, const float4* L, int grid,
 }
 
 int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_count, int cap, int steps,
-                int batch, float lr, uint64_t seed, float alpha_fixed) {
+                int batch, float lr, uint64_t seed, float alpha_fixed, int64_t total_steps) {
   steps = std::min(steps, g->max_steps);
   batch = std::max(kTile, (batch + kTile - 1) / kTile * kTile);
   const int tiles = batch / kTile;
@@ -449,7 +449,13 @@ int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_
     g->t += 1;
     const float c1 = 1.f - (float)std::pow((double)b1, (double)g->t);
     const float c2 = 1.f - (float)std::pow((double)b2, (double)g->t);
-    adam_kernel<<<64, 256, 0, s>>>(g->master, g->grad, g->mom, g->vel, kParams, lr, b1, b2, 1e-8f, c1, c2);
+    // cosine decay from lr to lr/10 over the planned steps (constant when none are planned)
+    float lr_t = lr;
+    if (total_steps > 0) {
+      const double x = std::min(1.0, (double)(g->t - 1) / (double)total_steps);
+      lr_t = (float)(lr * (0.1 + 0.45 * (1.0 + std::cos(3.14159265358979323846 * x))));
+    }
+    adam_kernel<<<64, 256, 0, s>>>(g->master, g->grad, g->mom, g->vel, kParams, lr_t, b1, b2, 1e-8f, c1, c2);
     guide_sync_bf16(g, s);
   }
   return cudaGetLastError() == cudaSuccess ? XB_OK : XB_E_CUDA;
@@ -713,7 +719,7 @@ int xb_guide_train(const float* params, const float* recs, int64_t n, int32_t st
   float* dR = s.upload(recs, (size_t)n * xbg::kRecFloats);
   int32_t* dN = s.upload(&cnt, 1);
   if (!dR || !dN) return xb::fail(XB_E_OOM, "xb_guide_train: out of device memory");
-  if (xbg::guide_train(h.g, 0, dR, dN, cnt, steps, batch, lr, seed, -1.f) != XB_OK)
+  if (xbg::guide_train(h.g, 0, dR, dN, cnt, steps, batch, lr, seed, -1.f, 0) != XB_OK)
     return xb::fail(XB_E_CUDA, "xb_guide_train: launch failed");
   if ((rc = finish(h.g, "xb_guide_train")) != XB_OK) return rc;
   if (cudaMemcpy(params_out, xbg::guide_master(h.g), xbg::kParams * 4, cudaMemcpyDeviceToHost) != cudaSuccess)

@@ -1403,7 +1403,8 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       const int steps = r->gcfg.steps_per_spp * spw;
       if (xbg::guide_train(gd, r->stream, xbg::guide_records(gd), xbg::guide_record_count(gd),
                            xbg::guide_record_capacity(gd), steps, r->gcfg.batch, r->gcfg.learning_rate,
-                           r->gcfg.seed, r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f) != XB_OK)
+                           r->gcfg.seed, r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f,
+                           (int64_t)r->gcfg.train_spp * r->gcfg.steps_per_spp) != XB_OK)
         return set_err(r, XB_E_CUDA, "guide training launch failed");
       r->last_loss_index = steps - 1;
     }
@@ -1958,8 +1959,8 @@ int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
   if (rc) return rc;
   if (!g) return set_err(r, XB_E_INVALID, "xb_set_guiding: null config");
   xb_guiding c = *g;
-  if (c.train_spp == 0) c.train_spp = 64;
-  if (c.steps_per_spp == 0) c.steps_per_spp = 32;
+  if (c.train_spp == 0) c.train_spp = 32;
+  if (c.steps_per_spp == 0) c.steps_per_spp = 64;
   if (c.batch == 0) c.batch = 16384;
   if (c.learning_rate == 0.f) c.learning_rate = 5e-3f;
   if (c.guide_fraction == 0.f) c.guide_fraction = 0.7f;
