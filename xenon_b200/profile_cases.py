@@ -1,0 +1,66 @@
+"""Small, fixed workloads for profiling single kernels (ncu) through the public API.
+
+    python -m xenon_b200.profile_cases shadow_d0 [W H]      config-2 scene, camera rays and their
+                                                            sun shadow rays only (max_bounces 1)
+    python -m xenon_b200.profile_cases guide_small          config-4 room 320x180, depth 16,
+                                                            guiding with 2 training samples
+    python -m xenon_b200.profile_cases guided_room [W H]    config-4 room, guided bounces with an
+                                                            untrained network (no training launches)
+
+Each case prints one line and exits 0; it renders a handful of samples so a capture of one
+launch ends quickly.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+
+def _lib():
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import xenon_b200 as xb
+    from xenon_b200 import autotune, scenes
+    return xb, autotune, scenes
+
+
+def shadow_d0(w: int = 1920, h: int = 1080) -> None:
+    xb, autotune, scenes = _lib()
+    desc = scenes.icosphere_scene(level=8, width=w, height=h)
+    r = xb.Renderer(w, h, max_bounces=1, min_bounces=3)
+    r.upload_scene(xb.HostScene.from_desc(desc))
+    t = autotune.load_tuning("config2")
+    if t:
+        r.set_tuning(**t)
+    r.render_frame(xb.camera(desc.eye, desc.target, desc.fov, w / h), 1)
+    st = r.stats()
+    print("shadow_d0", w, h, "ms", st.last_ms, "shadow rays", st.rays_shadow)
+
+
+def guide_small() -> None:
+    xb, _, scenes = _lib()
+    w, h = 320, 180
+    desc = scenes.guiding_room(level=6, width=w, height=h)
+    r = xb.Renderer(w, h, max_bounces=16, min_bounces=3)
+    r.upload_scene(xb.HostScene.from_desc(desc))
+    r.set_guiding(True, train_spp=2, steps_per_spp=4, batch=16384)
+    r.render_frame(xb.camera(desc.eye, desc.target, desc.fov, w / h), 6)
+    print("guide_small ms", r.stats().last_ms, r.guiding_stats())
+
+
+def guided_room(w: int = 320, h: int = 180) -> None:
+    xb, _, scenes = _lib()
+    desc = scenes.guiding_room(level=6, width=w, height=h)
+    r = xb.Renderer(w, h, max_bounces=16, min_bounces=3, wave_paths=1 << 19)
+    r.upload_scene(xb.HostScene.from_desc(desc))
+    r.set_guiding(True, train_spp=-1)
+    r.render_frame(xb.camera(desc.eye, desc.target, desc.fov, w / h), 8)
+    print("guided_room ms", r.stats().last_ms)
+
+
+CASES = {"shadow_d0": shadow_d0, "guide_small": guide_small, "guided_room": guided_room}
+
+if __name__ == "__main__":
+    if len(sys.argv) < 2 or sys.argv[1] not in CASES:
+        print(__doc__)
+        sys.exit(2)
+    CASES[sys.argv[1]](*[int(a) for a in sys.argv[2:]])
