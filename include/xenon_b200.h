@@ -291,6 +291,14 @@ typedef struct xb_view {
 int  xb_render_views(xb_renderer *r, const xb_view *views, int32_t count);
 /* Mean radiance, float[W*H*3], top-down rows. */
 int  xb_resolve(xb_renderer *r, float *out_rgb);
+/* xb_resolve without waiting: the mean image of the samples rendered so far is written into
+ * out_rgb (host memory, page-locked for the copy to overlap) while later calls proceed; the
+ * image is complete when xb_sync returns (or when the next-but-one xb_resolve_async has been
+ * enqueued and that call's images were synchronised). Lets a caller hand every sample's image
+ * to the host, as CudaRenderer::render_frame does, without stalling the GPU on the copy. */
+int  xb_resolve_async(xb_renderer *r, float *out_rgb);
+/* Waits for all work of the renderer, including asynchronous resolves. */
+int  xb_sync(xb_renderer *r);
 /* FP64 per-pixel sums and Welford M2 (needs XB_FLAG_FP64_ACCUM); each double[W*H*3]. */
 int  xb_resolve_fp64(xb_renderer *r, double *sum_rgb, double *m2_rgb);
 int  xb_get_spp(const xb_renderer *r);

@@ -108,3 +108,21 @@ def test_converged_cornell_matches_cpu_render(ref):
     print("relmse", relmse(got, want), "max fp32/fp64 diff", np.abs(s64 / spp - got).max())
     assert relmse(got, want) < 1e-3, relmse(got, want)
     assert np.allclose(s64 / spp, got, rtol=1e-3, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_resolve_async_matches_resolve():
+    desc = scenes.cornell()
+    r = Renderer(48, 40, desc.max_bounces, desc.min_bounces)
+    r.upload_scene(HostScene.from_desc(desc))
+    cam = camera(desc.eye, desc.target, desc.fov, 48 / 40)
+    outs = []
+    for k in range(3):
+        r.render_frame(cam, 1)
+        o = np.zeros((40, 48, 3), np.float32)
+        r.resolve_async(o)
+        outs.append(o)
+    r.sync()
+    assert np.array_equal(outs[-1], r.resolve())
+    assert not np.array_equal(outs[0], outs[-1])
+    r.close()

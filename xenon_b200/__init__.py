@@ -179,6 +179,14 @@ class Renderer:
         self._check(lib().xb_resolve(self.h, _p(out)))
         return out
 
+    def resolve_async(self, out: np.ndarray) -> None:
+        """xb_resolve_async into `out` (float32 [H, W, 3], ideally page-locked); complete after sync()."""
+        assert out.dtype == np.float32 and out.size == self.width * self.height * 3
+        self._check(lib().xb_resolve_async(self.h, out.ctypes.data_as(ctypes.c_void_p)))
+
+    def sync(self) -> None:
+        self._check(lib().xb_sync(self.h))
+
     def resolve_fp64(self):
         s = np.empty((self.height, self.width, 3), np.float64)
         m2 = np.empty_like(s)

@@ -58,7 +58,9 @@ enum {
   CNT_FETCH_SH_AREA = 4,
   CNT_FETCH_SH_SUN = 5,
 };
-enum { STAT_RAYS = 0, STAT_SHADOW = 1, STAT_PATHS = 2, STAT_OVERFLOW = 3, STAT_NONFINITE = 4,
+enum { STAT_RAYS = 0, STAT_SHADOW = 1, STAT_PATHS = 2, STAT_OVERFLOW = 3,
+       STAT_OVERFLOW_AT_START = 4,  // STAT_OVERFLOW when the current render call began
+       STAT_NONFINITE = 7,
        STAT_REC_DROPPED = 5,  // guiding: training records beyond the per-wave capacity
        STAT_REC_TOTAL = 6,    // guiding: training records collected
        STAT_EXT_WORK = 8,    // 4 counters: blas nodes, tris, tlas nodes, instances (closest hit)
@@ -120,6 +122,13 @@ struct xb_renderer {
   int spp = 0;                            // samples in the image
   int next_sample = 1;                    // index of the next sample xb_render renders
   float* resolve_buf = nullptr;
+  unsigned long long* host_ov = nullptr;  // page-locked: overflow counter now / at call start
+  // asynchronous resolve: two device images, read back on their own stream
+  float* resolve_async_buf[2] = {nullptr, nullptr};
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t resolved[2] = {nullptr, nullptr};   // image k written on the render stream
+  cudaEvent_t copied[2] = {nullptr, nullptr};     // image k read back
+  int resolve_slot = 0;
   WaveBuffers wb;
   int spp_per_wave = 1;
   unsigned long long* stats = nullptr;    // device totals
@@ -869,6 +878,10 @@ __global__ void resolve_view_kernel(const float4* accum, int W, int H, float inv
   }
 }
 
+__global__ void snapshot_kernel(unsigned long long* stats) {
+  if (threadIdx.x == 0) stats[STAT_OVERFLOW_AT_START] = stats[STAT_OVERFLOW];
+}
+
 // ── accumulate the wave into the framebuffer, in sample order ──────────────────
 __global__ void accumulate_kernel(const float4* L, int64_t npix, int spw, int spp_before,
                                   float4* accum, double* sum64, double* m2_64, double* mean64,
@@ -1496,8 +1509,14 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return bail(xb::fail(XB_E_CUDA, "cudaGetDeviceProperties failed"));
   r->num_sms = prop.multiProcessorCount;
-  if (cudaStreamCreateWithFlags(&r->stream2, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&r->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(xb::fail(XB_E_CUDA, "stream creation failed"));
+  for (int k = 0; k < 2; ++k)
+    if (cudaEventCreateWithFlags(&r->resolved[k], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->copied[k], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(r->copied[k], r->copy_stream) != cudaSuccess)
+      return bail(xb::fail(XB_E_CUDA, "event creation failed"));
   for (int d = 0; d < kMaxDepth; ++d)
     if (cudaEventCreateWithFlags(&r->ev_shade[d], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&r->ev_shadow[d], cudaEventDisableTiming) != cudaSuccess)
@@ -1508,6 +1527,9 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   const int64_t npix = (int64_t)cfg->width * cfg->height;
   if (cudaMalloc(&r->accum, npix * sizeof(float4)) != cudaSuccess ||
       cudaMalloc(&r->resolve_buf, npix * 3 * sizeof(float)) != cudaSuccess ||
+      cudaMallocHost(&r->host_ov, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&r->resolve_async_buf[0], npix * 3 * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&r->resolve_async_buf[1], npix * 3 * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&r->stats, STAT_COUNT * sizeof(unsigned long long)) != cudaSuccess)
     return bail(xb::fail(XB_E_OOM, "framebuffer allocation failed"));
   if (cfg->flags & XB_FLAG_FP64_ACCUM) {
@@ -1572,7 +1594,15 @@ void xb_destroy(xb_renderer* r) {
   free_scene(r);
   free_wave(r);
   xbg::guide_destroy(r->guide);
-  void* ptrs[] = {r->accum, r->sum64, r->m2_64, r->mean64, r->resolve_buf, r->stats, r->scratch};
+  if (r->copy_stream) cudaStreamSynchronize(r->copy_stream);
+  for (int k = 0; k < 2; ++k) {
+    if (r->resolved[k]) cudaEventDestroy(r->resolved[k]);
+    if (r->copied[k]) cudaEventDestroy(r->copied[k]);
+  }
+  if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
+  if (r->host_ov) cudaFreeHost(r->host_ov);
+  void* ptrs[] = {r->accum, r->sum64, r->m2_64, r->mean64, r->resolve_buf, r->stats, r->scratch,
+                  r->resolve_async_buf[0], r->resolve_async_buf[1]};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (cudaEvent_t e : r->ev_pool) cudaEventDestroy(e);
   if (r->ev0) cudaEventDestroy(r->ev0);
@@ -1791,8 +1821,9 @@ int xb_render_range(xb_renderer* r, const xb_camera* cam, int32_t spp_first, int
   if (!r->has_scene) return set_err(r, XB_E_STATE, "xb_render: no scene uploaded");
   if (spp_count < 0 || spp_first < 1) return set_err(r, XB_E_INVALID, "xb_render: bad sample range");
   if (spp_count == 0) return XB_OK;
-  unsigned long long ov_before = 0;
-  CK(cudaMemcpyAsync(&ov_before, r->stats + STAT_OVERFLOW, sizeof(ov_before), cudaMemcpyDeviceToHost, r->stream));
+  // the overflow counter is snapshotted on the device, so the call's only host read comes after
+  // its work (a read at the start would queue behind a pending xb_resolve_async copy)
+  snapshot_kernel<<<1, 32, 0, r->stream>>>(r->stats);
   CK(cudaEventRecord(r->ev0, r->stream));
   int kept = 0;
   rc = run_waves(r, cam, spp_first, spp_count, &kept);
@@ -1800,13 +1831,14 @@ int xb_render_range(xb_renderer* r, const xb_camera* cam, int32_t spp_first, int
   CK(cudaEventRecord(r->ev1, r->stream));
   r->spp += kept;
   r->next_sample = std::max(r->next_sample, spp_first + spp_count);
-  unsigned long long ov_after = 0;
-  CK(cudaMemcpyAsync(&ov_after, r->stats + STAT_OVERFLOW, sizeof(ov_after), cudaMemcpyDeviceToHost, r->stream));
+  CK(cudaMemcpyAsync(r->host_ov, r->stats + STAT_OVERFLOW, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     r->stream));
   CK(cudaStreamSynchronize(r->stream));
   CK(cudaEventElapsedTime(&r->last_ms, r->ev0, r->ev1));
   collect_stage_times(r);
-  if (ov_after != ov_before)
-    return set_err(r, XB_E_OVERFLOW, "%llu queue/stack overflows during render (work dropped)", ov_after - ov_before);
+  if (r->host_ov[0] != r->host_ov[1])
+    return set_err(r, XB_E_OVERFLOW, "%llu queue/stack overflows during render (work dropped)",
+                   r->host_ov[0] - r->host_ov[1]);
   return XB_OK;
 }
 
@@ -1875,6 +1907,34 @@ int xb_render_views(xb_renderer* r, const xb_view* views, int32_t count) {
   cudaFree(out);
   if (ov_after != ov_before)
     return set_err(r, XB_E_OVERFLOW, "%llu queue/stack overflows during render (work dropped)", ov_after - ov_before);
+  return XB_OK;
+}
+
+int xb_resolve_async(xb_renderer* r, float* out) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!out) return set_err(r, XB_E_INVALID, "xb_resolve_async: null output");
+  const int W = r->cfg.width, H = r->cfg.height;
+  const size_t bytes = (size_t)W * H * 3 * sizeof(float);
+  const int k = r->resolve_slot;
+  r->resolve_slot ^= 1;
+  // the image of two calls ago must be read back before this call overwrites its buffer
+  CK(cudaStreamWaitEvent(r->stream, r->copied[k], 0));
+  const float inv = r->spp > 0 ? 1.0f / (float)r->spp : 0.f;
+  resolve_kernel<<<r->num_sms * 8, 256, 0, r->stream>>>(r->accum, W, H, inv, r->resolve_async_buf[k]);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(r->resolved[k], r->stream));
+  CK(cudaStreamWaitEvent(r->copy_stream, r->resolved[k], 0));
+  CK(cudaMemcpyAsync(out, r->resolve_async_buf[k], bytes, cudaMemcpyDeviceToHost, r->copy_stream));
+  CK(cudaEventRecord(r->copied[k], r->copy_stream));
+  return XB_OK;
+}
+
+int xb_sync(xb_renderer* r) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(r->stream));
+  if (r->copy_stream) CK(cudaStreamSynchronize(r->copy_stream));
   return XB_OK;
 }
 
