@@ -274,7 +274,7 @@ int  xb_set_bounces(xb_renderer *r, int32_t min_bounces, int32_t max_bounces);
  * xb_get_spp then counts the image's samples. */
 int  xb_render(xb_renderer *r, const xb_camera *cam, int32_t spp_to_add);
 /* Many views in one call (config 5: dozens of cameras, 256^2 to 1024^2 pixels, 16 to 1024
- * samples): the views share the renderer's scene and bounce limits and are packed together into
+ * samples, bounce limits 6 to 16): the views share the renderer's scene and are packed together into
  * the same waves, so small views still fill the GPU. Each view renders samples 1..spp, seeded as
  * a render of that view alone (seed_pcg(p + k * 0xdeadbeef)), so its image equals a
  * single-view render of the same size; out_rgb receives the view's mean image (host memory,
@@ -285,7 +285,7 @@ typedef struct xb_view {
   xb_camera camera;
   int32_t width, height;
   int32_t spp;
-  int32_t reserved;        /* 0 */
+  int32_t max_bounces;     /* this view's bounce limit (0: the renderer's) */
   float *out_rgb;
 } xb_view;
 int  xb_render_views(xb_renderer *r, const xb_view *views, int32_t count);

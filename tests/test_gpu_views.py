@@ -69,3 +69,43 @@ def test_views_reject_bad_input():
     with pytest.raises(xb.XenonError):
         r.render_views([(cam, 0, 8, 1)])
     r.close()
+
+
+@pytest.mark.gpu
+def test_views_with_their_own_bounce_limits():
+    desc = scenes.cornell()
+    sc = xb.HostScene.from_desc(desc)
+    cam = xb.camera(desc.eye, desc.target, desc.fov, 1.0)
+    r = xb.Renderer(32, 32, max_bounces=8, min_bounces=3)
+    r.upload_scene(sc)
+    views = [(cam, 40, 40, 3, 2), (cam, 24, 24, 5, 5), (cam, 16, 16, 2, 0), (cam, 33, 21, 2, 12)]
+    imgs = r.render_views(views)
+    r.close()
+    for img, (c, w, h, spp, mb) in zip(imgs, views):
+        want = _single(sc, c, w, h, spp, mb or 8)
+        assert np.array_equal(img, want), (w, h, mb)
+
+
+@pytest.mark.gpu
+def test_guided_views_converge_to_plain_views():
+    """One network, trained on the renderer's own view, serves every view of the batch; the
+    guided views estimate the same images as plain ones."""
+    desc = scenes.cornell()
+    sc = xb.HostScene.from_desc(desc)
+    cam = xb.camera(desc.eye, desc.target, desc.fov, 1.0)
+    cam2 = xb.camera((2.0, 6.0, 16.0), (0.0, 4.0, 0.0), 45.0, 1.0)
+    views = [(cam, 48, 48, 1024, 8), (cam2, 40, 40, 1024, 6)]
+    plain = xb.Renderer(48, 48, max_bounces=8, min_bounces=3)
+    plain.upload_scene(sc)
+    pimgs = plain.render_views(views)
+    plain.close()
+    g = xb.Renderer(48, 48, max_bounces=8, min_bounces=3)
+    g.upload_scene(sc)
+    g.set_guiding(True, train_spp=32, steps_per_spp=16, batch=4096)
+    g.render_frame(cam, 32)                            # trains the shared network
+    assert g.guiding_stats()["adam_steps"] == 32 * 16
+    gimgs = g.render_views(views)
+    g.close()
+    for gi, pi in zip(gimgs, pimgs):
+        assert np.all(np.isfinite(gi))
+        assert abs(gi.mean() / pi.mean() - 1.0) < 0.02, (gi.mean(), pi.mean())

@@ -160,15 +160,17 @@ class Renderer:
         self._check(lib().xb_render_range(self.h, ctypes.byref(cam), int(spp_first), int(spp_count)))
 
     def render_views(self, views) -> list:
-        """xb_render_views: views = [(camera, width, height, spp), ...] rendered together in shared
-        waves; returns each view's mean image (height, width, 3), top-down rows."""
+        """xb_render_views: views = [(camera, width, height, spp[, max_bounces]), ...] rendered
+        together in shared waves; returns each view's mean image (height, width, 3), top-down."""
         arr = (abi.View * len(views))()
         outs = []
-        for i, (cam, w, h, spp) in enumerate(views):
+        for i, v in enumerate(views):
+            cam, w, h, spp = v[:4]
             o = np.empty((h, w, 3), np.float32)
             outs.append(o)
             arr[i].camera = cam
             arr[i].width, arr[i].height, arr[i].spp = int(w), int(h), int(spp)
+            arr[i].max_bounces = int(v[4]) if len(v) > 4 else 0
             arr[i].out_rgb = o.ctypes.data
         self._check(lib().xb_render_views(self.h, arr, len(views)))
         return outs

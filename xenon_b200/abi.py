@@ -209,7 +209,7 @@ class SceneConfig(ctypes.Structure):
 class View(ctypes.Structure):
     """xb_view: one camera of xb_render_views and its host output buffer."""
     _fields_ = [("camera", Camera), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
-                ("spp", ctypes.c_int32), ("reserved", ctypes.c_int32), ("out_rgb", ctypes.c_void_p)]
+                ("spp", ctypes.c_int32), ("max_bounces", ctypes.c_int32), ("out_rgb", ctypes.c_void_p)]
 
 
 assert ctypes.sizeof(View) == 72

@@ -97,6 +97,7 @@ struct WaveBuffers {
   int32_t* cnt = nullptr;                 // [kMaxDepth + 1][kCntStride]
   int32_t* rec[2] = {nullptr, nullptr};   // guiding: training record of the emitting vertex
   float* ratio[2] = {nullptr, nullptr};   // guiding: importance ratio of the path
+  int8_t* maxd = nullptr;                 // views: bounce limit of each path
 };
 
 }  // namespace
@@ -317,6 +318,7 @@ struct ShadeArgs {
   int32_t* cnt;         // this depth's counters
   int32_t* cnt_next;    // next depth's counters
   int depth, min_bounces, max_bounces;
+  const int8_t* path_maxd;   // per path bounce limit (views of different depths), or nullptr
   int capacity;
   unsigned long long* stats;
 };
@@ -341,7 +343,7 @@ __device__ __forceinline__ void add_L(float4* L, int p, V3 c) {
 __global__ void __launch_bounds__(128) shade_kernel(ShadeArgs a) {
   const int n = a.cnt[CNT_RAYS];
   const DevScene& sc = a.sc;
-  const bool last = (a.depth + 1 >= a.max_bounces);
+  const bool last_all = (a.depth + 1 >= a.max_bounces);
   for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     const int slot = base + threadIdx.x;
     bool emit_next = false, emit_area = false, emit_sun = false;
@@ -352,6 +354,7 @@ __global__ void __launch_bounds__(128) shade_kernel(ShadeArgs a) {
     if (slot < n) {
       const float4 ro = a.ray_o[slot], rd = a.ray_d[slot], tpv = a.tp[slot];
       pid = a.path[slot];
+      const bool last = a.path_maxd ? (a.depth + 1 >= (int)a.path_maxd[pid]) : last_all;
       Pcg rng{a.rng[slot]};
       const Ray ray{v3(ro.x, ro.y, ro.z), v3(rd.x, rd.y, rd.z), ro.w, rd.w};
       V3 tp = v3(tpv.x, tpv.y, tpv.z);
@@ -539,7 +542,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
   const int n = a.cnt[CNT_RAYS];
   if ((int)blockIdx.x * 128 >= n) return;
   const DevScene& sc = a.sc;
-  const bool last = (a.depth + 1 >= a.max_bounces);
+  const bool last_all = (a.depth + 1 >= a.max_bounces);
   const bool training = g.recs != nullptr;
   xbg::load_forward_weights(sW, sBias, g.wf, g.master);
   xbg::mma_setup(&tmem_slot, &mbar);
@@ -695,7 +698,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
           emit_sun = true;
         }
       }
-      if (last) break;
+      if (a.path_maxd ? (a.depth + 1 >= (int)a.path_maxd[pid]) : last_all) break;
       if (a.depth >= a.min_bounces) {
         // cpu_tiled.cpp:190-194 on the plain throughput: p = max(0.05, max(tp)), survive with
         // min(1, p), divide by p. Its part above 1 is a deterministic rescale and stays as is;
@@ -791,6 +794,7 @@ struct ViewPiece {
   CamDev cam;
   int W, H;
   int s_first, spp;        // 1-based first sample index, samples of every pixel in this wave
+  int max_bounces;         // the view's bounce limit
   int64_t path_off;        // first path of the piece in the wave
   int64_t pix_off;         // first pixel of the piece in the wave's pixel list
   int64_t accum_off;       // first pixel of the view in the accumulation buffer
@@ -801,7 +805,7 @@ struct ViewPieces {
 };
 
 __global__ void raygen_views_kernel(ViewPieces pk, int64_t paths, float4* ray_o, float4* ray_d, float4* tp,
-                                    uint64_t* rng, int32_t* path, float4* L, int32_t* cnt) {
+                                    uint64_t* rng, int32_t* path, float4* L, int8_t* maxd, int32_t* cnt) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < paths;
        p += (int64_t)gridDim.x * blockDim.x) {
     int i = 0;
@@ -824,6 +828,7 @@ __global__ void raygen_views_kernel(ViewPieces pk, int64_t paths, float4* ray_o,
     rng[p] = g.state;
     path[p] = (int32_t)p;
     L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    maxd[p] = (int8_t)v.max_bounces;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt[CNT_RAYS] = (int32_t)paths;
 }
@@ -1102,7 +1107,7 @@ void free_wave(xb_renderer* r) {
   void* ptrs[] = {w.ray_o[0], w.ray_o[1], w.ray_d[0], w.ray_d[1], w.tp[0], w.tp[1], w.rng[0],
                   w.rng[1], w.path[0], w.path[1], w.hit, w.hit_inst, w.sh_o[0], w.sh_o[1],
                   w.sh_d[0], w.sh_d[1], w.sh_c[0], w.sh_c[1], w.L, w.cnt, w.rec[0], w.rec[1],
-                  w.ratio[0], w.ratio[1]};
+                  w.ratio[0], w.ratio[1], w.maxd};
   for (void* p : ptrs) if (p) cudaFree(p);
   w = WaveBuffers();
 }
@@ -1147,6 +1152,7 @@ int alloc_wave(xb_renderer* r, int64_t cap) {
     ok &= A(&w.ratio[q], cap * sizeof(float));
   }
   ok &= A(&w.hit, cap * sizeof(float4));
+  ok &= A(&w.maxd, cap * sizeof(int8_t));
   ok &= A(&w.hit_inst, cap * sizeof(int32_t));
   ok &= A(&w.L, cap * sizeof(float4));
   ok &= A(&w.cnt, (kMaxDepth + 1) * kCntStride * sizeof(int32_t));
@@ -1295,9 +1301,9 @@ void launch_shadows(xb_renderer* r, int d, bool count, cudaStream_t s) {
 // run on the first: the two only share the scene (shadow rays add to the path radiance, closest
 // hits write the hit records), and shading d+1 waits for both. Each kernel's tail — a few warps
 // finishing long rays after the queue has drained — then runs beside the other kernel's bulk.
-int trace_bounces(xb_renderer* r, bool train, int rec_stride) {
+int trace_bounces(xb_renderer* r, bool train, int rec_stride, int depth_limit = -1, const int8_t* path_maxd = nullptr) {
   WaveBuffers& w = r->wb;
-  const int depth_max = std::min(r->max_bounces, kMaxDepth);
+  const int depth_max = std::min(depth_limit >= 0 ? depth_limit : r->max_bounces, kMaxDepth);
   const bool count = (r->prof_flags & XB_PROFILE_COUNT_TRAVERSAL) != 0;
   const bool ov = r->tune.overlap == 1 && r->stream2 != nullptr;
   xbg::Guide* gd = r->guiding ? r->guide : nullptr;
@@ -1316,6 +1322,7 @@ int trace_bounces(xb_renderer* r, bool train, int rec_stride) {
     sa.cnt = cd_;
     sa.cnt_next = w.cnt + (d + 1) * kCntStride;
     sa.depth = d; sa.min_bounces = r->min_bounces; sa.max_bounces = depth_max;
+    sa.path_maxd = path_maxd;
     sa.capacity = (int)w.capacity;
     sa.stats = r->stats;
     if (gd) {
@@ -1459,6 +1466,7 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
       p.path_off = paths;
       p.pix_off = pix_total;
       p.accum_off = accum_off[v];
+      p.max_bounces = std::min(views[v].max_bounces > 0 ? views[v].max_bounces : r->max_bounces, kMaxDepth);
       paths += npix * n;
       pix_total += npix;
       left[v] -= n;
@@ -1471,14 +1479,16 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
     {
       StageTimer t(r, STAGE_RAYGEN);
       raygen_views_kernel<<<g_rg, 256, 0, r->stream>>>(pk, paths, w.ray_o[0], w.ray_d[0], w.tp[0], w.rng[0],
-                                                       w.path[0], w.L, w.cnt);
+                                                       w.path[0], w.L, w.maxd, w.cnt);
     }
-    int rc = trace_bounces(r, false, 1);
+    int wave_depth = 0;
+    for (int i = 0; i < pk.n; ++i) wave_depth = std::max(wave_depth, pk.p[i].max_bounces);
+    int rc = trace_bounces(r, false, 1, wave_depth, w.maxd);
     if (rc) return rc;
     const int g_acc = (int)std::min<int64_t>((pix_total + 255) / 256, (int64_t)r->num_sms * 16);
     {
       StageTimer t(r, STAGE_ACCUM);
-      accumulate_views_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, pk, pix_total, accum, w.cnt, depth_max, paths,
+      accumulate_views_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, pk, pix_total, accum, w.cnt, wave_depth, paths,
                                                             r->stats);
     }
     CK(cudaGetLastError());
@@ -1856,8 +1866,8 @@ int xb_render_views(xb_renderer* r, const xb_view* views, int32_t count) {
   int64_t total = 0, max_npix = 0;
   for (int v = 0; v < count; ++v) {
     const xb_view& vw = views[v];
-    if (vw.width <= 0 || vw.height <= 0 || vw.spp < 0 || !vw.out_rgb ||
-        (int64_t)vw.width * vw.height > (1ll << 26))
+    if (vw.width <= 0 || vw.height <= 0 || vw.spp < 0 || !vw.out_rgb || vw.max_bounces < 0 ||
+        vw.max_bounces > kMaxDepth || (int64_t)vw.width * vw.height > (1ll << 26))
       return set_err(r, XB_E_INVALID, "xb_render_views: view %d has a bad size, sample count or output", v);
     off[v] = total;
     const int64_t npix = (int64_t)vw.width * vw.height;
