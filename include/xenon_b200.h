@@ -384,6 +384,12 @@ int  xb_bsdf_eval(const xb_material *m, int64_t n, const float *wo, const float 
  * bit1 = delta lobe. */
 int  xb_bsdf_sample(const xb_material *m, int64_t n, const float *wo, uint64_t *rng_state,
                     float *wi, float *f_rgb, float *pdf, int32_t *flags);
+/* The true density with which xb_bsdf_sample returns wi (per steradian, over all lobes), for
+ * non-delta, non-transmissive materials seen from the front (wo.z > 0; 0 otherwise). For the GGX
+ * lobes it is the returned pdf times cos^4 of the half vector's angle: the reference's GGX
+ * distribution (bsdf.h:67-76) carries an extra 1/cos^4 while its sampler draws the standard
+ * distribution. Guided sampling weighs by this density. No reference counterpart. */
+int  xb_bsdf_density(const xb_material *m, int64_t n, const float *wo, const float *wi, float *density);
 
 /* ── learned path guiding (no reference counterpart: the reference has no learned part) ── */
 

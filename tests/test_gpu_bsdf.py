@@ -72,3 +72,34 @@ def test_sample_matches_reference(name, ref):
     for got_, want_ in ((p, p_r), (f, f_r)):
         e = rel_err(got_[ok], want_[ok])
         assert e.max() < 1e-2 and np.quantile(e, 0.999) < 1e-4 and np.median(e) < 1e-6, (name, e.max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,mat", [
+    ("conductor r0.3", abi.material(base_color=(0.9, 0.6, 0.5), metallic=1.0, roughness=0.3)),
+    ("conductor r0.7", abi.material(base_color=(0.9, 0.6, 0.5), metallic=1.0, roughness=0.7)),
+    ("plastic", abi.material(base_color=(0.5, 0.5, 0.5), roughness=0.6)),
+    ("aniso", abi.material(base_color=(0.9, 0.9, 0.9), metallic=1.0, roughness=0.4, anisotropy=0.6)),
+    ("lambert", abi.material(base_color=(0.6, 0.6, 0.6), roughness=1.0, ior=1.0))])
+def test_bsdf_density_is_the_sampler_density(name, mat):
+    """xb_bsdf_density integrates, band by band in cos(theta), to the fraction of xb_bsdf_sample's
+    directions that land there (the stated GGX pdf does not: it is off by cos^4 theta_h)."""
+    rng = np.random.default_rng(3)
+    n = 400_000
+    for th in (0.3, 1.1):
+        wo1 = np.array([np.sin(th), 0.0, np.cos(th)], np.float32)
+        wo = np.tile(wo1, (n, 1))
+        states = rng.integers(1, 2 ** 63, n, dtype=np.uint64)
+        wi, f, pdf, flags, _ = xb.bsdf_sample(mat, wo, states)
+        ok = (flags & 1) == 1
+        edges = np.linspace(0, 1, 9)
+        frac = np.histogram(wi[ok, 2], bins=edges)[0] / n
+        M = 200_000
+        for k, (a, b) in enumerate(zip(edges[:-1], edges[1:])):
+            z = rng.uniform(a, b, M)
+            ph = rng.uniform(0, 2 * np.pi, M)
+            r = np.sqrt(1 - z * z)
+            d = np.stack([r * np.cos(ph), r * np.sin(ph), z], 1).astype(np.float32)
+            integral = xb.bsdf_density(mat, np.tile(wo1, (M, 1)), d).astype(np.float64).mean() * 2 * np.pi * (b - a)
+            se = np.sqrt(frac[k] / n) + 0.03 * integral + 2e-4     # sampling + quadrature error
+            assert abs(frac[k] - integral) < 4 * se, (name, th, k, frac[k], integral)

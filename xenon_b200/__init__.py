@@ -287,6 +287,16 @@ def bsdf_eval(mat: np.ndarray, wo: np.ndarray, wi: np.ndarray):
     return f, pdf
 
 
+def bsdf_density(mat: np.ndarray, wo: np.ndarray, wi: np.ndarray) -> np.ndarray:
+    """True density of bsdf_sample's directions (xb_bsdf_density)."""
+    wo = np.ascontiguousarray(wo, np.float32)
+    wi = np.ascontiguousarray(wi, np.float32)
+    out = np.empty(len(wo), np.float32)
+    m = np.ascontiguousarray(mat, np.float32)
+    check(lib().xb_bsdf_density(_p(m), len(wo), _p(wo), _p(wi), _p(out)))
+    return out
+
+
 def bsdf_sample(mat: np.ndarray, wo: np.ndarray, states):
     wo = np.ascontiguousarray(wo, np.float32)
     n = len(wo)

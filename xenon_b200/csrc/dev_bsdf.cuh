@@ -371,46 +371,61 @@ __device__ __forceinline__ bool bsdf_sample(V3 wo, const DevMaterial& m, Pcg& rn
   return true;
 }
 
-// ── the sampler's lobe values for a given direction (guided sampling; no reference counterpart)
-// For a non-delta material seen from its front side (wo.z > 0), bsdf_sample draws a lobe l with
-// probability P_l and a direction from that lobe's density pdf_l, and returns f_l and
-// P_l pdf_l. Given a direction wi drawn by another proposal, this returns what the sampler
-// would have returned had it produced wi: a lobe chosen with its posterior probability
-// P_l pdf_l(wi) / sum_k P_k pdf_k(wi) (u selects it), that lobe's f and P_l pdf_l, and the
-// sampler's marginal density sum_k P_k pdf_k(wi) (equal to bsdf_pdf for these materials).
-// Returns false where the sampler cannot produce wi.
+// ── the sampler's true densities (guided sampling; no reference counterpart) ──────
+// The reference's anisotropic GGX distribution (ggx_d_aniso, bsdf.h:67-76) squares
+// cos^4(theta_h) (1 + tan^2 ...) in its denominator, so every pdf built on it is the density of
+// the standard GGX visible normals divided by cos^4(theta_h). Its sampler (sample_vndf, Heitz
+// 2018) draws the standard visible normals, so the density of what mfr_sample actually returns
+// is the stated pdf times cos^4(theta_h). The plain tracer never needs the difference (it divides
+// f by the pdf of its own sample, where D cancels), but guided sampling weighs directions drawn
+// elsewhere by the sampler's density, which must be the true one.
+__device__ __forceinline__ float cos4(float c) { const float c2 = c * c; return c2 * c2; }
+
+__device__ __forceinline__ float mfr_density(V3 wo, V3 wi, const DevMaterial& m) {
+  const float p = mfr_pdf(wo, wi, m);
+  if (!(p > 0.f)) return 0.f;
+  return p * cos4(normalize(wo + wi).z);
+}
+
+// For a non-delta, non-transmissive material seen from its front side (wo.z > 0), bsdf_sample
+// draws a lobe l with probability P_l and a direction from that lobe, returning f_l and its
+// stated P_l pdf_l. Given a direction wi drawn by another proposal, this returns what the sampler
+// would have returned had it produced wi — a lobe chosen with its posterior P_l d_l(wi) /
+// sum_k P_k d_k(wi) (d: true densities; u selects it), that lobe's f and stated P_l pdf_l — and
+// the sampler's true marginal density sum_k P_k d_k(wi). Returns false where the sampler cannot
+// produce wi.
 __device__ __forceinline__ bool bsdf_lobe_for_direction(V3 wo, V3 wi, const DevMaterial& m, float u, V3& f,
-                                                        float& pdf_sel, float& pdf_marg) {
+                                                        float& pdf_sel, float& density) {
   if (m.flags & kMatConductor) {
-    pdf_sel = pdf_marg = mfr_pdf(wo, wi, m);
+    pdf_sel = mfr_pdf(wo, wi, m);
+    density = mfr_density(wo, wi, m);
     f = mfr_eval(wo, wi, m);
   } else if (m.flags & kMatSubsurface) {
-    pdf_sel = pdf_marg = diffuse_pdf(wi);
+    pdf_sel = density = diffuse_pdf(wi);
     f = (wi.z > 0.f) ? ss_color(m) * (1.f - m.metallic) * kInvPi : v3s(0.f);
-  } else if (m.flags & kMatTransmissive) {
-    const float fr = fresnel_dielectric(fabsf(wo.z), m.ior);
-    if (wi.z > 0.f) {
-      pdf_sel = fr * mfr_pdf(wo, wi, m);
-      f = mfr_eval(wo, wi, m);
-    } else {
-      pdf_sel = (1.f - fr) * mft_pdf(wo, wi, m);
-      f = mft_eval(wo, wi, m);
-    }
-    pdf_marg = pdf_sel;
   } else {
     const float spec = sclamp(m.f0[0], 0.f, 1.f), diff = 1.f - spec;
-    const float ps = spec * mfr_pdf(wo, wi, m), pd = diff * diffuse_pdf(wi);
-    pdf_marg = ps + pd;
-    if (!(pdf_marg > 0.f)) return false;
-    if (u * pdf_marg < ps) {
-      pdf_sel = ps;
+    const float ds = spec * mfr_density(wo, wi, m), dd = diff * diffuse_pdf(wi);
+    density = ds + dd;
+    if (!(density > 0.f)) return false;
+    if (u * density < ds) {
+      pdf_sel = spec * mfr_pdf(wo, wi, m);
       f = mfr_eval(wo, wi, m);
     } else {
-      pdf_sel = pd;
+      pdf_sel = dd;
       f = diffuse_eval(wi, m);
     }
   }
-  return pdf_sel >= 1e-8f && pdf_marg > 0.f;
+  return pdf_sel >= 1e-8f && density > 0.f;
+}
+
+// The true density with which bsdf_sample (front side; non-delta, non-transmissive material)
+// returns wi, over all lobes.
+__device__ __forceinline__ float bsdf_density(V3 wo, V3 wi, const DevMaterial& m) {
+  if (m.flags & kMatConductor) return mfr_density(wo, wi, m);
+  if (m.flags & kMatSubsurface) return diffuse_pdf(wi);
+  const float spec = sclamp(m.f0[0], 0.f, 1.f);
+  return spec * mfr_density(wo, wi, m) + (1.f - spec) * diffuse_pdf(wi);
 }
 
 }  // namespace xbd

@@ -503,7 +503,8 @@ __global__ void __launch_bounds__(128) shade_kernel(ShadeArgs a) {
 
 // ── guided shade: one bounce with the learned proposal (no reference counterpart) ──────
 // Guiding here importance-samples the plain estimator: at a guided vertex the direction comes
-// from the mixture p = a q_guide + (1 - a) p_bsdf (p_bsdf the density of bsdf_sample) and the
+// from the mixture p = a q_guide + (1 - a) p_bsdf (p_bsdf the true density of bsdf_sample, see
+// bsdf_density) and the
 // vertex keeps everything the plain sampler would have produced for that direction (the lobe,
 // its f and pdf, hence the MIS weights and the Russian-roulette throughput), while the path
 // carries the importance ratio prod p_bsdf / p as a separate scalar. The expectation therefore
@@ -607,9 +608,14 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
         }
         if (!hit_light) {
           alive = true;
-          // The network proposes at non-delta vertices seen from the front of the shading
-          // normal, where the sampler's density is bsdf_pdf; elsewhere the plain sampler runs.
-          guided = (sc.mats[fh.mat_id].flags & kMatDelta) == 0 && dot(fh.normal, -ray.d) > 0.f;
+          // The network proposes at non-delta, non-transmissive vertices seen from the front of
+          // the shading normal, where the density of bsdf_sample is known (bsdf_density);
+          // elsewhere the plain sampler runs. Rough dielectrics stay plain: the reference
+          // evaluates their transmission with a half vector (wo + wi / ior) other than the one
+          // its sampler refracts about (and its pdf can be NaN there), so neither its pdf nor a
+          // corrected form of it is the density of what its sampler returns.
+          const uint32_t mf = sc.mats[fh.mat_id].flags;
+          guided = (mf & (kMatDelta | kMatTransmissive)) == 0 && dot(fh.normal, -ray.d) > 0.f;
           for (int k = 0; k < 3; ++k) {
             const float pk = (k == 0 ? fh.pos.x : k == 1 ? fh.pos.y : fh.pos.z);
             feat[k] = fminf(fmaxf((pk - g.bmin[k]) * g.binv[k], 0.f), 1.f);
@@ -733,7 +739,7 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
         } else {
           if (!bsdf_sample(wo_l, mat, rng, s)) break;
           wiw = onb.to_world(s.wi);
-          pb = bsdf_pdf(wo_l, s.wi, mat);
+          pb = bsdf_density(wo_l, s.wi, mat);
         }
         const float pm = alpha * xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) + (1.f - alpha) * pb;
         if (!(pm > 0.f)) break;
@@ -998,6 +1004,15 @@ __global__ void bsdf_eval_kernel(DevMaterial m, int64_t n, const float* wo, cons
     V3 fv = bsdf_eval(o, w, m);
     f[3 * i] = fv.x; f[3 * i + 1] = fv.y; f[3 * i + 2] = fv.z;
     pdf[i] = bsdf_pdf(o, w, m);
+  }
+}
+
+__global__ void bsdf_density_kernel(DevMaterial m, int64_t n, const float* wo, const float* wi, float* dens) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const V3 o = v3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
+    const V3 w = v3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+    dens[i] = (o.z > 0.f && !(m.flags & (kMatDelta | kMatTransmissive))) ? bsdf_density(o, w, m) : 0.f;
   }
 }
 
@@ -2255,6 +2270,23 @@ int xb_bsdf_eval(const xb_material* m, int64_t n, const float* wo, const float* 
   cudaError_t e = cudaMemcpy(pdf, dp, n * sizeof(float), cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (e != cudaSuccess) return xb::fail(XB_E_CUDA, "xb_bsdf_eval: %s", cudaGetErrorString(e));
+  return XB_OK;
+}
+
+int xb_bsdf_density(const xb_material* m, int64_t n, const float* wo, const float* wi, float* density) {
+  if (!m || n < 0 || (n > 0 && (!wo || !wi || !density)))
+    return xb::fail(XB_E_INVALID, "xb_bsdf_density: bad arguments");
+  if (n == 0) return XB_OK;
+  float* d = nullptr;
+  if (cudaMalloc(&d, (size_t)n * 7 * sizeof(float)) != cudaSuccess)
+    return xb::fail(XB_E_OOM, "xb_bsdf_density: out of device memory");
+  float *dwo = d, *dwi = d + 3 * n, *dd = d + 6 * n;
+  cudaMemcpy(dwo, wo, n * 3 * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(dwi, wi, n * 3 * sizeof(float), cudaMemcpyHostToDevice);
+  bsdf_density_kernel<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256>>>(to_dev_material(*m), n, dwo, dwi, dd);
+  cudaError_t e = cudaMemcpy(density, dd, n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return xb::fail(XB_E_CUDA, "xb_bsdf_density: %s", cudaGetErrorString(e));
   return XB_OK;
 }
 
