@@ -58,11 +58,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--thread-per-ray", action="store_true", help="one-ray-per-thread traversal kernels")
     ap.add_argument("--no-guiding-study", action="store_true", help="skip the config-4 guided vs plain study")
-    ap.add_argument("--no-views-study", action="store_true", help="skip the config-5 batched-views comparison")
+    ap.add_argument("--no-views-study", action="store_true", help="skip the config-5 many-views study")
+    ap.add_argument("--views-max-spp", type=int, default=64, help="config 5: cap on a view's spp (0: none)")
     ap.add_argument("--guide-seconds", type=float, default=6.0, help="equal device-time budget per method")
     ap.add_argument("--guide-ref-spp", type=int, default=16384, help="samples of the plain FP64 reference")
-    ap.add_argument("--guide-train-spp", type=int, default=32)
-    ap.add_argument("--guide-steps-per-spp", type=int, default=64)
+    ap.add_argument("--guide-train-spp", type=int, default=64, help="config 4: trained on the first 64 spp")
+    ap.add_argument("--guide-steps-per-spp", type=int, default=32)
     ap.add_argument("--guide-fraction", type=float, default=0.0,
                     help="fixed probability of sampling the network (0: learned per vertex)")
     ap.add_argument("--guide-width", type=int, default=1280)
@@ -268,7 +269,8 @@ def guiding_study(args, device: int) -> dict:
     """Config 4: equal device-time relMSE of the guided and the plain wavefront against a plain
     FP64 reference. Both methods render in chunks of samples until their summed device time
     (CUDA events of each xb_render call) reaches the budget; the guided budget includes its
-    online training (the first train_spp samples, which are part of its image)."""
+    online training on the first train_spp samples, of which the second half (rendered once
+    half of the Adam steps are taken) is part of its image."""
     import xenon_b200 as xb
     from xenon_b200 import scenes
     W, H = args.guide_width, args.guide_height
@@ -306,7 +308,7 @@ def guiding_study(args, device: int) -> dict:
             fixed = args.guide_fraction > 0
             r.set_guiding(True, train_spp=args.guide_train_spp, steps_per_spp=args.guide_steps_per_spp,
                           batch=16384, guide_fraction=args.guide_fraction if fixed else 0.7,
-                          fixed_fraction=1 if fixed else 0)
+                          fixed_fraction=1 if fixed else 0, keep_training_samples=2)
         ms, rendered, chunk = 0.0, 0, 8
         while ms < args.guide_seconds * 1e3:
             r.render_frame(cam, chunk)
@@ -314,13 +316,13 @@ def guiding_study(args, device: int) -> dict:
             rendered += chunk
             if guided and rendered == args.guide_train_spp:
                 info["train_phase_ms"] = ms
-        spp = r.spp                              # image samples (training samples excluded)
+        spp = r.spp                              # image samples (the first half of training excluded)
         img = r.resolve().astype(np.float64)
         if guided:
             info.update(r.guiding_stats())
             info["config"] = {k: v for k, v in r.guiding().items() if k in
                               ("train_spp", "steps_per_spp", "batch", "learning_rate", "guide_fraction",
-                               "fixed_fraction")}
+                               "fixed_fraction", "keep_training_samples")}
         r.close()
         e = (img - ref) ** 2 / denom
         pix = e.mean(2).ravel()
@@ -344,41 +346,86 @@ def guiding_study(args, device: int) -> dict:
             "wall_s": time.perf_counter() - t0}
 
 
-def views_study(desc, hs, device: int) -> dict:
-    """Config 5 (reduced: 32 views of 256^2 or 512^2 pixels, 16 samples each): the same views
-    rendered by one xb_render_views call (shared waves) and one after the other (a renderer per
-    view size, one xb_render each), device time of the calls."""
+def views_study(args, device: int) -> dict:
+    """Config 5: 32 seeded views of the config-3 instanced scene (side log-uniform 256-1024 px,
+    spp from {16, 64, 256, 1024} capped at --views-max-spp, bounce limit 6-16) in one
+    xb_render_views call with guiding on — one network, trained on the scene's own view
+    (64 spp), serves every view — then per-view relMSE of those images against plain renders of
+    the same views with 4x the samples. For context: the same views plain, batched and one by one."""
     import xenon_b200 as xb
     from xenon_b200 import scenes
-    specs = scenes.orbit_views(desc, 32, seed=1, sizes=(256, 512), spps=(16,))
-    cams = [xb.camera(e, t, f, w / h) for (e, t, f, w, h, _) in specs]
-    views = [(c, w, h, spp) for c, (_, _, _, w, h, spp) in zip(cams, specs)]
-    paths = sum(w * h * spp for (_, w, h, spp) in views)
-    r = xb.Renderer(512, 512, desc.max_bounces, desc.min_bounces, device=device)
-    r.upload_scene(hs)
-    r.render_views(views[:2])                          # warm-up
+    desc = scenes.instanced_grid()
+    hs = xb.HostScene.from_desc(desc)
+    specs = scenes.config5_views(desc, 32, seed=1, max_spp=args.views_max_spp)
+    cams = [xb.camera(e, t, f, w / h) for (e, t, f, w, h, _, _) in specs]
+    views = [(c, w, h, spp, mb) for c, (_, _, _, w, h, spp, mb) in zip(cams, specs)]
+    paths = sum(w * h * spp for (_, w, h, spp, _) in views)
+    maxb = max(mb for (*_, mb) in views)
+
+    def renderer(w=512, h=512):
+        r = xb.Renderer(w, h, maxb, desc.min_bounces, device=device)
+        r.upload_scene(hs)
+        return r
+
+    # plain: batched vs one by one, and the 4x reference
+    r = renderer()
+    r.render_views(views[:2])
     r.reset_stats()
-    r.render_views(views)
-    batched_ms = r.stats().last_ms
+    plain_imgs = r.render_views(views)
+    plain_ms = r.stats().last_ms
     r.close()
-    rs = {}
     seq_ms = 0.0
-    for (c, w, h, spp) in views:
-        if (w, h) not in rs:
-            rr = xb.Renderer(w, h, desc.max_bounces, desc.min_bounces, device=device)
-            rr.upload_scene(hs)
-            rr.render_frame(c, 1)                      # warm-up
-            rs[(w, h)] = rr
-        rr = rs[(w, h)]
+    refs = []
+    for (c, w, h, spp, mb) in views:
+        rr = renderer(w, h)
+        rr.set_bounces(desc.min_bounces, mb)
+        rr.render_frame(c, 1)
         rr.reset()
         rr.render_frame(c, spp)
         seq_ms += rr.stats().last_ms
-    for rr in rs.values():
+        # the reference: 4x the samples at indices no timed render uses
+        rr.reset()
+        rr.render_range(c, 1 << 24, 4 * spp)
+        refs.append(rr.resolve())
         rr.close()
-    return {"workload": "config5 (reduced): 32 orbit views of the config-2 scene, 256^2 or 512^2 px, 16 spp",
-            "paths": paths, "batched_ms": batched_ms, "sequential_ms": seq_ms,
-            "batched_msamples_per_s": paths / batched_ms / 1e3, "sequential_msamples_per_s": paths / seq_ms / 1e3,
-            "speedup": seq_ms / max(batched_ms, 1e-9)}
+    # guided: one shared network, trained on the scene's own view
+    g = renderer(desc.width, desc.height)
+    g.set_guiding(True, train_spp=64, steps_per_spp=32)
+    main_cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
+    g.render_frame(main_cam, 64)
+    train_ms = g.stats().last_ms
+    g.reset_stats()
+    guided_imgs = g.render_views(views)
+    guided_ms = g.stats().last_ms
+    g.close()
+
+    def relmse(img, ref):
+        """Per-pixel relative squared error, channel mean: (raw mean, mean without the 0.1% largest
+        pixels). Caustic paths (light through the glass instances) leave a few pixels per view
+        thousands of times brighter than their mean in plain and guided renders alike; the raw
+        mean follows those few pixels, the trimmed one the rest of the image."""
+        img, ref = img.astype(np.float64), ref.astype(np.float64)
+        e = np.sort(((img - ref) ** 2 / (ref ** 2 + 1e-2)).mean(axis=2).ravel())
+        k = max(1, e.size // 1000)
+        return float(e.mean()), float(e[:-k].mean())
+    per_view = []
+    for (c, w, h, spp, mb), gi, pi, rf in zip(views, guided_imgs, plain_imgs, refs):
+        (g_raw, g_trim), (p_raw, p_trim) = relmse(gi, rf), relmse(pi, rf)
+        per_view.append({"size": w, "spp": spp, "max_bounces": mb, "relmse_guided": g_raw, "relmse_plain": p_raw,
+                         "relmse_guided_trimmed": g_trim, "relmse_plain_trimmed": p_trim})
+    raw = [v["relmse_plain"] / max(v["relmse_guided"], 1e-30) for v in per_view]
+    trim = [v["relmse_plain_trimmed"] / max(v["relmse_guided_trimmed"], 1e-30) for v in per_view]
+    speed = plain_ms / guided_ms   # relMSE falls as 1/samples: equal time scales the ratio by it
+    return {"workload": "config5: 32 views of config 3 (16x16 instances), side 256-1024 px log-uniform, "
+                        f"spp from {{16,64,256,1024}} capped at {args.views_max_spp}, depth 6-16",
+            "paths": paths, "guided_msamples_per_s": paths / guided_ms / 1e3, "guided_ms": guided_ms,
+            "guide_training_ms": train_ms, "plain_batched_msamples_per_s": paths / plain_ms / 1e3,
+            "plain_one_by_one_msamples_per_s": paths / seq_ms / 1e3,
+            "relmse_ratio_plain_over_guided_median": float(np.median(raw)),
+            "relmse_ratio_plain_over_guided_median_trimmed": float(np.median(trim)),
+            "relmse_ratio_equal_time_median_trimmed": float(np.median(trim)) * speed,
+            "relmse": "mean over pixels of (x - ref)^2 / (ref^2 + 0.01); trimmed: without the 0.1% largest pixels",
+            "reference": "plain renders of the same views with 4x the samples", "per_view": per_view}
 
 
 def main():
@@ -523,7 +570,7 @@ def main():
     views = None
     if rank == 0 and ws == 1 and not args.no_views_study:
         try:
-            views = views_study(desc, hs, local)
+            views = views_study(args, local)
         except Exception as e:
             views = {"error": f"{type(e).__name__}: {e}"}
     guiding = None

@@ -404,7 +404,8 @@ int  xb_bsdf_density(const xb_material *m, int64_t n, const float *wo, const flo
  * its guided vertices. The guided image therefore converges to the plain tracer's image for any
  * network and any scene. The network is trained online, on the first train_spp samples per
  * pixel, by Adam on the radiance-weighted negative log-likelihood of p at the sampled directions;
- * the training samples are part of the image. BF16 tensor cores (tcgen05), FP32 accumulation
+ * keep_training_samples says which of the training samples go into the image. BF16 tensor
+ * cores (tcgen05), FP32 accumulation
  * and master weights. */
 typedef struct xb_guiding {
   int32_t enabled;          /* 0: plain BSDF sampling (the reference's estimator) */
@@ -421,7 +422,9 @@ typedef struct xb_guiding {
   float bounds_min[3];      /* box mapped to [0,1]^3 for the network's position input; */
   float bounds_max[3];      /* an empty box selects the scene's bounds */
   int32_t keep_training_samples;  /* 0: samples 1..train_spp train the network only and stay out
-                                   * of the image (xb_get_spp counts image samples) */
+                                   * of the image (xb_get_spp counts image samples); 1: they are
+                                   * kept; 2: those after train_spp / 2 (rendered once half of
+                                   * the Adam steps are taken) are kept */
   int32_t fixed_fraction;   /* 0: the network also outputs the probability of sampling it at each
                              * vertex (in [0.05, 0.95], trained with the mixture);
                              * 1: guide_fraction everywhere */

@@ -127,6 +127,29 @@ def test_guide_params_round_trip_and_stats():
     r.close()
 
 
+@pytest.mark.gpu
+def test_keep_training_samples_modes():
+    """0: the training samples stay out; 1: all kept; 2: those after train_spp / 2 kept; the
+    kept ones are exactly the samples a plain accumulation of those indices would add."""
+    _, sc, cam = _room()
+    imgs = {}
+    for keep, want in ((0, 2), (1, 6), (2, 4)):
+        r = xb.Renderer(W, H, max_bounces=16, min_bounces=3)
+        r.upload_scene(sc)
+        r.set_guiding(True, train_spp=4, steps_per_spp=2, batch=1024, seed=3, keep_training_samples=keep)
+        r.render_frame(cam, 6)
+        assert r.spp == want and r.guiding_stats()["adam_steps"] == 8
+        imgs[keep] = r.resolve().copy()
+        r.close()
+    # samples 5-6 are common to every mode; mode 2 adds samples 3-4 and mode 1 samples 1-4
+    assert not np.array_equal(imgs[0], imgs[2]) and not np.array_equal(imgs[2], imgs[1])
+    r = xb.Renderer(W, H, max_bounces=16, min_bounces=3)
+    r.upload_scene(sc)
+    with pytest.raises(xb.XenonError):
+        r.set_guiding(True, keep_training_samples=3)
+    r.close()
+
+
 def _ground_box(kind):
     """A sky-lit 40x40 ground with a rotated box: an opaque dielectric (diffuse + GGX specular
     lobes) or a GGX conductor box — the lobes whose sampler density differs from the reference's

@@ -582,16 +582,14 @@ namespace {
 
 __global__ void mixture_pdf_kernel(const float* lobes, int64_t rows, const float* dirs, float* pdf) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
-    float P[xbg::kPrepRow];
-    xbg::prepare_lobes(lobes + i * xbg::kLobeFloats, P);
+    const float* P = lobes + i * xbg::kLobeFloats;
     pdf[i] = xbg::mix_pdf(P, dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]);
   }
 }
 
 __global__ void mixture_sample_kernel(const float* lobes, int64_t rows, const float* u, float* dirs, float* pdf) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows; i += (int64_t)gridDim.x * blockDim.x) {
-    float L[xbg::kPrepRow];
-    xbg::prepare_lobes(lobes + i * xbg::kLobeFloats, L);
+    const float* L = lobes + i * xbg::kLobeFloats;
     float d[3];
     xbg::mix_sample(L, u[3 * i], u[3 * i + 1], u[3 * i + 2], d);
     dirs[3 * i] = d[0]; dirs[3 * i + 1] = d[1]; dirs[3 * i + 2] = d[2];

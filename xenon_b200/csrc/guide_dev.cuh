@@ -30,6 +30,14 @@ __device__ __forceinline__ void store8_bf16(uint8_t* tile, int r, int k0, int K,
   *reinterpret_cast<uint4*>(tile + xbd::kmajor_offset(r, k0, K)) = *reinterpret_cast<const uint4*>(h);
 }
 
+// (lo, hi) -> bf16x2 (lo in the low half), each max(x, 0) rounded to nearest: one
+// cvt.rn.relu.bf16x2.f32, the same bits as rounding fmaxf(x, 0.f).
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+
 __device__ __forceinline__ float load_bf16(const uint8_t* tile, int r, int k, int K) {
   return __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(tile + xbd::kmajor_offset(r, k, K)));
 }
@@ -61,7 +69,10 @@ __device__ __forceinline__ void load_forward_weights(uint8_t* sW, float* sBias, 
 // [0,1]^3 (k < 6), the normal (k < 2) and the outgoing direction (k < 2), then p xyz and 1.
 // f: p01 xyz, n xyz, wo xyz. One sincospif per coordinate; the higher octaves follow from the
 // double-angle identities sin 2a = 2 sin a cos a, cos 2a = 1 - 2 sin^2 a (error doubling per
-// octave stays far below the bf16 rounding of the result).
+// octave stays far below the bf16 rounding of the result). kFast: __sincosf(pi x) instead
+// (|pi x| <= pi here: absolute error below 1e-6 before the doublings, 3e-5 after the fifth,
+// against the bf16 step of 4e-3 at 1).
+template <bool kFast = false>
 __device__ __forceinline__ void encode_row(const float* f, uint8_t* tile, int r) {
   float x[kIn];
 #pragma unroll
@@ -69,7 +80,8 @@ __device__ __forceinline__ void encode_row(const float* f, uint8_t* tile, int r)
     const int nf = c < 3 ? 6 : 2;
     const int o = c < 3 ? 12 * c : 36 + 4 * (c - 3);
     float s, co;
-    sincospif(f[c], &s, &co);
+    if (kFast) __sincosf(kGuidePi * f[c], &s, &co);
+    else sincospif(f[c], &s, &co);
 #pragma unroll
     for (int k = 0; k < nf; ++k) {
       x[o + 2 * k] = s;
@@ -154,10 +166,11 @@ __device__ __forceinline__ void hidden_epilogue(const Mma& m, const float* bias,
   for (int c = 0; c < kHid; c += 16) {
     float v[16];
     m.load16(c, v);
+    uint32_t h[8];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i] + bias[c + i], 0.f);
-    store8_bf16(dst, r, c, kK, v);
-    store8_bf16(dst, r, c + 8, kK, v + 8);
+    for (int i = 0; i < 8; ++i) h[i] = relu_bf16x2(v[2 * i] + bias[c + 2 * i], v[2 * i + 1] + bias[c + 2 * i + 1]);
+    *reinterpret_cast<uint4*>(dst + xbd::kmajor_offset(r, c, kK)) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(dst + xbd::kmajor_offset(r, c + 8, kK)) = make_uint4(h[4], h[5], h[6], h[7]);
   }
 }
 
@@ -183,7 +196,10 @@ __device__ __forceinline__ void forward_tile(Mma& m, uint8_t* sA, const uint8_t*
 }
 
 // Lobe k from raw[5k .. 5k+4]: mu = m / sqrt(|m|^2 + 1e-8), kappa = exp(clamp(raw, -4, 6)),
-// weights = softmax. Writes mu xyz, kappa, w per lobe (stride 5) to `out`.
+// weights = softmax. Writes mu xyz, kappa, w per lobe (stride 5) to `out`. kFast: exponentials
+// and the reciprocal through the hardware approximations (__expf, __fdividef: a few ulp), as the
+// renderer's guided bounce evaluates them; training keeps the correctly rounded forms.
+template <bool kFast = false>
 __device__ __forceinline__ void raw_to_lobes(const float* raw, float* out) {
   float mx = -3.0e38f;
 #pragma unroll
@@ -192,10 +208,10 @@ __device__ __forceinline__ void raw_to_lobes(const float* raw, float* out) {
   float e[kLobes];
 #pragma unroll
   for (int k = 0; k < kLobes; ++k) {
-    e[k] = expf(raw[5 * k + 4] - mx);
+    e[k] = kFast ? __expf(raw[5 * k + 4] - mx) : expf(raw[5 * k + 4] - mx);
     sum += e[k];
   }
-  const float inv = 1.f / sum;
+  const float inv = kFast ? __fdividef(1.f, sum) : 1.f / sum;
 #pragma unroll
   for (int k = 0; k < kLobes; ++k) {
     const float* m = raw + 5 * k;
@@ -203,61 +219,57 @@ __device__ __forceinline__ void raw_to_lobes(const float* raw, float* out) {
     out[5 * k] = m[0] * rs;
     out[5 * k + 1] = m[1] * rs;
     out[5 * k + 2] = m[2] * rs;
-    out[5 * k + 3] = expf(fminf(fmaxf(m[3], -4.f), 6.f));
+    const float lk = fminf(fmaxf(m[3], -4.f), 6.f);
+    out[5 * k + 3] = kFast ? __expf(lk) : expf(lk);
     out[5 * k + 4] = e[k] * inv;
   }
 }
 
 // Probability of sampling the network at the vertex: kAMin + (kAMax - kAMin) sigmoid(raw[kSelect]).
+template <bool kFast = false>
 __device__ __forceinline__ float selection(const float* raw) {
-  return kAMin + (kAMax - kAMin) / (1.f + expf(-raw[kSelect]));
+  return kFast ? kAMin + __fdividef(kAMax - kAMin, 1.f + __expf(-raw[kSelect]))
+               : kAMin + (kAMax - kAMin) / (1.f + expf(-raw[kSelect]));
 }
 
 // kappa / (2 pi (1 - exp(-2 kappa))): the vMF density's normalisation on the unit sphere.
 __device__ __forceinline__ float vmf_norm(float kappa) {
   return kappa / (2.f * kGuidePi * (-expm1f(-2.f * kappa)));
 }
-
-// Lobes prepared for evaluation, kPrepFloats per lobe: mu xyz, kappa, weight, and
-// weight * vmf_norm(kappa) (the lobe's density at its mean direction, times its weight).
-constexpr int kPrepFloats = 6;
-constexpr int kPrepRow = kLobes * kPrepFloats;
-
-__device__ __forceinline__ void prepare_lobes(const float* lob5, float* out) {
-#pragma unroll
-  for (int k = 0; k < kLobes; ++k) {
-    const float* L = lob5 + 5 * k;
-    float* o = out + kPrepFloats * k;
-    o[0] = L[0]; o[1] = L[1]; o[2] = L[2]; o[3] = L[3]; o[4] = L[4];
-    o[5] = L[4] * vmf_norm(L[3]);
-  }
+// The same through __expf / __fdividef. kappa >= e^-4 here, so 1 - e^{-2 kappa} >= 0.036 and
+// its absolute error of a few 1e-7 stays below 1e-5 relative.
+__device__ __forceinline__ float vmf_norm_fast(float kappa) {
+  return __fdividef(kappa, 2.f * kGuidePi * (1.f - __expf(-2.f * kappa)));
 }
 
-// Mixture pdf (per steradian) of the unit direction (x, y, z):
+// Mixture pdf (per steradian) of the unit direction (x, y, z), from the lobes as raw_to_lobes
+// writes them (mu xyz, kappa, w per lobe):
 //   q = sum_k w_k kappa_k / (2 pi (1 - e^{-2 kappa_k})) e^{kappa_k (mu_k . w - 1)}
-__device__ __forceinline__ float mix_pdf(const float* P, float x, float y, float z) {
+// The renderer samples with mix_sample and weighs with this pdf; both read the same stored
+// lobes, so the pdf is the sampler's density up to the rounding of the approximations.
+__device__ __forceinline__ float mix_pdf(const float* L5, float x, float y, float z) {
   float q = 0.f;
 #pragma unroll
   for (int k = 0; k < kLobes; ++k) {
-    const float* L = P + kPrepFloats * k;
+    const float* L = L5 + 5 * k;
     const float c = L[0] * x + L[1] * y + L[2] * z;
-    q += L[5] * expf(L[3] * (c - 1.f));
+    q += L[4] * vmf_norm_fast(L[3]) * __expf(L[3] * (c - 1.f));
   }
   return q;
 }
 
 // A direction from the mixture: u0 picks the lobe by its weight, u1 the angle to the mean
 // (inverse CDF of the vMF: cos = 1 + log(u1 + (1 - u1) e^{-2 kappa}) / kappa), u2 the azimuth.
-__device__ __forceinline__ void mix_sample(const float* P, float u0, float u1, float u2, float* d) {
+__device__ __forceinline__ void mix_sample(const float* L5, float u0, float u1, float u2, float* d) {
   int k = 0;
-  float cdf = P[4];
+  float cdf = L5[4];
   while (k < kLobes - 1 && u0 > cdf) {
     ++k;
-    cdf += P[kPrepFloats * k + 4];
+    cdf += L5[5 * k + 4];
   }
-  const float* L = P + kPrepFloats * k;
+  const float* L = L5 + 5 * k;
   const float kp = L[3];
-  float c = 1.f + logf(u1 + (1.f - u1) * expf(-2.f * kp)) / kp;
+  float c = 1.f + __fdividef(__logf(u1 + (1.f - u1) * __expf(-2.f * kp)), kp);
   c = fminf(fmaxf(c, -1.f), 1.f);
   const float s = sqrtf(fmaxf(0.f, 1.f - c * c));
   float sp, cp;

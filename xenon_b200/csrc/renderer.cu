@@ -528,15 +528,18 @@ struct GuideShadeArgs {
 };
 
 constexpr float kNaN = __builtin_nanf("");
-constexpr int kLobStride = xbg::kPrepRow + 1;   // conflict-free per-thread rows
+constexpr int kLobStride = xbg::kLobeFloats + 1;   // conflict-free per-thread rows
+// The lobes of a tile's rows take the activation tile's place once its last layer has run.
+constexpr size_t kLobBytes = (size_t)xbg::kTile * kLobStride * 4;
 constexpr size_t kGuidedShadeSmem =
-    xbg::kFwdWeightBytes + xbg::kTileBytes + (size_t)xbg::kTile * kLobStride * 4 + 1024;
+    xbg::kFwdWeightBytes + (kLobBytes > xbg::kTileBytes ? kLobBytes : xbg::kTileBytes) + 1024;
 
-__global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideShadeArgs g) {
+// 128 registers and 55 KB of shared memory: four CTAs (16 warps) per SM.
+__global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, GuideShadeArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sW = smem;
   uint8_t* sA = smem + xbg::kFwdWeightBytes;
-  float* sLob = reinterpret_cast<float*>(sA + xbg::kTileBytes);
+  float* sLob = reinterpret_cast<float*>(sA);
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_slot;
   __shared__ float sBias[xbg::kBiasFloats];
@@ -626,15 +629,16 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
       }
     }
     // ── the network on this CTA's 128 vertices ──
-    xbg::encode_row(feat, sA, threadIdx.x);
+    __syncthreads();   // the previous tile's lobes, in the same shared memory, are all read
+    xbg::encode_row<true>(feat, sA, threadIdx.x);
+    float alpha;
     {
       float raw[xbg::kOut];
       xbg::forward_tile(m, sA, sW, sBias, raw);
       if (!m.ok) break;   // uniform: every thread saw the same failed wait
-      float lo[xbg::kLobeFloats];
-      xbg::raw_to_lobes(raw, lo);
-      xbg::prepare_lobes(lo, lob);
-      lob[xbg::kPrepRow] = g.alpha >= 0.f ? g.alpha : xbg::selection(raw);
+      // every thread is past the last layer's completion: the activation tile is free
+      xbg::raw_to_lobes<true>(raw, lob);
+      alpha = g.alpha >= 0.f ? g.alpha : xbg::selection<true>(raw);
     }
     // ── phase 2: NEE, roulette, the next direction (cpu_tiled.cpp:89-216) ──
     if (alive) do {
@@ -727,7 +731,6 @@ __global__ void __launch_bounds__(128) guided_shade_kernel(ShadeArgs a, GuideSha
         wiw = onb.to_world(s.wi);
       } else {
         float pb;
-        const float alpha = lob[xbg::kPrepRow];
         if (rng.next_float() < alpha) {
           const float u0 = rng.next_float(), u1 = rng.next_float(), u2 = rng.next_float();
           float d[3];
@@ -1426,7 +1429,8 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       StageTimer t(r, STAGE_ACCUM);
       // samples rendered while the guide trains stay out of the image unless asked for (their
       // proposal is the still-untrained network); the kernel still counts the wave's rays
-      const bool keep = !train || r->gcfg.keep_training_samples != 0;
+      const bool keep = !train || r->gcfg.keep_training_samples == 1 ||
+                        (r->gcfg.keep_training_samples == 2 && 2 * (sample0 - 1) >= r->gcfg.train_spp);
       accumulate_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, npix, keep ? spw : 0, r->spp + kept, r->accum,
                                                       r->sum64, r->m2_64, r->mean64, w.cnt, depth_max, paths,
                                                       r->stats);
@@ -2054,7 +2058,7 @@ int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
   if (c.train_spp < -1 || c.steps_per_spp < 0 || c.steps_per_spp > xbg::kMaxTrainSteps || c.batch < 0 ||
       c.batch % 128 != 0 || c.batch > (1 << 20) || !(c.learning_rate > 0.f) || !(c.guide_fraction > 0.f) ||
       c.guide_fraction > 1.f || c.max_records < 128 || c.max_records > (1 << 24) || c.record_stride < 0 ||
-      (c.fixed_fraction != 0 && c.fixed_fraction != 1) || (c.keep_training_samples != 0 && c.keep_training_samples != 1))
+      (c.fixed_fraction != 0 && c.fixed_fraction != 1) || c.keep_training_samples < 0 || c.keep_training_samples > 2)
     return set_err(r, XB_E_INVALID, "xb_set_guiding: bad configuration");
   if (!c.enabled) {
     r->guiding = false;

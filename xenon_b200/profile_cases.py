@@ -6,6 +6,7 @@
                                                             guiding with 2 training samples
     python -m xenon_b200.profile_cases guided_room [W H]    config-4 room, guided bounces with an
                                                             untrained network (no training launches)
+    python -m xenon_b200.profile_cases plain_room [W H]     the same renders with plain sampling
 
 Each case prints one line and exits 0; it renders a handful of samples so a capture of one
 launch ends quickly.
@@ -47,17 +48,23 @@ def guide_small() -> None:
     print("guide_small ms", r.stats().last_ms, r.guiding_stats())
 
 
-def guided_room(w: int = 320, h: int = 180) -> None:
+def guided_room(w: int = 320, h: int = 180, guided: bool = True) -> None:
     xb, _, scenes = _lib()
     desc = scenes.guiding_room(level=6, width=w, height=h)
     r = xb.Renderer(w, h, max_bounces=16, min_bounces=3, wave_paths=1 << 19)
     r.upload_scene(xb.HostScene.from_desc(desc))
-    r.set_guiding(True, train_spp=-1)
+    if guided:
+        r.set_guiding(True, train_spp=-1)
     r.render_frame(xb.camera(desc.eye, desc.target, desc.fov, w / h), 8)
-    print("guided_room ms", r.stats().last_ms)
+    print("guided_room" if guided else "plain_room", "ms", r.stats().last_ms)
 
 
-CASES = {"shadow_d0": shadow_d0, "guide_small": guide_small, "guided_room": guided_room}
+def plain_room(w: int = 320, h: int = 180) -> None:
+    guided_room(w, h, guided=False)
+
+
+CASES = {"shadow_d0": shadow_d0, "guide_small": guide_small, "guided_room": guided_room,
+         "plain_room": plain_room}
 
 if __name__ == "__main__":
     if len(sys.argv) < 2 or sys.argv[1] not in CASES:

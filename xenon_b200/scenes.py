@@ -407,3 +407,27 @@ def orbit_views(desc: SceneDesc, n: int = 32, seed: int = 1, sizes=VIEW_SIZES, s
         s = int(rng.choice(sizes))
         out.append((tuple(float(x) for x in eye), tuple(float(x) for x in c), 40.0, s, s, int(rng.choice(spps))))
     return out
+
+
+def config5_views(desc: SceneDesc, n: int = 32, seed: int = 1, max_spp: int | None = None) -> list:
+    """Config 5: n square views of the scene from the seed — side log-uniform in [256, 1024] px,
+    spp from {16, 64, 256, 1024} (capped at max_spp when given), bounce limit uniform in 6..16 —
+    looking at the scene's centre from the upper hemisphere at 0.6-1.2 scene radii.
+    Returns [(eye, target, fov, width, height, spp, max_bounces), ...]."""
+    lo, hi = scene_bounds(desc)
+    c = (lo + hi) / 2
+    rad = float(np.linalg.norm(hi - lo)) / 2
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        d = rng.normal(size=3)
+        d[1] = abs(d[1]) + 0.3
+        d /= np.linalg.norm(d)
+        eye = c + d * rad * rng.uniform(0.6, 1.2)
+        side = int(round(float(np.exp(rng.uniform(np.log(256), np.log(1024))))))
+        spp = int(rng.choice(VIEW_SPP))
+        if max_spp:
+            spp = min(spp, max_spp)
+        out.append((tuple(float(x) for x in eye), tuple(float(x) for x in c), 45.0, side, side, spp,
+                    int(rng.integers(6, 17))))
+    return out
