@@ -42,7 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Mrays/s; equal-time relMSE, guided vs plain GPU wavefront (1×B200)"
-WORKLOAD = "config2: displaced icosphere L8 (1,310,722 tris incl. ground) 1920x1080, depth 10, 1 spp/step"
+WORKLOAD = "config2: displaced icosphere L8 (1,310,722 tris incl. ground) 1920x1080, depth 10"
 
 
 def parse():
@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = config 2)")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--spp-per-step", type=int, default=4,
+                    help="samples per pixel rendered by one xb_render call (one step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--thread-per-ray", action="store_true", help="one-ray-per-thread traversal kernels")
@@ -469,9 +471,10 @@ def main():
 
     # warm-up
     r.set_profiling(0)
-    base = rank * (args.steps + args.warmup + 8) + 1
+    sps = args.spp_per_step
+    base = rank * (args.steps + args.warmup + 8) * sps + 1
     for s in range(args.warmup):
-        r.render_range(cam, base + s, 1)
+        r.render_range(cam, base + s * sps, sps)
     r.reset()
     r.reset_stats()
     r.reset_profile()
@@ -485,7 +488,7 @@ def main():
         for s in range(args.steps):
             flush.zero_()                      # L2 flush between timed steps (outside the events)
             torch.cuda.synchronize()
-            r.render_range(cam, base + args.warmup + s, 1)
+            r.render_range(cam, base + (args.warmup + s) * sps, sps)
             dev_ms += r.stats().last_ms
     torch.cuda.synchronize()
     barrier(ws)
@@ -513,11 +516,33 @@ def main():
             tj = json.load(f)
         if tj.get("dram_bytes_per_closest_ray"):
             traffic = tj["dram_bytes_per_closest_ray"] * st.rays_closest / max(prof.extend_launches, 1)
+    # the same kernel with one wave in flight (untimed pass): its launches then have the GPU to
+    # themselves, while in the timed region the other lane's kernels run beside them
+    lanes = r.tuning()["waves"]
+    one_lane = None
+    if lanes == 2:
+        r.set_tuning(waves=1)
+        r.reset_profile()
+        r.reset_stats()
+        n1 = max(3, min(args.steps, 10))
+        for s in range(n1):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r.render_range(cam, base + (args.warmup + args.steps + s) * sps, sps)
+        p1 = r.profile()
+        a1 = ext_bytes_per_ray * r.stats().rays_closest / max(p1.extend_ms * 1e-3, 1e-12) / 1e9
+        one_lane = {"achieved": a1, "frac": a1 / peaks["hbm_gbs"], "extend_ms_per_launch":
+                    p1.extend_ms / max(p1.extend_launches, 1)}
+        r.set_tuning(waves=2)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                 "peak_source": peaks["source"], "kernel": "extend_kernel (closest-hit traversal)",
-                "algorithmic_bytes_per_ray": ext_bytes_per_ray, "extend_share_of_step":
-                    prof.extend_ms / max(dev_ms, 1e-9), **work}
+                "algorithmic_bytes_per_ray": ext_bytes_per_ray,
+                "extend_launch_ms_per_step": prof.extend_ms / args.steps, "waves_in_flight": lanes,
+                "note": "two waves in flight: in the timed region each extend launch shares the GPU with "
+                        "the other lane's kernels, so its duration includes that sharing; one_lane is the "
+                        "same kernel with one wave in flight" if lanes == 2 else None,
+                "one_lane": one_lane, **work}
 
     # e2e through the public API with host buffers: render + resolve to pinned host memory
     host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True)
@@ -526,7 +551,7 @@ def main():
     host2 = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True)
     outs = (host, host2)
     for s in range(2):                       # untimed warm-up of the same calls
-        xb.native.check(L.xb_render(r.h, ctypes.byref(cam), 1), r.h)
+        xb.native.check(L.xb_render(r.h, ctypes.byref(cam), sps), r.h)
         xb.native.check(L.xb_resolve_async(r.h, ctypes.c_void_p(outs[s % 2].data_ptr())), r.h)
     xb.native.check(L.xb_sync(r.h), r.h)
     r.reset()
@@ -536,8 +561,8 @@ def main():
     t0 = time.perf_counter()
     e2e_steps = max(3, min(args.steps, 20))
     for s in range(e2e_steps):
-        xb.native.check(L.xb_render(r.h, ctypes.byref(cam), 1), r.h)
-        # every sample's mean image goes to the host; the copy of sample k overlaps sample k+1
+        xb.native.check(L.xb_render(r.h, ctypes.byref(cam), sps), r.h)
+        # every step's mean image goes to the host; the copy of step k overlaps step k+1
         xb.native.check(L.xb_resolve_async(r.h, ctypes.c_void_p(outs[s % 2].data_ptr())), r.h)
     xb.native.check(L.xb_sync(r.h), r.h)
     torch.cuda.synchronize()
@@ -548,9 +573,9 @@ def main():
     e2e = {"value": e2e_rays / e2e_s / 1e6, "unit": "Mrays/s",
            "h2d_bytes_per_step": int(ctypes.sizeof(cam)),
            "d2h_bytes_per_step": int(W * H * 3 * 4), "steps": e2e_steps,
-           "note": "host wall clock over back-to-back samples (no L2 flush between them, unlike "
-                   "`value`); each sample's mean image is read back by xb_resolve_async, overlapping "
-                   "the next sample, and xb_sync ends the timed region"}
+           "note": f"host wall clock over back-to-back steps of {sps} spp (no L2 flush between them, "
+                   "unlike `value`); each step's mean image is read back by xb_resolve_async, "
+                   "overlapping the next step, and xb_sync ends the timed region"}
 
     # the single exchange of the multi-GPU path: framebuffer reduce to rank 0 (untimed)
     if ws > 1:
@@ -585,7 +610,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded procedural scene, seed 1)",
-                "config": {"workload": WORKLOAD, "paths_per_step": npix, "rays_per_path": rays_per_path,
+                "config": {"workload": WORKLOAD, "spp_per_step": sps, "paths_per_step": npix * sps,
+                           "rays_per_path": rays_per_path,
                            "msamples_per_s": msamples, "l2": "flushed between timed steps (256 MiB write)",
                            "parallelism": f"sample-sharded x{ws}" if ws > 1 else "1 GPU",
                            "tuning": r.tuning(), "tuning_source": "xenon_b200/tuning (autotuner)" if tuned else "defaults",

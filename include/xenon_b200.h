@@ -334,6 +334,11 @@ typedef struct xb_tuning {
   int32_t overlap;                      /* 1: a bounce's shadow rays run on a second stream,
                                            concurrently with the next bounce's closest hits;
                                            2: one stream */
+  int32_t waves;                        /* waves in flight: 2 (default) runs consecutive waves
+                                           on two stream lanes at once (twice the queue
+                                           memory); 1 one at a time. Same image either way. */
+  int32_t lane_stagger;                 /* with two lanes, a call's second wave starts once the
+                                           first has shaded this many bounces (1-16) */
 } xb_tuning;
 int  xb_set_tuning(xb_renderer *r, const xb_tuning *t);
 int  xb_get_tuning(const xb_renderer *r, xb_tuning *out);

@@ -8,6 +8,8 @@ two passes), and keeps the fastest setting:
   shadow_persistent              persistent warps or one ray per thread for shadow rays
   shadow_order                   nearer or farther child first for shadow (any-hit) rays
   overlap                        shadow rays of a bounce concurrent with the next bounce's closest hits
+  waves                          waves in flight (two stream lanes or one)
+  lane_stagger                   bounces the first lane shades before the second lane starts
   refill                         idle lanes that trigger a warp refill
   extend/shadow/shade_blocks_per_sm   resident blocks per SM (grid size)
   wave_paths                     paths in flight per wave (queue capacity)
@@ -29,6 +31,8 @@ SPACE = {
     "shadow_persistent": [1, 2],
     "shadow_order": [1, 2],
     "overlap": [1, 2],
+    "waves": [1, 2],
+    "lane_stagger": [1, 2, 3],
     "refill": [2, 4, 8, 16, 24],
     "extend_blocks_per_sm": [3, 4, 5, 6, 64],
     "shadow_blocks_per_sm": [3, 4, 5, 6, 64],
@@ -57,25 +61,26 @@ def load_tuning(workload: str, gpu: str | None = None) -> dict | None:
     return None
 
 
-def measure(renderer, cam, spp: int, first: int) -> float:
-    """Device ms per sample over `spp` samples (after one warm-up sample)."""
-    renderer.render_range(cam, first, 1)
+def measure(renderer, cam, calls: int, spp_per_call: int, first: int) -> float:
+    """Device ms per sample over `calls` xb_render calls of `spp_per_call` samples each (after
+    one warm-up call); several waves per call, so two waves in flight are measured as used."""
+    renderer.render_range(cam, first, spp_per_call)
     ms = 0.0
-    for k in range(spp):
-        renderer.render_range(cam, first + 1 + k, 1)
+    for k in range(calls):
+        renderer.render_range(cam, first + (1 + k) * spp_per_call, spp_per_call)
         ms += renderer.stats().last_ms
-    return ms / spp
+    return ms / (calls * spp_per_call)
 
 
-def autotune(renderer, cam, workload: str, spp: int = 4, passes: int = 2, save: bool = True,
-             log=print) -> dict:
+def autotune(renderer, cam, workload: str, calls: int = 4, spp_per_call: int = 4, passes: int = 2,
+             save: bool = True, log=print) -> dict:
     best = dict(renderer.tuning())
     seq = [1000]
 
     def run(t):
         renderer.set_tuning(**t)
-        seq[0] += spp + 1
-        return measure(renderer, cam, spp, seq[0])
+        seq[0] += (calls + 1) * spp_per_call
+        return measure(renderer, cam, calls, spp_per_call, seq[0])
 
     best_ms = run(best)
     log(f"start {best_ms:.3f} ms/spp {best}")
@@ -110,7 +115,8 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="config2")
     ap.add_argument("--out", default=None, help="also write the result JSON here")
-    ap.add_argument("--spp", type=int, default=4, help="samples per measurement")
+    ap.add_argument("--calls", type=int, default=4, help="xb_render calls per measurement")
+    ap.add_argument("--spp-per-call", type=int, default=4, help="samples per xb_render call")
     ap.add_argument("--from-saved", action="store_true", help="start from the stored tuning")
     a = ap.parse_args()
     if a.workload == "config2":
@@ -127,7 +133,7 @@ if __name__ == "__main__":
     cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
     if a.from_saved and load_tuning(a.workload):
         r.set_tuning(**load_tuning(a.workload))
-    res = autotune(r, cam, a.workload, spp=a.spp)
+    res = autotune(r, cam, a.workload, calls=a.calls, spp_per_call=a.spp_per_call)
     print(json.dumps(res))
     if a.out:
         with open(a.out, "w") as f:

@@ -109,6 +109,14 @@ struct xb_renderer {
   cudaStream_t stream2 = nullptr;         // shadow rays, concurrent with the next bounce's hits
   cudaEvent_t ev_shade[kMaxDepth] = {};   // bounce d's shading done (its shadow queues are full)
   cudaEvent_t ev_shadow[kMaxDepth] = {};  // bounce d's shadow rays done (path radiance final)
+  // the second wave lane (two waves in flight): its own queues, streams and per-bounce events
+  WaveBuffers wb_b;
+  cudaStream_t stream_b = nullptr, stream_b2 = nullptr;
+  cudaEvent_t ev_shade_b[kMaxDepth] = {};
+  cudaEvent_t ev_shadow_b[kMaxDepth] = {};
+  cudaEvent_t lane_done[2] = {nullptr, nullptr};   // each lane's last wave finished
+  cudaEvent_t lane_acc[2] = {nullptr, nullptr};    // each lane's last accumulation finished
+  cudaEvent_t ev_fork = nullptr;                   // the main stream's work before a call's waves
   int num_sms = 0;
   std::string err;
   // scene
@@ -1120,14 +1128,19 @@ void free_scene(xb_renderer* r) {
   std::memset(&r->scene, 0, sizeof(r->scene));
 }
 
-void free_wave(xb_renderer* r) {
-  WaveBuffers& w = r->wb;
+void free_wave_buffers(WaveBuffers& w) {
   void* ptrs[] = {w.ray_o[0], w.ray_o[1], w.ray_d[0], w.ray_d[1], w.tp[0], w.tp[1], w.rng[0],
                   w.rng[1], w.path[0], w.path[1], w.hit, w.hit_inst, w.sh_o[0], w.sh_o[1],
                   w.sh_d[0], w.sh_d[1], w.sh_c[0], w.sh_c[1], w.L, w.cnt, w.rec[0], w.rec[1],
                   w.ratio[0], w.ratio[1], w.maxd};
   for (void* p : ptrs) if (p) cudaFree(p);
   w = WaveBuffers();
+}
+
+void free_wave(xb_renderer* r) {
+  for (cudaStream_t s : {r->stream, r->stream2, r->stream_b, r->stream_b2}) if (s) cudaStreamSynchronize(s);
+  free_wave_buffers(r->wb);
+  free_wave_buffers(r->wb_b);
 }
 
 template <class T>
@@ -1149,9 +1162,7 @@ float4 node_hi(const xb_bvh_node& n, uint32_t child) {
   return make_float4(n.mx[1], n.mx[2], u32_bits_to_f(child), u32_bits_to_f(n.count));
 }
 
-int alloc_wave(xb_renderer* r, int64_t cap) {
-  free_wave(r);
-  WaveBuffers& w = r->wb;
+bool alloc_wave_buffers(WaveBuffers& w, int64_t cap) {
   w.capacity = cap;
   auto A = [&](auto** p, size_t bytes) -> bool {
     return cudaMalloc((void**)p, bytes) == cudaSuccess;
@@ -1174,7 +1185,13 @@ int alloc_wave(xb_renderer* r, int64_t cap) {
   ok &= A(&w.hit_inst, cap * sizeof(int32_t));
   ok &= A(&w.L, cap * sizeof(float4));
   ok &= A(&w.cnt, (kMaxDepth + 1) * kCntStride * sizeof(int32_t));
-  if (!ok) {
+  return ok;
+}
+
+// Queues for `cap` paths per wave, in both lanes when two waves run at once.
+int alloc_wave(xb_renderer* r, int64_t cap) {
+  free_wave(r);
+  if (!alloc_wave_buffers(r->wb, cap) || (r->tune.waves == 2 && !alloc_wave_buffers(r->wb_b, cap))) {
     free_wave(r);
     return set_err(r, XB_E_OOM, "cannot allocate wave buffers for %lld paths", (long long)cap);
   }
@@ -1201,6 +1218,8 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.wave_paths = pick(t.wave_paths, c.wave_paths, 1 << 21);
   c.shadow_order = pick(t.shadow_order, c.shadow_order, 1);
   c.overlap = pick(t.overlap, c.overlap, 1);
+  c.waves = std::min(2, pick(t.waves, c.waves, 2));
+  c.lane_stagger = std::min(kMaxDepth, pick(t.lane_stagger, c.lane_stagger, 1));
   r->ext_persistent_from = c.extend_persistent_from_depth;
   r->shadow_persistent = c.shadow_persistent == 1;
   r->refill = c.refill;
@@ -1212,7 +1231,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   r->grid_gshade = r->num_sms * std::min(r->occ_gshade, c.shade_blocks_per_sm);
   const int64_t npix = (int64_t)r->cfg.width * r->cfg.height;
   const int spw = (int)std::min<int64_t>(1024, std::max<int64_t>(1, c.wave_paths / npix));
-  if (spw != r->spp_per_wave || r->wb.capacity == 0) {
+  if (spw != r->spp_per_wave || r->wb.capacity == 0 || (c.waves == 2) != (r->wb_b.capacity > 0)) {
     r->spp_per_wave = spw;
     return alloc_wave(r, npix * spw);
   }
@@ -1272,26 +1291,37 @@ void guide_box(xb_renderer* r) {
   }
 }
 
-// The bounce loop of one wave whose camera rays are in queue 0: for every depth, closest hits,
-// shading (plain or guided), then the area-light and sun shadow rays (cpu_tiled.cpp:34-217).
-void launch_extend(xb_renderer* r, int d, bool count) {
-  WaveBuffers& w = r->wb;
+// A wave lane: the queues one wave uses and the streams and events of its bounce loop.
+struct LaneRef {
+  WaveBuffers* w;
+  cudaStream_t s, s2;
+  cudaEvent_t* ev_shade;
+  cudaEvent_t* ev_shadow;
+};
+
+LaneRef lane_ref(xb_renderer* r, int k) {
+  return k == 0 ? LaneRef{&r->wb, r->stream, r->stream2, r->ev_shade, r->ev_shadow}
+                : LaneRef{&r->wb_b, r->stream_b, r->stream_b2, r->ev_shade_b, r->ev_shadow_b};
+}
+
+void launch_extend(xb_renderer* r, const LaneRef& L, int d, bool count) {
+  WaveBuffers& w = *L.w;
   const int q = d & 1;
   int32_t* cd_ = w.cnt + d * kCntStride;
-  StageTimer t(r, STAGE_EXTEND);
+  StageTimer t(r, STAGE_EXTEND, L.s);
   if (r->thread_per_ray || d < r->ext_persistent_from) {
     auto kern = count ? extend_kernel<true> : extend_kernel<false>;
-    kern<<<r->grid_ext, 128, 0, r->stream>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_, r->stats);
+    kern<<<r->grid_ext, 128, 0, L.s>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_, r->stats);
   } else {
     TraceQueue tq{w.ray_o[q], w.ray_d[q], cd_ + CNT_RAYS, cd_ + CNT_FETCH_EXT, w.hit, w.hit_inst,
                   nullptr, nullptr, r->stats, 0};
     auto kern = count ? extend_persistent_kernel<true> : extend_persistent_kernel<false>;
-    kern<<<r->grid_pext, 128, 0, r->stream>>>(r->scene, tq, r->refill);
+    kern<<<r->grid_pext, 128, 0, L.s>>>(r->scene, tq, r->refill);
   }
 }
 
-void launch_shadows(xb_renderer* r, int d, bool count, cudaStream_t s) {
-  WaveBuffers& w = r->wb;
+void launch_shadows(xb_renderer* r, const LaneRef& L, int d, bool count, cudaStream_t s) {
+  WaveBuffers& w = *L.w;
   int32_t* cd_ = w.cnt + d * kCntStride;
   for (int k = 0; k < 2; ++k) {
     if (k == 0 && r->scene.num_lights == 0) continue;
@@ -1319,16 +1349,17 @@ void launch_shadows(xb_renderer* r, int d, bool count, cudaStream_t s) {
 // run on the first: the two only share the scene (shadow rays add to the path radiance, closest
 // hits write the hit records), and shading d+1 waits for both. Each kernel's tail — a few warps
 // finishing long rays after the queue has drained — then runs beside the other kernel's bulk.
-int trace_bounces(xb_renderer* r, bool train, int rec_stride, int depth_limit = -1, const int8_t* path_maxd = nullptr) {
-  WaveBuffers& w = r->wb;
+int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, int depth_limit = -1,
+                  const int8_t* path_maxd = nullptr) {
+  WaveBuffers& w = *L.w;
   const int depth_max = std::min(depth_limit >= 0 ? depth_limit : r->max_bounces, kMaxDepth);
   const bool count = (r->prof_flags & XB_PROFILE_COUNT_TRAVERSAL) != 0;
-  const bool ov = r->tune.overlap == 1 && r->stream2 != nullptr;
+  const bool ov = r->tune.overlap == 1 && L.s2 != nullptr;
   xbg::Guide* gd = r->guiding ? r->guide : nullptr;
   for (int d = 0; d < depth_max; ++d) {
     const int q = d & 1, nq = q ^ 1;
     int32_t* cd_ = w.cnt + d * kCntStride;
-    if (d == 0 || !ov) launch_extend(r, d, count);
+    if (d == 0 || !ov) launch_extend(r, L, d, count);
     ShadeArgs sa;
     sa.sc = r->scene;
     sa.ray_o = w.ray_o[q]; sa.ray_d = w.ray_d[q]; sa.tp = w.tp[q]; sa.rng = w.rng[q]; sa.path = w.path[q];
@@ -1358,22 +1389,22 @@ int trace_bounces(xb_renderer* r, bool train, int rec_stride, int depth_limit = 
       ga.rec_in = (train && d > 0) ? w.rec[q] : nullptr;
       ga.rec_out = train ? w.rec[nq] : nullptr;
       ga.err = xbg::guide_error(gd);
-      StageTimer t(r, STAGE_SHADE);
-      guided_shade_kernel<<<r->grid_gshade, 128, kGuidedShadeSmem, r->stream>>>(sa, ga);
+      StageTimer t(r, STAGE_SHADE, L.s);
+      guided_shade_kernel<<<r->grid_gshade, 128, kGuidedShadeSmem, L.s>>>(sa, ga);
     } else {
-      StageTimer t(r, STAGE_SHADE);
-      shade_kernel<<<r->grid_shade, 128, 0, r->stream>>>(sa);
+      StageTimer t(r, STAGE_SHADE, L.s);
+      shade_kernel<<<r->grid_shade, 128, 0, L.s>>>(sa);
     }
+    CK(cudaEventRecord(L.ev_shade[d], L.s));
     if (!ov) {
-      launch_shadows(r, d, count, r->stream);
+      launch_shadows(r, L, d, count, L.s);
       continue;
     }
-    CK(cudaEventRecord(r->ev_shade[d], r->stream));
-    CK(cudaStreamWaitEvent(r->stream2, r->ev_shade[d], 0));
-    launch_shadows(r, d, count, r->stream2);
-    CK(cudaEventRecord(r->ev_shadow[d], r->stream2));
-    if (d + 1 < depth_max) launch_extend(r, d + 1, count);
-    CK(cudaStreamWaitEvent(r->stream, r->ev_shadow[d], 0));
+    CK(cudaStreamWaitEvent(L.s2, L.ev_shade[d], 0));
+    launch_shadows(r, L, d, count, L.s2);
+    CK(cudaEventRecord(L.ev_shadow[d], L.s2));
+    if (d + 1 < depth_max) launch_extend(r, L, d + 1, count);
+    CK(cudaStreamWaitEvent(L.s, L.ev_shadow[d], 0));
   }
   CK(cudaGetLastError());
   return XB_OK;
@@ -1385,6 +1416,53 @@ CamDev cam_dev(const xb_camera& c) {
                 v3(c.vertical[0], c.vertical[1], c.vertical[2])};
 }
 
+// Two waves in flight: wave i of a call runs on lane i % 2 (lane 0 is the renderer's stream),
+// so one wave's latency-bound stretches and kernel tails run beside the other's bulk. Lane 1
+// first waits for the main stream's work before the call. Every accumulation waits for the
+// previous wave's, so the image's sums keep sample order and equal a single lane's bit for bit.
+// A serial wave (guide training: the network changes after it and the records buffer is
+// shared) waits for the other lane, and the other lane's next wave waits for it. At the end
+// the main stream waits for lane 1.
+struct LaneSched {
+  xb_renderer* r;
+  int lanes;
+  int next = 0;
+  int last_acc = -1;
+  bool has[2] = {false, false}, serial[2] = {false, false};
+
+  LaneSched(xb_renderer* rr) : r(rr), lanes(rr->tune.waves == 2 && rr->wb_b.capacity > 0 ? 2 : 1) {}
+  int begin(bool is_serial) {
+    const int k = next;
+    next = (next + 1) % lanes;
+    const int o = k ^ 1;
+    const LaneRef L = lane_ref(r, k);
+    if (k == 1 && !has[1]) {
+      // lane 1's first wave starts once lane 0's has shaded its first lane_stagger bounces, so
+      // the two waves' widest bounces do not coincide (the main stream's work before the call,
+      // which lane 0 follows, is then done as well)
+      const int d = std::min(r->tune.lane_stagger, std::min(r->max_bounces, kMaxDepth)) - 1;
+      cudaEvent_t e = d >= 0 ? r->ev_shade[d] : r->ev_fork;
+      if (d < 0) cudaEventRecord(r->ev_fork, r->stream);
+      cudaStreamWaitEvent(L.s, e, 0);
+    }
+    if (lanes == 2 && has[o] && (is_serial || serial[o])) cudaStreamWaitEvent(L.s, r->lane_done[o], 0);
+    has[k] = true;
+    serial[k] = is_serial;
+    return k;
+  }
+  void before_accumulate(int k) {
+    if (last_acc >= 0 && last_acc != k) cudaStreamWaitEvent(lane_ref(r, k).s, r->lane_acc[last_acc], 0);
+  }
+  void after_accumulate(int k) {
+    cudaEventRecord(r->lane_acc[k], lane_ref(r, k).s);
+    last_acc = k;
+  }
+  void end_wave(int k) { cudaEventRecord(r->lane_done[k], lane_ref(r, k).s); }
+  ~LaneSched() {   // every return path: the main stream takes in lane 1's work
+    if (has[1]) cudaStreamWaitEvent(r->stream, r->lane_done[1], 0);
+  }
+};
+
 // Renders samples [spp_first, spp_first + spp_count) and returns, in *kept_out, how many of
 // them went into the image.
 int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count, int* kept_out) {
@@ -1393,11 +1471,11 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
   const int W = r->cfg.width, H = r->cfg.height;
   const int64_t npix = (int64_t)W * H;
   const CamDev cd = cam_dev(*cam);
-  WaveBuffers& w = r->wb;
   const int depth_max = std::min(r->max_bounces, kMaxDepth);
   int done = 0;
   xbg::Guide* gd = r->guiding ? r->guide : nullptr;
   if (gd) guide_box(r);
+  LaneSched ls(r);
   while (done < spp_count) {
     const int sample0 = spp_first + done;   // 1-based index of the wave's first sample
     const bool train = gd && sample0 <= r->gcfg.train_spp;
@@ -1406,47 +1484,57 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       // a training wave ends at train_spp and stays within one guide_train call's step budget
       spw = std::min(spw, r->gcfg.train_spp - sample0 + 1);
       spw = std::max(1, std::min(spw, xbg::kMaxTrainSteps / std::max(1, r->gcfg.steps_per_spp)));
+      // and, when the second half is kept, at its first sample
+      const int first_kept = (r->gcfg.train_spp + 1) / 2 + 1;
+      if (r->gcfg.keep_training_samples == 2 && sample0 < first_kept) spw = std::min(spw, first_kept - sample0);
     }
-    const int64_t paths = npix * spw;
-    CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), r->stream));
-    int rec_stride = 1;
-    if (train) {
-      CK(cudaMemsetAsync(xbg::guide_record_count(gd), 0, sizeof(int32_t), r->stream));
-      const int64_t cap = xbg::guide_record_capacity(gd);
-      rec_stride = r->gcfg.record_stride > 0 ? r->gcfg.record_stride
-                                             : (int)std::max<int64_t>(1, (paths * 4 + cap - 1) / cap);
-    }
-    const int g_rg = (int)std::min<int64_t>((paths + 255) / 256, (int64_t)r->num_sms * 16);
+    // samples rendered while the guide trains stay out of the image unless asked for (their
+    // proposal is the still-untrained network); the accumulation still counts the wave's rays
+    const bool keep = !train || r->gcfg.keep_training_samples == 1 ||
+                      (r->gcfg.keep_training_samples == 2 && sample0 >= (r->gcfg.train_spp + 1) / 2 + 1);
     {
-      StageTimer t(r, STAGE_RAYGEN);
-      raygen_kernel<<<g_rg, 256, 0, r->stream>>>(cd, W, H, spp_first + done, paths, w.ray_o[0],
-                                                 w.ray_d[0], w.tp[0], w.rng[0], w.path[0], w.L, w.cnt);
+      const int k = ls.begin(train);
+      const LaneRef L = lane_ref(r, k);
+      WaveBuffers& w = *L.w;
+      const int64_t paths = npix * spw;
+      CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), L.s));
+      int rec_stride = 1;
+      if (train) {
+        CK(cudaMemsetAsync(xbg::guide_record_count(gd), 0, sizeof(int32_t), L.s));
+        const int64_t cap = xbg::guide_record_capacity(gd);
+        rec_stride = r->gcfg.record_stride > 0 ? r->gcfg.record_stride
+                                               : (int)std::max<int64_t>(1, (paths * 4 + cap - 1) / cap);
+      }
+      const int g_rg = (int)std::min<int64_t>((paths + 255) / 256, (int64_t)r->num_sms * 16);
+      {
+        StageTimer t(r, STAGE_RAYGEN, L.s);
+        raygen_kernel<<<g_rg, 256, 0, L.s>>>(cd, W, H, sample0, paths, w.ray_o[0], w.ray_d[0], w.tp[0],
+                                             w.rng[0], w.path[0], w.L, w.cnt);
+      }
+      int rc = trace_bounces(r, L, train, rec_stride);
+      if (rc) return rc;
+      const int g_acc = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)r->num_sms * 16);
+      ls.before_accumulate(k);
+      {
+        StageTimer t(r, STAGE_ACCUM, L.s);
+        accumulate_kernel<<<g_acc, 256, 0, L.s>>>(w.L, npix, keep ? spw : 0, r->spp + kept, r->accum, r->sum64,
+                                                  r->m2_64, r->mean64, w.cnt, depth_max, paths, r->stats);
+      }
+      ls.after_accumulate(k);
+      if (train) {
+        StageTimer t(r, STAGE_TRAIN, L.s);
+        xbg::guide_finalize_records(gd, L.s, w.L, r->num_sms * 8, r->stats + STAT_REC_TOTAL);
+        const int steps = r->gcfg.steps_per_spp * spw;
+        if (xbg::guide_train(gd, L.s, xbg::guide_records(gd), xbg::guide_record_count(gd),
+                             xbg::guide_record_capacity(gd), steps, r->gcfg.batch, r->gcfg.learning_rate,
+                             r->gcfg.seed, r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f,
+                             (int64_t)r->gcfg.train_spp * r->gcfg.steps_per_spp) != XB_OK)
+          return set_err(r, XB_E_CUDA, "guide training launch failed");
+        r->last_loss_index = steps - 1;
+      }
+      ls.end_wave(k);
     }
-    int rc = trace_bounces(r, train, rec_stride);
-    if (rc) return rc;
-    const int g_acc = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)r->num_sms * 16);
-    {
-      StageTimer t(r, STAGE_ACCUM);
-      // samples rendered while the guide trains stay out of the image unless asked for (their
-      // proposal is the still-untrained network); the kernel still counts the wave's rays
-      const bool keep = !train || r->gcfg.keep_training_samples == 1 ||
-                        (r->gcfg.keep_training_samples == 2 && 2 * (sample0 - 1) >= r->gcfg.train_spp);
-      accumulate_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, npix, keep ? spw : 0, r->spp + kept, r->accum,
-                                                      r->sum64, r->m2_64, r->mean64, w.cnt, depth_max, paths,
-                                                      r->stats);
-      if (keep) kept += spw;
-    }
-    if (train) {
-      StageTimer t(r, STAGE_TRAIN);
-      xbg::guide_finalize_records(gd, r->stream, w.L, r->num_sms * 8, r->stats + STAT_REC_TOTAL);
-      const int steps = r->gcfg.steps_per_spp * spw;
-      if (xbg::guide_train(gd, r->stream, xbg::guide_records(gd), xbg::guide_record_count(gd),
-                           xbg::guide_record_capacity(gd), steps, r->gcfg.batch, r->gcfg.learning_rate,
-                           r->gcfg.seed, r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f,
-                           (int64_t)r->gcfg.train_spp * r->gcfg.steps_per_spp) != XB_OK)
-        return set_err(r, XB_E_CUDA, "guide training launch failed");
-      r->last_loss_index = steps - 1;
-    }
+    if (keep) kept += spw;
     CK(cudaGetLastError());
     done += spw;
   }
@@ -1459,13 +1547,13 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
 // piece are laid out sample-major like a single-view wave, so each path is seeded exactly as a
 // render of that view alone would seed it and the accumulation runs in sample order.
 int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accum, const int64_t* accum_off) {
-  WaveBuffers& w = r->wb;
   const int depth_max = std::min(r->max_bounces, kMaxDepth);
   xbg::Guide* gd = r->guiding ? r->guide : nullptr;
   if (gd) guide_box(r);
   std::vector<int> left(count);
   for (int v = 0; v < count; ++v) left[v] = views[v].spp;
   int v0 = 0;
+  LaneSched ls(r);
   while (v0 < count) {
     ViewPieces pk{};
     int64_t paths = 0;
@@ -1473,7 +1561,7 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
     for (int v = v0; v < count && pk.n < kMaxPieces; ++v) {
       if (left[v] == 0) { if (v == v0) ++v0; continue; }
       const int64_t npix = (int64_t)views[v].width * views[v].height;
-      const int64_t room = (w.capacity - paths) / npix;
+      const int64_t room = (r->wb.capacity - paths) / npix;   // both lanes hold this many paths
       if (room <= 0) break;
       const int n = (int)std::min<int64_t>(left[v], room);
       ViewPiece& p = pk.p[pk.n++];
@@ -1493,23 +1581,29 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
     }
     while (v0 < count && left[v0] == 0) ++v0;
     if (pk.n == 0) break;
-    CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), r->stream));
+    const int k = ls.begin(false);
+    const LaneRef L = lane_ref(r, k);
+    WaveBuffers& w = *L.w;
+    CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), L.s));
     const int g_rg = (int)std::min<int64_t>((paths + 255) / 256, (int64_t)r->num_sms * 16);
     {
-      StageTimer t(r, STAGE_RAYGEN);
-      raygen_views_kernel<<<g_rg, 256, 0, r->stream>>>(pk, paths, w.ray_o[0], w.ray_d[0], w.tp[0], w.rng[0],
+      StageTimer t(r, STAGE_RAYGEN, L.s);
+      raygen_views_kernel<<<g_rg, 256, 0, L.s>>>(pk, paths, w.ray_o[0], w.ray_d[0], w.tp[0], w.rng[0],
                                                        w.path[0], w.L, w.maxd, w.cnt);
     }
     int wave_depth = 0;
     for (int i = 0; i < pk.n; ++i) wave_depth = std::max(wave_depth, pk.p[i].max_bounces);
-    int rc = trace_bounces(r, false, 1, wave_depth, w.maxd);
+    int rc = trace_bounces(r, L, false, 1, wave_depth, w.maxd);
     if (rc) return rc;
     const int g_acc = (int)std::min<int64_t>((pix_total + 255) / 256, (int64_t)r->num_sms * 16);
     {
-      StageTimer t(r, STAGE_ACCUM);
-      accumulate_views_kernel<<<g_acc, 256, 0, r->stream>>>(w.L, pk, pix_total, accum, w.cnt, wave_depth, paths,
-                                                            r->stats);
+      ls.before_accumulate(k);
+      StageTimer t(r, STAGE_ACCUM, L.s);
+      accumulate_views_kernel<<<g_acc, 256, 0, L.s>>>(w.L, pk, pix_total, accum, w.cnt, wave_depth, paths,
+                                                      r->stats);
     }
+    ls.after_accumulate(k);
+    ls.end_wave(k);
     CK(cudaGetLastError());
   }
   return XB_OK;
@@ -1548,7 +1642,17 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
       return bail(xb::fail(XB_E_CUDA, "event creation failed"));
   for (int d = 0; d < kMaxDepth; ++d)
     if (cudaEventCreateWithFlags(&r->ev_shade[d], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&r->ev_shadow[d], cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&r->ev_shadow[d], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev_shade_b[d], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev_shadow_b[d], cudaEventDisableTiming) != cudaSuccess)
+      return bail(xb::fail(XB_E_CUDA, "event creation failed"));
+  if (cudaStreamCreateWithFlags(&r->stream_b, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&r->stream_b2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&r->ev_fork, cudaEventDisableTiming) != cudaSuccess)
+    return bail(xb::fail(XB_E_CUDA, "stream creation failed"));
+  for (int k = 0; k < 2; ++k)
+    if (cudaEventCreateWithFlags(&r->lane_done[k], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->lane_acc[k], cudaEventDisableTiming) != cudaSuccess)
       return bail(xb::fail(XB_E_CUDA, "event creation failed"));
   if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess)
@@ -1620,6 +1724,7 @@ void xb_destroy(xb_renderer* r) {
   if (!r) return;
   cudaSetDevice(r->cfg.device);
   if (r->stream) cudaStreamSynchronize(r->stream);
+  for (cudaStream_t s : {r->stream_b, r->stream_b2}) if (s) cudaStreamSynchronize(s);
   free_scene(r);
   free_wave(r);
   xbg::guide_destroy(r->guide);
@@ -1637,10 +1742,12 @@ void xb_destroy(xb_renderer* r) {
   if (r->ev0) cudaEventDestroy(r->ev0);
   if (r->ev1) cudaEventDestroy(r->ev1);
   if (r->stream2) cudaStreamSynchronize(r->stream2);
-  for (int d = 0; d < kMaxDepth; ++d) {
-    if (r->ev_shade[d]) cudaEventDestroy(r->ev_shade[d]);
-    if (r->ev_shadow[d]) cudaEventDestroy(r->ev_shadow[d]);
-  }
+  for (int d = 0; d < kMaxDepth; ++d)
+    for (cudaEvent_t e : {r->ev_shade[d], r->ev_shadow[d], r->ev_shade_b[d], r->ev_shadow_b[d]})
+      if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : {r->lane_done[0], r->lane_done[1], r->lane_acc[0], r->lane_acc[1], r->ev_fork})
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t s : {r->stream_b, r->stream_b2}) if (s) cudaStreamDestroy(s);
   if (r->stream2) cudaStreamDestroy(r->stream2);
   if (r->stream) cudaStreamDestroy(r->stream);
   delete r;
