@@ -281,9 +281,14 @@ def guiding_study(args, device: int) -> dict:
     cam = xb.camera(desc.eye, desc.target, desc.fov, W / H)
     eps = 1e-2
 
+    from xenon_b200 import autotune
+    tuned = autotune.load_tuning("config4") if (W, H) == (1280, 720) else None
+
     def renderer(fp64=False):
         r = xb.Renderer(W, H, desc.max_bounces, desc.min_bounces, device=device, fp64=fp64)
         r.upload_scene(hs)
+        if tuned:
+            r.set_tuning(**tuned)
         return r
 
     t0 = time.perf_counter()
@@ -337,6 +342,7 @@ def guiding_study(args, device: int) -> dict:
     guided = equal_time(True)
     return {"workload": "config4: closed room, light above a baffle, smooth glass icosphere L7 "
                         f"(327,680 tris), {W}x{H}, depth 16",
+            "tuning": tuned or "defaults",
             "budget_device_s": args.guide_seconds, "reference": {"spp": done, "device_ms": ref_ms,
                                                                "image_mean": float(ref.mean()),
                                                                "expected_relmse": ref_err},
@@ -364,9 +370,14 @@ def views_study(args, device: int) -> dict:
     paths = sum(w * h * spp for (_, w, h, spp, _) in views)
     maxb = max(mb for (*_, mb) in views)
 
+    from xenon_b200 import autotune
+    tuned = autotune.load_tuning("config3")
+
     def renderer(w=512, h=512):
         r = xb.Renderer(w, h, maxb, desc.min_bounces, device=device)
         r.upload_scene(hs)
+        if tuned:
+            r.set_tuning(**tuned)
         return r
 
     # plain: batched vs one by one, and the 4x reference
@@ -420,6 +431,7 @@ def views_study(args, device: int) -> dict:
     speed = plain_ms / guided_ms   # relMSE falls as 1/samples: equal time scales the ratio by it
     return {"workload": "config5: 32 views of config 3 (16x16 instances), side 256-1024 px log-uniform, "
                         f"spp from {{16,64,256,1024}} capped at {args.views_max_spp}, depth 6-16",
+            "tuning": tuned or "defaults",
             "paths": paths, "guided_msamples_per_s": paths / guided_ms / 1e3, "guided_ms": guided_ms,
             "guide_training_ms": train_ms, "plain_batched_msamples_per_s": paths / plain_ms / 1e3,
             "plain_one_by_one_msamples_per_s": paths / seq_ms / 1e3,

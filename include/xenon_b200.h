@@ -325,9 +325,9 @@ typedef struct xb_tuning {
                                            warps, earlier bounces one ray per thread (64: never) */
   int32_t shadow_persistent;            /* 1: persistent warps for shadow rays, 2: one per thread */
   int32_t refill;                       /* persistent warps refill when this many lanes idle */
-  int32_t extend_blocks_per_sm;         /* resident blocks of 128 threads per SM for the trace */
-  int32_t shadow_blocks_per_sm;         /* kernels; bounded by the kernel's occupancy limit */
-  int32_t shade_blocks_per_sm;
+  int32_t extend_blocks_per_sm;         /* blocks of 128 threads per SM in the grid of the trace */
+  int32_t shadow_blocks_per_sm;         /* and shade kernels (1-64); for the persistent ones */
+  int32_t shade_blocks_per_sm;          /* bounded by the blocks that fit on an SM at once */
   int32_t wave_paths;                   /* paths in flight per wave (reallocates queues) */
   int32_t shadow_order;                 /* shadow rays: 1 nearer child first, 2 farther first
                                            (the occlusion answer does not depend on it) */

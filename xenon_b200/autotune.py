@@ -11,7 +11,8 @@ two passes), and keeps the fastest setting:
   waves                          waves in flight (two stream lanes or one)
   lane_stagger                   bounces the first lane shades before the second lane starts
   refill                         idle lanes that trigger a warp refill
-  extend/shadow/shade_blocks_per_sm   resident blocks per SM (grid size)
+  extend/shadow/shade_blocks_per_sm   blocks per SM in the grids (persistent kernels: at most
+                                      those resident at once)
   wave_paths                     paths in flight per wave (queue capacity)
 
 Results are stored as JSON under xenon_b200/tuning/<gpu>/<workload>.json and loaded by
@@ -34,9 +35,9 @@ SPACE = {
     "waves": [1, 2],
     "lane_stagger": [1, 2, 3],
     "refill": [2, 4, 8, 16, 24],
-    "extend_blocks_per_sm": [3, 4, 5, 6, 64],
-    "shadow_blocks_per_sm": [3, 4, 5, 6, 64],
-    "shade_blocks_per_sm": [2, 3, 4, 64],
+    "extend_blocks_per_sm": [2, 4, 8, 16, 64],
+    "shadow_blocks_per_sm": [2, 4, 8, 16, 64],
+    "shade_blocks_per_sm": [2, 4, 8, 16, 64],
     "wave_paths": [1 << 20, 1 << 21, 1 << 22],
 }
 
@@ -124,7 +125,7 @@ if __name__ == "__main__":
     elif a.workload == "config1":
         desc = scenes.cornell()
     elif a.workload == "config4":
-        desc = scenes.guiding_room(level=8)
+        desc = scenes.guiding_room(level=7)
     else:
         desc = scenes.instanced_grid()
     hs = xb.HostScene.from_desc(desc)

@@ -1212,9 +1212,9 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.extend_persistent_from_depth = pick(t.extend_persistent_from_depth, c.extend_persistent_from_depth, 1);
   c.shadow_persistent = pick(t.shadow_persistent, c.shadow_persistent, 1);
   c.refill = std::min(32, pick(t.refill, c.refill, 8));
-  c.extend_blocks_per_sm = pick(t.extend_blocks_per_sm, c.extend_blocks_per_sm, 64);
-  c.shadow_blocks_per_sm = pick(t.shadow_blocks_per_sm, c.shadow_blocks_per_sm, 64);
-  c.shade_blocks_per_sm = pick(t.shade_blocks_per_sm, c.shade_blocks_per_sm, 64);
+  c.extend_blocks_per_sm = std::min(64, pick(t.extend_blocks_per_sm, c.extend_blocks_per_sm, 64));
+  c.shadow_blocks_per_sm = std::min(64, pick(t.shadow_blocks_per_sm, c.shadow_blocks_per_sm, 64));
+  c.shade_blocks_per_sm = std::min(64, pick(t.shade_blocks_per_sm, c.shade_blocks_per_sm, 64));
   c.wave_paths = pick(t.wave_paths, c.wave_paths, 1 << 21);
   c.shadow_order = pick(t.shadow_order, c.shadow_order, 1);
   c.overlap = pick(t.overlap, c.overlap, 1);
@@ -1223,11 +1223,15 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   r->ext_persistent_from = c.extend_persistent_from_depth;
   r->shadow_persistent = c.shadow_persistent == 1;
   r->refill = c.refill;
-  r->grid_ext = r->num_sms * std::min(r->occ_ext, c.extend_blocks_per_sm);
+  // Persistent kernels (their blocks loop until the queue is empty) launch at most the blocks
+  // that fit at once; the others fetch warps of work from a counter or take tiles in a
+  // grid-stride loop, so blocks beyond the resident ones queue and, as they start while others
+  // retire, interleave with the other wave lane's kernels.
+  r->grid_ext = r->num_sms * c.extend_blocks_per_sm;
   r->grid_pext = r->num_sms * std::min(r->occ_pext, c.extend_blocks_per_sm);
-  r->grid_shadow = r->num_sms * std::min(r->occ_shadow, c.shadow_blocks_per_sm);
+  r->grid_shadow = r->num_sms * c.shadow_blocks_per_sm;
   r->grid_pshadow = r->num_sms * std::min(r->occ_pshadow, c.shadow_blocks_per_sm);
-  r->grid_shade = r->num_sms * std::min(r->occ_shade, c.shade_blocks_per_sm);
+  r->grid_shade = r->num_sms * c.shade_blocks_per_sm;
   r->grid_gshade = r->num_sms * std::min(r->occ_gshade, c.shade_blocks_per_sm);
   const int64_t npix = (int64_t)r->cfg.width * r->cfg.height;
   const int spw = (int)std::min<int64_t>(1024, std::max<int64_t>(1, c.wave_paths / npix));
@@ -1497,7 +1501,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       const LaneRef L = lane_ref(r, k);
       WaveBuffers& w = *L.w;
       const int64_t paths = npix * spw;
-      CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), L.s));
+      CK(cudaMemsetAsync(w.cnt, 0, (depth_max + 1) * kCntStride * sizeof(int32_t), L.s));
       int rec_stride = 1;
       if (train) {
         CK(cudaMemsetAsync(xbg::guide_record_count(gd), 0, sizeof(int32_t), L.s));
@@ -1547,7 +1551,6 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
 // piece are laid out sample-major like a single-view wave, so each path is seeded exactly as a
 // render of that view alone would seed it and the accumulation runs in sample order.
 int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accum, const int64_t* accum_off) {
-  const int depth_max = std::min(r->max_bounces, kMaxDepth);
   xbg::Guide* gd = r->guiding ? r->guide : nullptr;
   if (gd) guide_box(r);
   std::vector<int> left(count);
@@ -1584,15 +1587,16 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
     const int k = ls.begin(false);
     const LaneRef L = lane_ref(r, k);
     WaveBuffers& w = *L.w;
-    CK(cudaMemsetAsync(w.cnt, 0, (kMaxDepth + 1) * kCntStride * sizeof(int32_t), L.s));
+    int wave_depth = 0;
+    for (int i = 0; i < pk.n; ++i) wave_depth = std::max(wave_depth, pk.p[i].max_bounces);
+    // the counters of every depth the wave's bounce loop reads start at zero
+    CK(cudaMemsetAsync(w.cnt, 0, (wave_depth + 1) * kCntStride * sizeof(int32_t), L.s));
     const int g_rg = (int)std::min<int64_t>((paths + 255) / 256, (int64_t)r->num_sms * 16);
     {
       StageTimer t(r, STAGE_RAYGEN, L.s);
       raygen_views_kernel<<<g_rg, 256, 0, L.s>>>(pk, paths, w.ray_o[0], w.ray_d[0], w.tp[0], w.rng[0],
-                                                       w.path[0], w.L, w.maxd, w.cnt);
+                                                 w.path[0], w.L, w.maxd, w.cnt);
     }
-    int wave_depth = 0;
-    for (int i = 0; i < pk.n; ++i) wave_depth = std::max(wave_depth, pk.p[i].max_bounces);
     int rc = trace_bounces(r, L, false, 1, wave_depth, w.maxd);
     if (rc) return rc;
     const int g_acc = (int)std::min<int64_t>((pix_total + 255) / 256, (int64_t)r->num_sms * 16);
