@@ -282,13 +282,17 @@ def guiding_study(args, device: int) -> dict:
     eps = 1e-2
 
     from xenon_b200 import autotune
-    tuned = autotune.load_tuning("config4") if (W, H) == (1280, 720) else None
+    # each method with the launch settings the autotuner picked for it on this workload
+    full = (W, H) == (1280, 720)
+    tuned = autotune.load_tuning("config4") if full else None
+    tuned_g = (autotune.load_tuning("config4g") or tuned) if full else None
 
-    def renderer(fp64=False):
+    def renderer(fp64=False, guided=False):
         r = xb.Renderer(W, H, desc.max_bounces, desc.min_bounces, device=device, fp64=fp64)
         r.upload_scene(hs)
-        if tuned:
-            r.set_tuning(**tuned)
+        t = tuned_g if guided else tuned
+        if t:
+            r.set_tuning(**t)
         return r
 
     t0 = time.perf_counter()
@@ -309,7 +313,7 @@ def guiding_study(args, device: int) -> dict:
     ref_err = float(np.mean(ref_var / done / denom))   # the reference's own expected relMSE
 
     def equal_time(guided: bool) -> dict:
-        r = renderer()
+        r = renderer(guided=guided)
         info = {}
         if guided:
             fixed = args.guide_fraction > 0
@@ -342,7 +346,7 @@ def guiding_study(args, device: int) -> dict:
     guided = equal_time(True)
     return {"workload": "config4: closed room, light above a baffle, smooth glass icosphere L7 "
                         f"(327,680 tris), {W}x{H}, depth 16",
-            "tuning": tuned or "defaults",
+            "tuning": {"plain": tuned or "defaults", "guided": tuned_g or "defaults"},
             "budget_device_s": args.guide_seconds, "reference": {"spp": done, "device_ms": ref_ms,
                                                                "image_mean": float(ref.mean()),
                                                                "expected_relmse": ref_err},

@@ -124,7 +124,7 @@ if __name__ == "__main__":
         desc = scenes.icosphere_scene(level=8)
     elif a.workload == "config1":
         desc = scenes.cornell()
-    elif a.workload == "config4":
+    elif a.workload in ("config4", "config4g"):
         desc = scenes.guiding_room(level=7)
     else:
         desc = scenes.instanced_grid()
@@ -134,6 +134,11 @@ if __name__ == "__main__":
     cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
     if a.from_saved and load_tuning(a.workload):
         r.set_tuning(**load_tuning(a.workload))
+    if a.workload == "config4g":
+        # guided rendering with a network trained on the first 64 samples, then held fixed
+        r.set_guiding(True, train_spp=64, steps_per_spp=32, keep_training_samples=2)
+        r.render_frame(cam, 64)
+        r.set_guiding(True, train_spp=-1)
     res = autotune(r, cam, a.workload, calls=a.calls, spp_per_call=a.spp_per_call)
     print(json.dumps(res))
     if a.out:
