@@ -372,8 +372,8 @@ int  xb_trace_rays_device(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit 
 
 /* Same as xb_trace_rays_device, but the call allocates nothing (no cudaMalloc, cudaFree or
  * allocating library routine): for callers that cannot allocate device memory while they trace,
- * e.g. code running while a stream is captured into a CUDA graph, or a plugin whose host
- * application owns all device memory. Its scratch (ray cursor, count, overflow counter) is a
+ * e.g. a plugin whose host application owns all device memory (its own allocator, or a fixed
+ * budget set at start-up). Its scratch (ray cursor, count, overflow counter) is a
  * fixed 256-byte device array inside the library, shared by every call: calls that overlap on
  * the GPU race on it, so issue them on one stream or otherwise one at a time. The first call on a
  * device looks up that array's address (cudaGetSymbolAddress, once per device, with the device

@@ -1,5 +1,5 @@
-"""xb_trace_rays_noalloc: tracing for callers that cannot allocate device memory (code running
-while a stream is captured into a CUDA graph, or a plugin whose host owns all device memory).
+"""xb_trace_rays_noalloc: tracing for callers that cannot allocate device memory (a plugin
+whose host application owns all device memory through its own allocator or a fixed budget).
 
 The entry point must give exactly the hit records of xb_trace_rays_device, on two calls in a
 row (its scratch is a fixed array shared by all calls, cleared at the start of each), and

@@ -1044,8 +1044,8 @@ __global__ void bsdf_sample_kernel(DevMaterial m, int64_t n, const float* wo, ui
 }
 
 // ── trace without allocation (xb_trace_rays_noalloc) ─────────────────────────────
-// Some callers cannot call cudaMalloc while they trace: code that runs while a stream is being
-// captured into a CUDA graph, or a plugin whose host application owns every device allocation.
+// Some callers cannot call cudaMalloc while they trace: a plugin whose host application owns
+// every device allocation (its own allocator, or a fixed memory budget set at start-up).
 // For them the work-stealing trace keeps its scratch (the ray cursor, the ray count and an
 // overflow counter) in this fixed file-scope array instead of renderer-allocated memory. It is
 // 256 bytes; every GPU that loads the library holds one copy until the process exits.
