@@ -28,7 +28,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TUNING_DIR = os.path.join(HERE, "tuning")
 
 SPACE = {
-    "extend_persistent_from_depth": [0, 1, 2, 3, 64],
+    # no 0: a zero field keeps the current value (the xb_tuning convention)
+    "extend_persistent_from_depth": [1, 2, 3, 64],
     "shadow_persistent": [1, 2],
     "shadow_order": [1, 2],
     "overlap": [1, 2],
