@@ -339,6 +339,10 @@ typedef struct xb_tuning {
                                            memory); 1 one at a time. Same image either way. */
   int32_t lane_stagger;                 /* with two lanes, a call's second wave starts once the
                                            first has shaded this many bounces (1-16) */
+  int32_t graph;                        /* 1 (default): the bounce loop of a full, non-training
+                                           wave of xb_render replays a CUDA graph captured from
+                                           its launches on first use; 2: direct launches. Not
+                                           used while profiling. Same image either way. */
 } xb_tuning;
 int  xb_set_tuning(xb_renderer *r, const xb_tuning *t);
 int  xb_get_tuning(const xb_renderer *r, xb_tuning *out);

@@ -131,6 +131,53 @@ def test_two_waves_in_flight_render_identically():
 
 
 @pytest.mark.gpu
+def test_captured_bounce_loops_render_identically():
+    """Replayed CUDA graphs of the bounce loop give the direct launches' images, and a change of
+    bounces, guiding or scene drops the captured graphs (the next render matches a fresh one)."""
+    desc = scenes.instanced_grid(grid=3, levels=(3, 3, 3, 3), with_prims=True)
+    hs = HostScene.from_desc(desc)
+    other = HostScene.from_desc(scenes.cornell())
+    W, H = 64, 48
+    cam = camera(desc.eye, desc.target, desc.fov, W / H)
+
+    def fresh(graph, bounces=None, guided=False, scene=hs, spp=4):
+        r = Renderer(W, H, desc.max_bounces, desc.min_bounces, wave_paths=W * H)
+        r.upload_scene(scene)
+        r.set_tuning(graph=graph)
+        if bounces:
+            r.set_bounces(desc.min_bounces, bounces)
+        if guided:
+            r.set_guiding(True, train_spp=-1)
+        r.render_frame(cam, spp)
+        img = r.resolve().copy()
+        r.close()
+        return img
+
+    for kw in ({}, {"guided": True}):
+        assert np.array_equal(fresh(1, **kw), fresh(2, **kw))
+    r = Renderer(W, H, desc.max_bounces, desc.min_bounces, wave_paths=W * H)
+    r.upload_scene(hs)
+    r.set_tuning(graph=1)
+    r.render_frame(cam, 4)                      # captures the graphs
+    assert np.array_equal(r.resolve(), fresh(2))
+    r.reset()
+    r.set_bounces(desc.min_bounces, 3)
+    r.render_frame(cam, 4)
+    assert np.array_equal(r.resolve(), fresh(2, bounces=3))
+    r.reset()
+    r.set_guiding(True, train_spp=-1)
+    r.render_frame(cam, 4)
+    assert np.array_equal(r.resolve(), fresh(2, bounces=3, guided=True))
+    r.set_guiding(False)
+    r.set_bounces(desc.min_bounces, desc.max_bounces)
+    r.upload_scene(other)
+    r.reset()
+    r.render_frame(cam, 4)
+    assert np.array_equal(r.resolve(), fresh(2, scene=other))
+    r.close()
+
+
+@pytest.mark.gpu
 def test_converged_cornell_matches_cpu_render(ref):
     desc = scenes.cornell(max_bounces=8)
     w = h = 64

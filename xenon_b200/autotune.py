@@ -10,6 +10,7 @@ two passes), and keeps the fastest setting:
   overlap                        shadow rays of a bounce concurrent with the next bounce's closest hits
   waves                          waves in flight (two stream lanes or one)
   lane_stagger                   bounces the first lane shades before the second lane starts
+  graph                          captured CUDA graph of a wave's bounce loop, or direct launches
   refill                         idle lanes that trigger a warp refill
   extend/shadow/shade_blocks_per_sm   blocks per SM in the grids (persistent kernels: at most
                                       those resident at once)
@@ -35,6 +36,7 @@ SPACE = {
     "overlap": [1, 2],
     "waves": [1, 2],
     "lane_stagger": [1, 2, 3],
+    "graph": [1, 2],
     "refill": [2, 4, 8, 16, 24],
     "extend_blocks_per_sm": [2, 4, 8, 16, 64],
     "shadow_blocks_per_sm": [2, 4, 8, 16, 64],

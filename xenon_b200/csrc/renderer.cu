@@ -116,7 +116,10 @@ struct xb_renderer {
   cudaEvent_t ev_shadow_b[kMaxDepth] = {};
   cudaEvent_t lane_done[2] = {nullptr, nullptr};   // each lane's last wave finished
   cudaEvent_t lane_acc[2] = {nullptr, nullptr};    // each lane's last accumulation finished
-  cudaEvent_t ev_fork = nullptr;                   // the main stream's work before a call's waves
+  cudaEvent_t ev_stagger = nullptr;                // lane 0's wave has shaded lane_stagger bounces
+  // captured bounce loops of full waves: [lane][plain, guided][bounces before, from the stagger]
+  cudaGraphExec_t bounce_graph[2][2][2] = {};
+  bool graph_broken = false;                       // a capture failed: direct launches from then on
   int num_sms = 0;
   std::string err;
   // scene
@@ -1121,7 +1124,25 @@ DevMaterial to_dev_material(const xb_material& m) {
   return o;
 }
 
+// Drops the captured bounce loops (after their launches have finished).
+void drop_graphs(xb_renderer* r) {
+  bool any = false;
+  for (auto& a : r->bounce_graph)
+    for (auto& b : a)
+      for (cudaGraphExec_t g : b) any = any || g != nullptr;
+  if (!any) return;
+  for (cudaStream_t s : {r->stream, r->stream2, r->stream_b, r->stream_b2}) if (s) cudaStreamSynchronize(s);
+  for (auto& a : r->bounce_graph)
+    for (auto& b : a)
+      for (cudaGraphExec_t& g : b)
+        if (g) {
+          cudaGraphExecDestroy(g);
+          g = nullptr;
+        }
+}
+
 void free_scene(xb_renderer* r) {
+  drop_graphs(r);
   for (void* p : r->scene_mem) cudaFree(p);
   r->scene_mem.clear();
   r->has_scene = false;
@@ -1138,6 +1159,7 @@ void free_wave_buffers(WaveBuffers& w) {
 }
 
 void free_wave(xb_renderer* r) {
+  drop_graphs(r);
   for (cudaStream_t s : {r->stream, r->stream2, r->stream_b, r->stream_b2}) if (s) cudaStreamSynchronize(s);
   free_wave_buffers(r->wb);
   free_wave_buffers(r->wb_b);
@@ -1220,6 +1242,8 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.overlap = pick(t.overlap, c.overlap, 1);
   c.waves = std::min(2, pick(t.waves, c.waves, 2));
   c.lane_stagger = std::min(kMaxDepth, pick(t.lane_stagger, c.lane_stagger, 1));
+  c.graph = std::min(2, pick(t.graph, c.graph, 1));
+  drop_graphs(r);
   r->ext_persistent_from = c.extend_persistent_from_depth;
   r->shadow_persistent = c.shadow_persistent == 1;
   r->refill = c.refill;
@@ -1353,14 +1377,17 @@ void launch_shadows(xb_renderer* r, const LaneRef& L, int d, bool count, cudaStr
 // run on the first: the two only share the scene (shadow rays add to the path radiance, closest
 // hits write the hit records), and shading d+1 waits for both. Each kernel's tail — a few warps
 // finishing long rays after the queue has drained — then runs beside the other kernel's bulk.
+// Bounces [d0, d1) of the loop (d1 < 0: to the last); a later range continues where an earlier
+// one stopped (its closest hits of bounce d0 are already traced when overlap is on).
 int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, int depth_limit = -1,
-                  const int8_t* path_maxd = nullptr) {
+                  const int8_t* path_maxd = nullptr, int d0 = 0, int d1 = -1) {
   WaveBuffers& w = *L.w;
   const int depth_max = std::min(depth_limit >= 0 ? depth_limit : r->max_bounces, kMaxDepth);
   const bool count = (r->prof_flags & XB_PROFILE_COUNT_TRAVERSAL) != 0;
   const bool ov = r->tune.overlap == 1 && L.s2 != nullptr;
   xbg::Guide* gd = r->guiding ? r->guide : nullptr;
-  for (int d = 0; d < depth_max; ++d) {
+  const int d_end = d1 < 0 ? depth_max : std::min(d1, depth_max);
+  for (int d = d0; d < d_end; ++d) {
     const int q = d & 1, nq = q ^ 1;
     int32_t* cd_ = w.cnt + d * kCntStride;
     if (d == 0 || !ov) launch_extend(r, L, d, count);
@@ -1414,6 +1441,50 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
   return XB_OK;
 }
 
+// Bounces [d0, d1) of lane k's wave. With `graph` tuning 1, a full non-training wave of a
+// single-view render replays a CUDA graph captured from the same launches the first time (one
+// per lane, plain or guided, and range); the graphs hold the scene, queue and network pointers
+// and launch settings by value, so every change of those drops them (drop_graphs). Replaying
+// gives the same kernels in the same order, hence the same image.
+int bounce_range(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_stride, int d0, int d1) {
+  if (d0 >= d1) return XB_OK;
+  const bool guided = r->guiding && r->guide;
+  if (r->tune.graph != 1 || train || r->prof_flags != 0 || r->graph_broken)
+    return trace_bounces(r, L, train, rec_stride, -1, nullptr, d0, d1);
+  cudaGraphExec_t& ge = r->bounce_graph[k][guided ? 1 : 0][d0 == 0 ? 0 : 1];
+  if (!ge) {
+    cudaGraph_t g = nullptr;
+    int rc = XB_OK;
+    cudaError_t e = cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      rc = trace_bounces(r, L, false, 1, -1, nullptr, d0, d1);
+      e = cudaStreamEndCapture(L.s, &g);
+    }
+    if (e == cudaSuccess && rc == XB_OK && g) e = cudaGraphInstantiate(&ge, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess || rc != XB_OK || !ge) {
+      // the launches themselves work without capture: take them directly from now on
+      cudaGetLastError();
+      ge = nullptr;
+      r->graph_broken = true;
+      return trace_bounces(r, L, train, rec_stride, -1, nullptr, d0, d1);
+    }
+  }
+  CK(cudaGraphLaunch(ge, L.s));
+  return XB_OK;
+}
+
+// A wave's whole bounce loop: the bounces before the stagger point, lane 0's stagger event,
+// the rest.
+int run_bounces(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_stride) {
+  const int depth_max = std::min(r->max_bounces, kMaxDepth);
+  const int sp = std::min(r->tune.lane_stagger, depth_max);
+  int rc = bounce_range(r, L, k, train, rec_stride, 0, sp);
+  if (rc) return rc;
+  if (k == 0) CK(cudaEventRecord(r->ev_stagger, L.s));
+  return bounce_range(r, L, k, train, rec_stride, sp, depth_max);
+}
+
 CamDev cam_dev(const xb_camera& c) {
   return CamDev{v3(c.eye[0], c.eye[1], c.eye[2]), v3(c.lower_left[0], c.lower_left[1], c.lower_left[2]),
                 v3(c.horizontal[0], c.horizontal[1], c.horizontal[2]),
@@ -1441,13 +1512,10 @@ struct LaneSched {
     const int o = k ^ 1;
     const LaneRef L = lane_ref(r, k);
     if (k == 1 && !has[1]) {
-      // lane 1's first wave starts once lane 0's has shaded its first lane_stagger bounces, so
-      // the two waves' widest bounces do not coincide (the main stream's work before the call,
-      // which lane 0 follows, is then done as well)
-      const int d = std::min(r->tune.lane_stagger, std::min(r->max_bounces, kMaxDepth)) - 1;
-      cudaEvent_t e = d >= 0 ? r->ev_shade[d] : r->ev_fork;
-      if (d < 0) cudaEventRecord(r->ev_fork, r->stream);
-      cudaStreamWaitEvent(L.s, e, 0);
+      // lane 1's first wave starts once lane 0's has shaded its first lane_stagger bounces
+      // (ev_stagger), so the two waves' widest bounces do not coincide; the main stream's work
+      // before the call, which lane 0 follows, is then done as well
+      cudaStreamWaitEvent(L.s, r->ev_stagger, 0);
     }
     if (lanes == 2 && has[o] && (is_serial || serial[o])) cudaStreamWaitEvent(L.s, r->lane_done[o], 0);
     has[k] = true;
@@ -1515,7 +1583,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
         raygen_kernel<<<g_rg, 256, 0, L.s>>>(cd, W, H, sample0, paths, w.ray_o[0], w.ray_d[0], w.tp[0],
                                              w.rng[0], w.path[0], w.L, w.cnt);
       }
-      int rc = trace_bounces(r, L, train, rec_stride);
+      int rc = run_bounces(r, L, k, train, rec_stride);
       if (rc) return rc;
       const int g_acc = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)r->num_sms * 16);
       ls.before_accumulate(k);
@@ -1597,7 +1665,11 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
       raygen_views_kernel<<<g_rg, 256, 0, L.s>>>(pk, paths, w.ray_o[0], w.ray_d[0], w.tp[0], w.rng[0],
                                                  w.path[0], w.L, w.maxd, w.cnt);
     }
-    int rc = trace_bounces(r, L, false, 1, wave_depth, w.maxd);
+    const int sp = std::min(r->tune.lane_stagger, wave_depth);
+    int rc = trace_bounces(r, L, false, 1, wave_depth, w.maxd, 0, sp);
+    if (rc) return rc;
+    if (k == 0) CK(cudaEventRecord(r->ev_stagger, L.s));
+    rc = trace_bounces(r, L, false, 1, wave_depth, w.maxd, sp, wave_depth);
     if (rc) return rc;
     const int g_acc = (int)std::min<int64_t>((pix_total + 255) / 256, (int64_t)r->num_sms * 16);
     {
@@ -1652,7 +1724,7 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
       return bail(xb::fail(XB_E_CUDA, "event creation failed"));
   if (cudaStreamCreateWithFlags(&r->stream_b, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&r->stream_b2, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&r->ev_fork, cudaEventDisableTiming) != cudaSuccess)
+      cudaEventCreateWithFlags(&r->ev_stagger, cudaEventDisableTiming) != cudaSuccess)
     return bail(xb::fail(XB_E_CUDA, "stream creation failed"));
   for (int k = 0; k < 2; ++k)
     if (cudaEventCreateWithFlags(&r->lane_done[k], cudaEventDisableTiming) != cudaSuccess ||
@@ -1749,7 +1821,8 @@ void xb_destroy(xb_renderer* r) {
   for (int d = 0; d < kMaxDepth; ++d)
     for (cudaEvent_t e : {r->ev_shade[d], r->ev_shadow[d], r->ev_shade_b[d], r->ev_shadow_b[d]})
       if (e) cudaEventDestroy(e);
-  for (cudaEvent_t e : {r->lane_done[0], r->lane_done[1], r->lane_acc[0], r->lane_acc[1], r->ev_fork})
+  drop_graphs(r);
+  for (cudaEvent_t e : {r->lane_done[0], r->lane_done[1], r->lane_acc[0], r->lane_acc[1], r->ev_stagger})
     if (e) cudaEventDestroy(e);
   for (cudaStream_t s : {r->stream_b, r->stream_b2}) if (s) cudaStreamDestroy(s);
   if (r->stream2) cudaStreamDestroy(r->stream2);
@@ -1768,6 +1841,7 @@ int xb_set_bounces(xb_renderer* r, int32_t min_b, int32_t max_b) {
   int rc = check_ready(r);
   if (rc) return rc;
   if (min_b < 0 || max_b < 0 || max_b > kMaxDepth) return set_err(r, XB_E_INVALID, "bad bounces %d..%d", min_b, max_b);
+  drop_graphs(r);
   r->min_bounces = min_b;
   r->max_bounces = max_b;
   return XB_OK;
@@ -2158,6 +2232,7 @@ int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
   int rc = check_ready(r);
   if (rc) return rc;
   if (!g) return set_err(r, XB_E_INVALID, "xb_set_guiding: null config");
+  drop_graphs(r);
   xb_guiding c = *g;
   if (c.train_spp == 0) c.train_spp = 32;
   if (c.steps_per_spp == 0) c.steps_per_spp = 64;
