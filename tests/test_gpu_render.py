@@ -155,6 +155,17 @@ def test_captured_bounce_loops_render_identically():
 
     for kw in ({}, {"guided": True}):
         assert np.array_equal(fresh(1, **kw), fresh(2, **kw))
+    views = [(camera(desc.eye, desc.target, f, 1.0), sz, sz, spp, mb)
+             for f, sz, spp, mb in ((40.0, 32, 3, 0), (55.0, 48, 2, 4), (30.0, 40, 4, 6))]
+    vimgs = []
+    for graph in (1, 2):
+        r = Renderer(W, H, desc.max_bounces, desc.min_bounces, wave_paths=W * H)
+        r.upload_scene(hs)
+        r.set_tuning(graph=graph)
+        vimgs.append(r.render_views(views) + r.render_views(views))   # the second call replays
+        r.close()
+    for a, b in zip(*vimgs):
+        assert np.array_equal(a, b)
     r = Renderer(W, H, desc.max_bounces, desc.min_bounces, wave_paths=W * H)
     r.upload_scene(hs)
     r.set_tuning(graph=1)

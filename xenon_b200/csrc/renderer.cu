@@ -26,6 +26,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -117,8 +118,8 @@ struct xb_renderer {
   cudaEvent_t lane_done[2] = {nullptr, nullptr};   // each lane's last wave finished
   cudaEvent_t lane_acc[2] = {nullptr, nullptr};    // each lane's last accumulation finished
   cudaEvent_t ev_stagger = nullptr;                // lane 0's wave has shaded lane_stagger bounces
-  // captured bounce loops of full waves: [lane][plain, guided][bounces before, from the stagger]
-  cudaGraphExec_t bounce_graph[2][2][2] = {};
+  // captured bounce loops, by lane, plain or guided, depth range and bounce limits (bounce_key)
+  std::map<uint32_t, cudaGraphExec_t> bounce_graphs;
   bool graph_broken = false;                       // a capture failed: direct launches from then on
   int num_sms = 0;
   std::string err;
@@ -1126,19 +1127,10 @@ DevMaterial to_dev_material(const xb_material& m) {
 
 // Drops the captured bounce loops (after their launches have finished).
 void drop_graphs(xb_renderer* r) {
-  bool any = false;
-  for (auto& a : r->bounce_graph)
-    for (auto& b : a)
-      for (cudaGraphExec_t g : b) any = any || g != nullptr;
-  if (!any) return;
+  if (r->bounce_graphs.empty()) return;
   for (cudaStream_t s : {r->stream, r->stream2, r->stream_b, r->stream_b2}) if (s) cudaStreamSynchronize(s);
-  for (auto& a : r->bounce_graph)
-    for (auto& b : a)
-      for (cudaGraphExec_t& g : b)
-        if (g) {
-          cudaGraphExecDestroy(g);
-          g = nullptr;
-        }
+  for (auto& kv : r->bounce_graphs) cudaGraphExecDestroy(kv.second);
+  r->bounce_graphs.clear();
 }
 
 void free_scene(xb_renderer* r) {
@@ -1441,23 +1433,29 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
   return XB_OK;
 }
 
-// Bounces [d0, d1) of lane k's wave. With `graph` tuning 1, a full non-training wave of a
-// single-view render replays a CUDA graph captured from the same launches the first time (one
-// per lane, plain or guided, and range); the graphs hold the scene, queue and network pointers
-// and launch settings by value, so every change of those drops them (drop_graphs). Replaying
-// gives the same kernels in the same order, hence the same image.
-int bounce_range(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_stride, int d0, int d1) {
+// Bounces [d0, d1) of lane k's wave, for a bounce loop of `depth` bounces (per-path limits in
+// path_maxd, or none). With `graph` tuning 1, a non-training wave replays a CUDA graph captured
+// from the same launches the first time (one per lane, plain or guided, depth range and bounce
+// limits); the graphs hold the scene, queue and network pointers and launch settings by value,
+// so every change of those drops them (drop_graphs). Raygen and accumulation, which carry the
+// wave's samples and views, are not part of them. Replaying gives the same kernels in the same
+// order, hence the same image.
+int bounce_range(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_stride, int depth,
+                 const int8_t* path_maxd, int d0, int d1) {
   if (d0 >= d1) return XB_OK;
   const bool guided = r->guiding && r->guide;
   if (r->tune.graph != 1 || train || r->prof_flags != 0 || r->graph_broken)
-    return trace_bounces(r, L, train, rec_stride, -1, nullptr, d0, d1);
-  cudaGraphExec_t& ge = r->bounce_graph[k][guided ? 1 : 0][d0 == 0 ? 0 : 1];
-  if (!ge) {
+    return trace_bounces(r, L, train, rec_stride, depth, path_maxd, d0, d1);
+  const uint32_t key = (uint32_t)k | (guided ? 2u : 0u) | (d0 == 0 ? 0u : 4u) | (path_maxd ? 8u : 0u) |
+                       ((uint32_t)depth << 4) | ((uint32_t)d0 << 12);
+  auto it = r->bounce_graphs.find(key);
+  if (it == r->bounce_graphs.end()) {
     cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
     int rc = XB_OK;
     cudaError_t e = cudaStreamBeginCapture(L.s, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      rc = trace_bounces(r, L, false, 1, -1, nullptr, d0, d1);
+      rc = trace_bounces(r, L, false, 1, depth, path_maxd, d0, d1);
       e = cudaStreamEndCapture(L.s, &g);
     }
     if (e == cudaSuccess && rc == XB_OK && g) e = cudaGraphInstantiate(&ge, g, 0);
@@ -1465,24 +1463,25 @@ int bounce_range(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_st
     if (e != cudaSuccess || rc != XB_OK || !ge) {
       // the launches themselves work without capture: take them directly from now on
       cudaGetLastError();
-      ge = nullptr;
+      if (ge) cudaGraphExecDestroy(ge);
       r->graph_broken = true;
-      return trace_bounces(r, L, train, rec_stride, -1, nullptr, d0, d1);
+      return trace_bounces(r, L, train, rec_stride, depth, path_maxd, d0, d1);
     }
+    it = r->bounce_graphs.emplace(key, ge).first;
   }
-  CK(cudaGraphLaunch(ge, L.s));
+  CK(cudaGraphLaunch(it->second, L.s));
   return XB_OK;
 }
 
 // A wave's whole bounce loop: the bounces before the stagger point, lane 0's stagger event,
 // the rest.
-int run_bounces(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_stride) {
-  const int depth_max = std::min(r->max_bounces, kMaxDepth);
-  const int sp = std::min(r->tune.lane_stagger, depth_max);
-  int rc = bounce_range(r, L, k, train, rec_stride, 0, sp);
+int run_bounces(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_stride, int depth,
+                const int8_t* path_maxd) {
+  const int sp = std::min(r->tune.lane_stagger, depth);
+  int rc = bounce_range(r, L, k, train, rec_stride, depth, path_maxd, 0, sp);
   if (rc) return rc;
   if (k == 0) CK(cudaEventRecord(r->ev_stagger, L.s));
-  return bounce_range(r, L, k, train, rec_stride, sp, depth_max);
+  return bounce_range(r, L, k, train, rec_stride, depth, path_maxd, sp, depth);
 }
 
 CamDev cam_dev(const xb_camera& c) {
@@ -1583,7 +1582,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
         raygen_kernel<<<g_rg, 256, 0, L.s>>>(cd, W, H, sample0, paths, w.ray_o[0], w.ray_d[0], w.tp[0],
                                              w.rng[0], w.path[0], w.L, w.cnt);
       }
-      int rc = run_bounces(r, L, k, train, rec_stride);
+      int rc = run_bounces(r, L, k, train, rec_stride, depth_max, nullptr);
       if (rc) return rc;
       const int g_acc = (int)std::min<int64_t>((npix + 255) / 256, (int64_t)r->num_sms * 16);
       ls.before_accumulate(k);
@@ -1665,11 +1664,7 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
       raygen_views_kernel<<<g_rg, 256, 0, L.s>>>(pk, paths, w.ray_o[0], w.ray_d[0], w.tp[0], w.rng[0],
                                                  w.path[0], w.L, w.maxd, w.cnt);
     }
-    const int sp = std::min(r->tune.lane_stagger, wave_depth);
-    int rc = trace_bounces(r, L, false, 1, wave_depth, w.maxd, 0, sp);
-    if (rc) return rc;
-    if (k == 0) CK(cudaEventRecord(r->ev_stagger, L.s));
-    rc = trace_bounces(r, L, false, 1, wave_depth, w.maxd, sp, wave_depth);
+    int rc = run_bounces(r, L, k, false, 1, wave_depth, w.maxd);
     if (rc) return rc;
     const int g_acc = (int)std::min<int64_t>((pix_total + 255) / 256, (int64_t)r->num_sms * 16);
     {
