@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--thread-per-ray", action="store_true", help="one-ray-per-thread traversal kernels")
     ap.add_argument("--no-guiding-study", action="store_true", help="skip the config-4 guided vs plain study")
     ap.add_argument("--no-views-study", action="store_true", help="skip the config-5 many-views study")
+    ap.add_argument("--no-config3", action="store_true", help="skip the config-3 throughput entry")
     ap.add_argument("--views-max-spp", type=int, default=64, help="config 5: cap on a view's spp (0: none)")
     ap.add_argument("--guide-seconds", type=float, default=6.0, help="equal device-time budget per method")
     ap.add_argument("--guide-ref-spp", type=int, default=16384, help="samples of the plain FP64 reference")
@@ -358,6 +359,43 @@ def guiding_study(args, device: int) -> dict:
             "wall_s": time.perf_counter() - t0}
 
 
+def config3_study(args, device: int) -> dict:
+    """Config 3: TLAS over 16x16 instances of 4 seeded meshes (random materials), sky + 4 quad
+    lights, 1920x1080, depth 12, with its autotuned launch settings; device Mrays/s and
+    Msamples/s over a few steps of 4 samples, L2 flushed between steps. The config's 512 spp are
+    this step repeated; its time per sample is what the steps measure."""
+    import torch
+    import xenon_b200 as xb
+    from xenon_b200 import autotune, scenes
+    desc = scenes.instanced_grid()
+    hs = xb.HostScene.from_desc(desc)
+    r = xb.Renderer(desc.width, desc.height, desc.max_bounces, desc.min_bounces, device=device)
+    r.upload_scene(hs)
+    tuned = autotune.load_tuning("config3")
+    if tuned:
+        r.set_tuning(**tuned)
+    cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
+    sps, steps = 4, 6
+    for s in range(2):
+        r.render_range(cam, 1 + s * sps, sps)
+    r.reset()
+    r.reset_stats()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ms = 0.0
+    for s in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        r.render_range(cam, 1 + (2 + s) * sps, sps)
+        ms += r.stats().last_ms
+    st = r.stats()
+    r.close()
+    return {"workload": "config3: 16x16 instances of 4 meshes (82k-328k tris), 1920x1080, depth 12, sky + 4 quads",
+            "spp_per_step": sps, "steps": steps, "ms_per_spp": ms / (steps * sps),
+            "mrays_per_s": (st.rays_closest + st.rays_shadow) / ms / 1e3,
+            "msamples_per_s": st.paths / ms / 1e3, "tuning": tuned or "defaults",
+            "l2": "flushed between steps"}
+
+
 def views_study(args, device: int) -> dict:
     """Config 5: 32 seeded views of the config-3 instanced scene (side log-uniform 256-1024 px,
     spp from {16, 64, 256, 1024} capped at --views-max-spp, bounce limit 6-16) in one
@@ -626,6 +664,12 @@ def main():
             cpu = {"value": None, "unit": "Mrays/s", "cores": None, "kind": "reference",
                    "sample": f"failed: {e}"}
 
+    config3 = None
+    if rank == 0 and ws == 1 and not args.no_config3:
+        try:
+            config3 = config3_study(args, local)
+        except Exception as e:
+            config3 = {"error": f"{type(e).__name__}: {e}"}
     views = None
     if rank == 0 and ws == 1 and not args.no_views_study:
         try:
@@ -652,7 +696,7 @@ def main():
                            "stage_ms_per_step_profiled": {k: getattr(prof, k) / n_prof for k in
                                                  ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms")}},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "guiding": guiding, "views": views}
+                "clocks": clk.summary(), "config3": config3, "guiding": guiding, "views": views}
         print(json.dumps(line))
     r.close()
     if ws > 1:
