@@ -437,6 +437,9 @@ typedef struct xb_guiding {
   int32_t fixed_fraction;   /* 0: the network also outputs the probability of sampling it at each
                              * vertex (in [0.05, 0.95], trained with the mixture);
                              * 1: guide_fraction everywhere */
+  int32_t guided_bounces;   /* the network proposes at bounces 0 .. guided_bounces - 1; later
+                             * vertices sample their BSDF (the path's importance ratio carries
+                             * on); default: every bounce */
 } xb_guiding;
 
 /* Enables, disables or reconfigures guiding (0 fields take defaults). The first enabling, or a

@@ -546,7 +546,11 @@ constexpr size_t kLobBytes = (size_t)xbg::kTile * kLobStride * 4;
 constexpr size_t kGuidedShadeSmem =
     xbg::kFwdWeightBytes + (kLobBytes > xbg::kTileBytes ? kLobBytes : xbg::kTileBytes) + 1024;
 
-// 128 registers and 55 KB of shared memory: four CTAs (16 warps) per SM.
+// 128 registers and 55 KB of shared memory: four CTAs (16 warps) per SM. kNet = false is the
+// same bounce past the bounces the network serves (xb_guiding.guided_bounces): every vertex
+// samples its BSDF, the importance ratio of the path's earlier guided vertices is carried on, and
+// there is no network, shared memory or barrier, so it launches like the plain bounce.
+template <bool kNet>
 __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, GuideShadeArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sW = smem;
@@ -560,8 +564,10 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
   const DevScene& sc = a.sc;
   const bool last_all = (a.depth + 1 >= a.max_bounces);
   const bool training = g.recs != nullptr;
-  xbg::load_forward_weights(sW, sBias, g.wf, g.master);
-  xbg::mma_setup(&tmem_slot, &mbar);
+  if constexpr (kNet) {
+    xbg::load_forward_weights(sW, sBias, g.wf, g.master);
+    xbg::mma_setup(&tmem_slot, &mbar);
+  }
   xbg::Mma m{tmem_slot, &mbar, 0u, g.err, true};
   float* lob = sLob + threadIdx.x * kLobStride;
   for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -630,7 +636,7 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
           // its sampler refracts about (and its pdf can be NaN there), so neither its pdf nor a
           // corrected form of it is the density of what its sampler returns.
           const uint32_t mf = sc.mats[fh.mat_id].flags;
-          guided = (mf & (kMatDelta | kMatTransmissive)) == 0 && dot(fh.normal, -ray.d) > 0.f;
+          guided = kNet && (mf & (kMatDelta | kMatTransmissive)) == 0 && dot(fh.normal, -ray.d) > 0.f;
           for (int k = 0; k < 3; ++k) {
             const float pk = (k == 0 ? fh.pos.x : k == 1 ? fh.pos.y : fh.pos.z);
             feat[k] = fminf(fmaxf((pk - g.bmin[k]) * g.binv[k], 0.f), 1.f);
@@ -641,10 +647,10 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
       }
     }
     // ── the network on this CTA's 128 vertices ──
-    __syncthreads();   // the previous tile's lobes, in the same shared memory, are all read
-    xbg::encode_row<true>(feat, sA, threadIdx.x);
-    float alpha;
-    {
+    float alpha = 0.f;
+    if constexpr (kNet) {
+      __syncthreads();   // the previous tile's lobes, in the same shared memory, are all read
+      xbg::encode_row<true>(feat, sA, threadIdx.x);
       float raw[xbg::kOut];
       xbg::forward_tile(m, sA, sW, sBias, raw);
       if (!m.ok) break;   // uniform: every thread saw the same failed wait
@@ -806,7 +812,7 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
     idx = warp_append(a.cnt + CNT_SH_SUN, emit_sun, a.capacity, a.stats + STAT_OVERFLOW);
     if (idx >= 0) { a.sh_o[1][idx] = s_o; a.sh_d[1][idx] = s_d; a.sh_c[1][idx] = s_c; }
   }
-  xbg::mma_teardown(m.tmem);
+  if constexpr (kNet) xbg::mma_teardown(m.tmem);
 }
 
 // ── many views: raygen and accumulation over a table of pieces ────────────────────
@@ -1413,7 +1419,10 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
       ga.rec_out = train ? w.rec[nq] : nullptr;
       ga.err = xbg::guide_error(gd);
       StageTimer t(r, STAGE_SHADE, L.s);
-      guided_shade_kernel<<<r->grid_gshade, 128, kGuidedShadeSmem, L.s>>>(sa, ga);
+      if (d < r->gcfg.guided_bounces)
+        guided_shade_kernel<true><<<r->grid_gshade, 128, kGuidedShadeSmem, L.s>>>(sa, ga);
+      else
+        guided_shade_kernel<false><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
     } else {
       StageTimer t(r, STAGE_SHADE, L.s);
       shade_kernel<<<r->grid_shade, 128, 0, L.s>>>(sa);
@@ -1752,7 +1761,7 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   r->occ_shade = std::max(occ, 1);
   // guided shade: dynamic shared memory for the weights, one activation tile and the lobes; at
   // most 4 CTAs per SM so their TMEM (64 columns each) always fits the SM's 512 columns
-  if (cudaFuncSetAttribute(guided_shade_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(guided_shade_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kGuidedShadeSmem) != cudaSuccess)
     return bail(xb::fail(XB_E_CUDA, "guided shade kernel attribute failed"));
   {
@@ -1763,7 +1772,7 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, cfg->device);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, cfg->device);
     cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, cfg->device);
-    if (cudaFuncGetAttributes(&fa, guided_shade_kernel) != cudaSuccess)
+    if (cudaFuncGetAttributes(&fa, guided_shade_kernel<true>) != cudaSuccess)
       return bail(xb::fail(XB_E_CUDA, "guided shade kernel attributes failed"));
     const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;
     const int by_regs = regs_sm / std::max(1, warp_regs * 4);
@@ -2236,9 +2245,10 @@ int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
   if (c.guide_fraction == 0.f) c.guide_fraction = 0.7f;
   if (c.max_records == 0) c.max_records = 1 << 21;
   if (c.seed == 0) c.seed = 1;
+  if (c.guided_bounces == 0) c.guided_bounces = kMaxDepth;
   if (c.train_spp < -1 || c.steps_per_spp < 0 || c.steps_per_spp > xbg::kMaxTrainSteps || c.batch < 0 ||
       c.batch % 128 != 0 || c.batch > (1 << 20) || !(c.learning_rate > 0.f) || !(c.guide_fraction > 0.f) ||
-      c.guide_fraction > 1.f || c.max_records < 128 || c.max_records > (1 << 24) || c.record_stride < 0 ||
+      c.guide_fraction > 1.f || c.max_records < 128 || c.max_records > (1 << 24) || c.record_stride < 0 || c.guided_bounces < 0 ||
       (c.fixed_fraction != 0 && c.fixed_fraction != 1) || c.keep_training_samples < 0 || c.keep_training_samples > 2)
     return set_err(r, XB_E_INVALID, "xb_set_guiding: bad configuration");
   if (!c.enabled) {
