@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--level", type=int, default=8, help="icosphere subdivision level (8 = config 2)")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
-    ap.add_argument("--spp-per-step", type=int, default=4,
+    ap.add_argument("--spp-per-step", type=int, default=8,
                     help="samples per pixel rendered by one xb_render call (one step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -375,7 +375,7 @@ def config3_study(args, device: int) -> dict:
     if tuned:
         r.set_tuning(**tuned)
     cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
-    sps, steps = 4, 6
+    sps, steps = 8, 4
     for s in range(2):
         r.render_range(cam, 1 + s * sps, sps)
     r.reset()

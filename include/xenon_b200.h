@@ -334,11 +334,11 @@ typedef struct xb_tuning {
   int32_t overlap;                      /* 1: a bounce's shadow rays run on a second stream,
                                            concurrently with the next bounce's closest hits;
                                            2: one stream */
-  int32_t waves;                        /* waves in flight: 2 (default) runs consecutive waves
-                                           on two stream lanes at once (twice the queue
-                                           memory); 1 one at a time. Same image either way. */
-  int32_t lane_stagger;                 /* with two lanes, a call's second wave starts once the
-                                           first has shaded this many bounces (1-16) */
+  int32_t waves;                        /* waves in flight, 1-4 (default 2): a call's consecutive
+                                           waves run on that many stream lanes at once (each
+                                           lane holds its own queues). Same image either way. */
+  int32_t lane_stagger;                 /* a lane's first wave of a call starts once the previous
+                                           lane's has shaded this many bounces (1-16) */
   int32_t graph;                        /* 1 (default): the bounce loop of a full, non-training
                                            wave of xb_render replays a CUDA graph captured from
                                            its launches on first use; 2: direct launches. Not

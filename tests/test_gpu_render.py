@@ -98,8 +98,8 @@ def test_traversal_variants_render_identically(builder):
 
 @pytest.mark.gpu
 def test_two_waves_in_flight_render_identically():
-    """Consecutive waves on two stream lanes accumulate in sample order: the images (FP32 and
-    FP64 sums, plain and guided, one view and many) equal the one-lane images bit for bit."""
+    """Consecutive waves on two to four stream lanes accumulate in sample order: the images (FP32
+    and FP64 sums, plain and guided, one view and many) equal the one-lane images bit for bit."""
     desc = scenes.instanced_grid(grid=3, levels=(3, 3, 3, 3), with_prims=True)
     hs = HostScene.from_desc(desc)
     W, H = 64, 48
@@ -108,7 +108,7 @@ def test_two_waves_in_flight_render_identically():
              for f, s, spp, mb in ((40.0, 32, 3, 0), (55.0, 48, 2, 4), (30.0, 40, 4, 6))]
     params = None
     out = {}
-    for waves in (1, 2):
+    for waves in (1, 2, 3, 4):
         r = Renderer(W, H, desc.max_bounces, desc.min_bounces, fp64=True, wave_paths=W * H)
         r.upload_scene(hs)
         r.set_tuning(waves=waves)
@@ -126,8 +126,9 @@ def test_two_waves_in_flight_render_identically():
         res += r.render_views(views)             # views split over several waves
         r.close()
         out[waves] = res
-    for a, b in zip(out[1], out[2]):
-        assert np.array_equal(a, b)
+    for waves in (2, 3, 4):
+        for a, b in zip(out[1], out[waves]):
+            assert np.array_equal(a, b)
 
 
 @pytest.mark.gpu

@@ -34,7 +34,7 @@ SPACE = {
     "shadow_persistent": [1, 2],
     "shadow_order": [1, 2],
     "overlap": [1, 2],
-    "waves": [1, 2],
+    "waves": [1, 2, 3, 4],
     "lane_stagger": [1, 2, 3],
     "graph": [1, 2],
     "refill": [2, 4, 8, 16, 24],
@@ -76,7 +76,7 @@ def measure(renderer, cam, calls: int, spp_per_call: int, first: int) -> float:
     return ms / (calls * spp_per_call)
 
 
-def autotune(renderer, cam, workload: str, calls: int = 4, spp_per_call: int = 4, passes: int = 2,
+def autotune(renderer, cam, workload: str, calls: int = 3, spp_per_call: int = 8, passes: int = 2,
              save: bool = True, log=print) -> dict:
     best = dict(renderer.tuning())
     seq = [1000]
@@ -119,8 +119,8 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="config2")
     ap.add_argument("--out", default=None, help="also write the result JSON here")
-    ap.add_argument("--calls", type=int, default=4, help="xb_render calls per measurement")
-    ap.add_argument("--spp-per-call", type=int, default=4, help="samples per xb_render call")
+    ap.add_argument("--calls", type=int, default=3, help="xb_render calls per measurement")
+    ap.add_argument("--spp-per-call", type=int, default=8, help="samples per xb_render call")
     ap.add_argument("--from-saved", action="store_true", help="start from the stored tuning")
     a = ap.parse_args()
     if a.workload == "config2":

@@ -50,6 +50,7 @@ inline float u32_bits_to_f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return
 inline float i32_bits_to_f(int32_t i) { float f; std::memcpy(&f, &i, 4); return f; }
 
 constexpr int kMaxDepth = 64;
+constexpr int kMaxLanes = 4;         // waves in flight at most
 constexpr int kCntStride = 8;        // counters per depth
 enum {
   CNT_RAYS = 0,                      // rays in queue for this depth
@@ -111,13 +112,18 @@ struct xb_renderer {
   cudaEvent_t ev_shade[kMaxDepth] = {};   // bounce d's shading done (its shadow queues are full)
   cudaEvent_t ev_shadow[kMaxDepth] = {};  // bounce d's shadow rays done (path radiance final)
   // the second wave lane (two waves in flight): its own queues, streams and per-bounce events
-  WaveBuffers wb_b;
-  cudaStream_t stream_b = nullptr, stream_b2 = nullptr;
-  cudaEvent_t ev_shade_b[kMaxDepth] = {};
-  cudaEvent_t ev_shadow_b[kMaxDepth] = {};
-  cudaEvent_t lane_done[2] = {nullptr, nullptr};   // each lane's last wave finished
-  cudaEvent_t lane_acc[2] = {nullptr, nullptr};    // each lane's last accumulation finished
-  cudaEvent_t ev_stagger = nullptr;                // lane 0's wave has shaded lane_stagger bounces
+  // wave lanes 1 .. kMaxLanes - 1 (several waves in flight; lane 0 is the fields above): each
+  // with its own queues, streams and per-bounce events
+  struct ExtraLane {
+    WaveBuffers wb;
+    cudaStream_t s = nullptr, s2 = nullptr;
+    cudaEvent_t ev_shade[kMaxDepth] = {};
+    cudaEvent_t ev_shadow[kMaxDepth] = {};
+  } lane_x[kMaxLanes - 1];
+  int lanes_alloc = 0;                              // lanes whose queues are allocated
+  cudaEvent_t lane_done[kMaxLanes] = {};            // each lane's last wave finished
+  cudaEvent_t lane_acc[kMaxLanes] = {};             // each lane's last accumulation finished
+  cudaEvent_t ev_stagger[kMaxLanes] = {};           // the lane's wave has shaded lane_stagger bounces
   // captured bounce loops, by lane, plain or guided, depth range and bounce limits (bounce_key)
   std::map<uint32_t, cudaGraphExec_t> bounce_graphs;
   bool graph_broken = false;                       // a capture failed: direct launches from then on
@@ -1131,10 +1137,16 @@ DevMaterial to_dev_material(const xb_material& m) {
   return o;
 }
 
+void sync_lanes(xb_renderer* r) {
+  for (cudaStream_t s : {r->stream, r->stream2}) if (s) cudaStreamSynchronize(s);
+  for (auto& x : r->lane_x)
+    for (cudaStream_t s : {x.s, x.s2}) if (s) cudaStreamSynchronize(s);
+}
+
 // Drops the captured bounce loops (after their launches have finished).
 void drop_graphs(xb_renderer* r) {
   if (r->bounce_graphs.empty()) return;
-  for (cudaStream_t s : {r->stream, r->stream2, r->stream_b, r->stream_b2}) if (s) cudaStreamSynchronize(s);
+  sync_lanes(r);
   for (auto& kv : r->bounce_graphs) cudaGraphExecDestroy(kv.second);
   r->bounce_graphs.clear();
 }
@@ -1158,9 +1170,10 @@ void free_wave_buffers(WaveBuffers& w) {
 
 void free_wave(xb_renderer* r) {
   drop_graphs(r);
-  for (cudaStream_t s : {r->stream, r->stream2, r->stream_b, r->stream_b2}) if (s) cudaStreamSynchronize(s);
+  sync_lanes(r);
   free_wave_buffers(r->wb);
-  free_wave_buffers(r->wb_b);
+  for (auto& x : r->lane_x) free_wave_buffers(x.wb);
+  r->lanes_alloc = 0;
 }
 
 template <class T>
@@ -1211,10 +1224,13 @@ bool alloc_wave_buffers(WaveBuffers& w, int64_t cap) {
 // Queues for `cap` paths per wave, in both lanes when two waves run at once.
 int alloc_wave(xb_renderer* r, int64_t cap) {
   free_wave(r);
-  if (!alloc_wave_buffers(r->wb, cap) || (r->tune.waves == 2 && !alloc_wave_buffers(r->wb_b, cap))) {
+  bool ok = alloc_wave_buffers(r->wb, cap);
+  for (int k = 1; ok && k < r->tune.waves; ++k) ok = alloc_wave_buffers(r->lane_x[k - 1].wb, cap);
+  if (!ok) {
     free_wave(r);
     return set_err(r, XB_E_OOM, "cannot allocate wave buffers for %lld paths", (long long)cap);
   }
+  r->lanes_alloc = r->tune.waves;
   return XB_OK;
 }
 
@@ -1238,7 +1254,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.wave_paths = pick(t.wave_paths, c.wave_paths, 1 << 21);
   c.shadow_order = pick(t.shadow_order, c.shadow_order, 1);
   c.overlap = pick(t.overlap, c.overlap, 1);
-  c.waves = std::min(2, pick(t.waves, c.waves, 2));
+  c.waves = std::min(kMaxLanes, pick(t.waves, c.waves, 2));
   c.lane_stagger = std::min(kMaxDepth, pick(t.lane_stagger, c.lane_stagger, 1));
   c.graph = std::min(2, pick(t.graph, c.graph, 1));
   drop_graphs(r);
@@ -1257,7 +1273,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   r->grid_gshade = r->num_sms * std::min(r->occ_gshade, c.shade_blocks_per_sm);
   const int64_t npix = (int64_t)r->cfg.width * r->cfg.height;
   const int spw = (int)std::min<int64_t>(1024, std::max<int64_t>(1, c.wave_paths / npix));
-  if (spw != r->spp_per_wave || r->wb.capacity == 0 || (c.waves == 2) != (r->wb_b.capacity > 0)) {
+  if (spw != r->spp_per_wave || r->wb.capacity == 0 || c.waves != r->lanes_alloc) {
     r->spp_per_wave = spw;
     return alloc_wave(r, npix * spw);
   }
@@ -1326,8 +1342,9 @@ struct LaneRef {
 };
 
 LaneRef lane_ref(xb_renderer* r, int k) {
-  return k == 0 ? LaneRef{&r->wb, r->stream, r->stream2, r->ev_shade, r->ev_shadow}
-                : LaneRef{&r->wb_b, r->stream_b, r->stream_b2, r->ev_shade_b, r->ev_shadow_b};
+  if (k == 0) return LaneRef{&r->wb, r->stream, r->stream2, r->ev_shade, r->ev_shadow};
+  auto& x = r->lane_x[k - 1];
+  return LaneRef{&x.wb, x.s, x.s2, x.ev_shade, x.ev_shadow};
 }
 
 void launch_extend(xb_renderer* r, const LaneRef& L, int d, bool count) {
@@ -1455,8 +1472,8 @@ int bounce_range(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_st
   const bool guided = r->guiding && r->guide;
   if (r->tune.graph != 1 || train || r->prof_flags != 0 || r->graph_broken)
     return trace_bounces(r, L, train, rec_stride, depth, path_maxd, d0, d1);
-  const uint32_t key = (uint32_t)k | (guided ? 2u : 0u) | (d0 == 0 ? 0u : 4u) | (path_maxd ? 8u : 0u) |
-                       ((uint32_t)depth << 4) | ((uint32_t)d0 << 12);
+  const uint32_t key = (uint32_t)k | (guided ? 4u : 0u) | (path_maxd ? 8u : 0u) | ((uint32_t)depth << 4) |
+                       ((uint32_t)d0 << 12);
   auto it = r->bounce_graphs.find(key);
   if (it == r->bounce_graphs.end()) {
     cudaGraph_t g = nullptr;
@@ -1489,7 +1506,7 @@ int run_bounces(xb_renderer* r, const LaneRef& L, int k, bool train, int rec_str
   const int sp = std::min(r->tune.lane_stagger, depth);
   int rc = bounce_range(r, L, k, train, rec_stride, depth, path_maxd, 0, sp);
   if (rc) return rc;
-  if (k == 0) CK(cudaEventRecord(r->ev_stagger, L.s));
+  CK(cudaEventRecord(r->ev_stagger[k], L.s));
   return bounce_range(r, L, k, train, rec_stride, depth, path_maxd, sp, depth);
 }
 
@@ -1499,33 +1516,30 @@ CamDev cam_dev(const xb_camera& c) {
                 v3(c.vertical[0], c.vertical[1], c.vertical[2])};
 }
 
-// Two waves in flight: wave i of a call runs on lane i % 2 (lane 0 is the renderer's stream),
-// so one wave's latency-bound stretches and kernel tails run beside the other's bulk. Lane 1
-// first waits for the main stream's work before the call. Every accumulation waits for the
+// Several waves in flight: wave i of a call runs on lane i % lanes (lane 0 is the renderer's
+// stream), so one wave's latency-bound stretches and kernel tails run beside the others' bulk.
+// The first wave of lane k > 0 starts once lane k - 1's first wave has shaded its first
+// lane_stagger bounces (ev_stagger), so the waves' widest bounces do not coincide; through lane
+// 0 it also follows the main stream's work before the call. Every accumulation waits for the
 // previous wave's, so the image's sums keep sample order and equal a single lane's bit for bit.
 // A serial wave (guide training: the network changes after it and the records buffer is
-// shared) waits for the other lane, and the other lane's next wave waits for it. At the end
-// the main stream waits for lane 1.
+// shared) waits for every other lane, and every other lane's next wave waits for it. At the end
+// the main stream waits for every lane.
 struct LaneSched {
   xb_renderer* r;
   int lanes;
   int next = 0;
   int last_acc = -1;
-  bool has[2] = {false, false}, serial[2] = {false, false};
+  bool has[kMaxLanes] = {}, serial[kMaxLanes] = {};
 
-  LaneSched(xb_renderer* rr) : r(rr), lanes(rr->tune.waves == 2 && rr->wb_b.capacity > 0 ? 2 : 1) {}
+  LaneSched(xb_renderer* rr) : r(rr), lanes(std::max(1, std::min(rr->tune.waves, rr->lanes_alloc))) {}
   int begin(bool is_serial) {
     const int k = next;
     next = (next + 1) % lanes;
-    const int o = k ^ 1;
     const LaneRef L = lane_ref(r, k);
-    if (k == 1 && !has[1]) {
-      // lane 1's first wave starts once lane 0's has shaded its first lane_stagger bounces
-      // (ev_stagger), so the two waves' widest bounces do not coincide; the main stream's work
-      // before the call, which lane 0 follows, is then done as well
-      cudaStreamWaitEvent(L.s, r->ev_stagger, 0);
-    }
-    if (lanes == 2 && has[o] && (is_serial || serial[o])) cudaStreamWaitEvent(L.s, r->lane_done[o], 0);
+    if (k > 0 && !has[k]) cudaStreamWaitEvent(L.s, r->ev_stagger[k - 1], 0);
+    for (int o = 0; o < lanes; ++o)
+      if (o != k && has[o] && (is_serial || serial[o])) cudaStreamWaitEvent(L.s, r->lane_done[o], 0);
     has[k] = true;
     serial[k] = is_serial;
     return k;
@@ -1538,8 +1552,9 @@ struct LaneSched {
     last_acc = k;
   }
   void end_wave(int k) { cudaEventRecord(r->lane_done[k], lane_ref(r, k).s); }
-  ~LaneSched() {   // every return path: the main stream takes in lane 1's work
-    if (has[1]) cudaStreamWaitEvent(r->stream, r->lane_done[1], 0);
+  ~LaneSched() {   // every return path: the main stream takes in the other lanes' work
+    for (int k = 1; k < lanes; ++k)
+      if (has[k]) cudaStreamWaitEvent(r->stream, r->lane_done[k], 0);
   }
 };
 
@@ -1722,17 +1737,21 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
       return bail(xb::fail(XB_E_CUDA, "event creation failed"));
   for (int d = 0; d < kMaxDepth; ++d)
     if (cudaEventCreateWithFlags(&r->ev_shade[d], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&r->ev_shadow[d], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&r->ev_shade_b[d], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&r->ev_shadow_b[d], cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&r->ev_shadow[d], cudaEventDisableTiming) != cudaSuccess)
       return bail(xb::fail(XB_E_CUDA, "event creation failed"));
-  if (cudaStreamCreateWithFlags(&r->stream_b, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&r->stream_b2, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&r->ev_stagger, cudaEventDisableTiming) != cudaSuccess)
-    return bail(xb::fail(XB_E_CUDA, "stream creation failed"));
-  for (int k = 0; k < 2; ++k)
+  for (auto& x : r->lane_x) {
+    if (cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&x.s2, cudaStreamNonBlocking) != cudaSuccess)
+      return bail(xb::fail(XB_E_CUDA, "stream creation failed"));
+    for (int d = 0; d < kMaxDepth; ++d)
+      if (cudaEventCreateWithFlags(&x.ev_shade[d], cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&x.ev_shadow[d], cudaEventDisableTiming) != cudaSuccess)
+        return bail(xb::fail(XB_E_CUDA, "event creation failed"));
+  }
+  for (int k = 0; k < kMaxLanes; ++k)
     if (cudaEventCreateWithFlags(&r->lane_done[k], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&r->lane_acc[k], cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&r->lane_acc[k], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ev_stagger[k], cudaEventDisableTiming) != cudaSuccess)
       return bail(xb::fail(XB_E_CUDA, "event creation failed"));
   if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&r->ev0) != cudaSuccess || cudaEventCreate(&r->ev1) != cudaSuccess)
@@ -1804,7 +1823,7 @@ void xb_destroy(xb_renderer* r) {
   if (!r) return;
   cudaSetDevice(r->cfg.device);
   if (r->stream) cudaStreamSynchronize(r->stream);
-  for (cudaStream_t s : {r->stream_b, r->stream_b2}) if (s) cudaStreamSynchronize(s);
+  sync_lanes(r);
   free_scene(r);
   free_wave(r);
   xbg::guide_destroy(r->guide);
@@ -1823,12 +1842,18 @@ void xb_destroy(xb_renderer* r) {
   if (r->ev1) cudaEventDestroy(r->ev1);
   if (r->stream2) cudaStreamSynchronize(r->stream2);
   for (int d = 0; d < kMaxDepth; ++d)
-    for (cudaEvent_t e : {r->ev_shade[d], r->ev_shadow[d], r->ev_shade_b[d], r->ev_shadow_b[d]})
+    for (cudaEvent_t e : {r->ev_shade[d], r->ev_shadow[d]})
       if (e) cudaEventDestroy(e);
   drop_graphs(r);
-  for (cudaEvent_t e : {r->lane_done[0], r->lane_done[1], r->lane_acc[0], r->lane_acc[1], r->ev_stagger})
-    if (e) cudaEventDestroy(e);
-  for (cudaStream_t s : {r->stream_b, r->stream_b2}) if (s) cudaStreamDestroy(s);
+  for (int k = 0; k < kMaxLanes; ++k)
+    for (cudaEvent_t e : {r->lane_done[k], r->lane_acc[k], r->ev_stagger[k]})
+      if (e) cudaEventDestroy(e);
+  for (auto& x : r->lane_x) {
+    for (int d = 0; d < kMaxDepth; ++d)
+      for (cudaEvent_t e : {x.ev_shade[d], x.ev_shadow[d]})
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t st : {x.s, x.s2}) if (st) cudaStreamDestroy(st);
+  }
   if (r->stream2) cudaStreamDestroy(r->stream2);
   if (r->stream) cudaStreamDestroy(r->stream);
   delete r;
