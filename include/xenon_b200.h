@@ -343,6 +343,9 @@ typedef struct xb_tuning {
                                            wave of xb_render replays a CUDA graph captured from
                                            its launches on first use; 2: direct launches. Not
                                            used while profiling. Same image either way. */
+  int32_t guided_form;                  /* guided bounces: 1 (default) a plain-form bounce kernel
+                                           plus a network pass over the guided vertices; 2 one
+                                           fused kernel. Same image either way. */
 } xb_tuning;
 int  xb_set_tuning(xb_renderer *r, const xb_tuning *t);
 int  xb_get_tuning(const xb_renderer *r, xb_tuning *out);

@@ -131,6 +131,31 @@ def test_guide_params_round_trip_and_stats():
 
 
 @pytest.mark.gpu
+def test_guided_forms_render_identically():
+    """The two-kernel guided bounce (plain-form bounce + network pass over the guided vertices)
+    and the fused one draw the same numbers and evaluate the same network per vertex: equal
+    images, for one view and for views, with a network that holds still (no training)."""
+    d, sc, cam = _room(True)
+    params = None
+    out = {}
+    for form in (1, 2):
+        r = xb.Renderer(W, H, max_bounces=16, min_bounces=3, wave_paths=W * H)
+        r.upload_scene(sc)
+        r.set_tuning(guided_form=form)
+        r.set_guiding(True, train_spp=-1)
+        if params is None:
+            params = xb.guide_init_params(7)
+            params[-48:] += 0.3       # output biases: lobes and selection away from the symmetric start
+        r.set_guide_params(params)
+        r.render_frame(cam, 4)
+        views = [(xb.camera(d.eye, d.target, 50.0, 1.0), 24, 24, 3, 12)]
+        out[form] = [r.resolve().copy()] + r.render_views(views)
+        r.close()
+    for a, b in zip(out[1], out[2]):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
 def test_keep_training_samples_modes():
     """0: the training samples stay out; 1: all kept; 2: those after train_spp / 2 kept; the
     kept ones are exactly the samples a plain accumulation of those indices would add."""

@@ -37,6 +37,7 @@ SPACE = {
     "waves": [1, 2, 3, 4],
     "lane_stagger": [1, 2, 3],
     "graph": [1, 2],
+    "guided_form": [1, 2],
     "refill": [2, 4, 8, 16, 24],
     "extend_blocks_per_sm": [2, 4, 8, 16, 64],
     "shadow_blocks_per_sm": [2, 4, 8, 16, 64],

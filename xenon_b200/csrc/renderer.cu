@@ -59,6 +59,7 @@ enum {
   CNT_FETCH_EXT = 3,                 // work-fetch cursors
   CNT_FETCH_SH_AREA = 4,
   CNT_FETCH_SH_SUN = 5,
+  CNT_GUIDE = 6,                     // guided vertices deferred to the network pass
 };
 enum { STAT_RAYS = 0, STAT_SHADOW = 1, STAT_PATHS = 2, STAT_OVERFLOW = 3,
        STAT_OVERFLOW_AT_START = 4,  // STAT_OVERFLOW when the current render call began
@@ -100,6 +101,11 @@ struct WaveBuffers {
   int32_t* rec[2] = {nullptr, nullptr};   // guiding: training record of the emitting vertex
   float* ratio[2] = {nullptr, nullptr};   // guiding: importance ratio of the path
   int8_t* maxd = nullptr;                 // views: bounce limit of each path
+  // guiding, two-kernel form: vertices whose direction the network pass samples (see
+  // guide_sample_kernel): position + material, shading normal + path, geometric normal + ratio,
+  // outgoing direction, throughput; and the PCG state
+  float4* gq[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  uint64_t* gq_rng = nullptr;
 };
 
 }  // namespace
@@ -543,6 +549,8 @@ struct GuideShadeArgs {
   const int32_t* rec_in;     // record of the vertex that emitted each incoming ray (or nullptr)
   int32_t* rec_out;          // same for the outgoing queue
   int* err;
+  float4* gq[5];             // two-kernel form: the deferred vertices (nullptr: fused form)
+  uint64_t* gq_rng;
 };
 
 constexpr float kNaN = __builtin_nanf("");
@@ -578,13 +586,14 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
   float* lob = sLob + threadIdx.x * kLobStride;
   for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     const int slot = base + threadIdx.x;
-    bool emit_next = false, emit_area = false, emit_sun = false, emit_rec = false;
+    bool emit_next = false, emit_area = false, emit_sun = false, emit_rec = false, emit_defer = false;
     float4 n_o, n_d, n_tp;
     uint64_t n_rng = 0;
     int32_t pid = 0;
     float n_ratio = 1.f;
     float4 a_o, a_d, a_c, s_o, s_d, s_c;
     float4 rec[6];
+    float4 dq[5];
     // ── phase 1: emitter test and the network's input ──
     bool alive = false, guided = false;
     float feat[9] = {0.5f, 0.5f, 0.5f, 0.f, 0.f, 1.f, 0.f, 0.f, 1.f};
@@ -642,7 +651,8 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
           // its sampler refracts about (and its pdf can be NaN there), so neither its pdf nor a
           // corrected form of it is the density of what its sampler returns.
           const uint32_t mf = sc.mats[fh.mat_id].flags;
-          guided = kNet && (mf & (kMatDelta | kMatTransmissive)) == 0 && dot(fh.normal, -ray.d) > 0.f;
+          guided = (kNet || g.gq[0] != nullptr) && (mf & (kMatDelta | kMatTransmissive)) == 0 &&
+                   dot(fh.normal, -ray.d) > 0.f;
           for (int k = 0; k < 3; ++k) {
             const float pk = (k == 0 ? fh.pos.x : k == 1 ? fh.pos.y : fh.pos.z);
             feat[k] = fminf(fmaxf((pk - g.bmin[k]) * g.binv[k], 0.f), 1.f);
@@ -745,6 +755,17 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
         tp = tp / p;
         ratio = ratio * (surv / surv_g);
       }
+      if (!kNet && guided) {
+        // two-kernel form: the network pass samples this vertex's direction
+        dq[0] = make_float4(fh.pos.x, fh.pos.y, fh.pos.z, __int_as_float(fh.mat_id));
+        dq[1] = make_float4(fh.normal.x, fh.normal.y, fh.normal.z, __int_as_float(pid));
+        dq[2] = make_float4(fh.geo_normal.x, fh.geo_normal.y, fh.geo_normal.z, ratio);
+        dq[3] = make_float4(-ray.d.x, -ray.d.y, -ray.d.z, 0.f);
+        dq[4] = make_float4(tp.x, tp.y, tp.z, 0.f);
+        n_rng = rng.state;
+        emit_defer = true;
+        break;
+      }
       const Onb onb(fh.normal);
       const V3 wo_l = onb.to_local(-ray.d);
       BsdfSample s;
@@ -798,6 +819,13 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
       emit_next = true;
     } while (false);
     if (!emit_next) emit_rec = false;
+    if constexpr (!kNet) {
+      const int gi = warp_append(a.cnt + CNT_GUIDE, emit_defer, a.capacity, a.stats + STAT_OVERFLOW);
+      if (gi >= 0) {
+        for (int k = 0; k < 5; ++k) g.gq[k][gi] = dq[k];
+        g.gq_rng[gi] = n_rng;
+      }
+    }
     int ridx = -1;
     if (training) {
       ridx = warp_append(g.rec_count, emit_rec, g.rec_cap, a.stats + STAT_REC_DROPPED);
@@ -819,6 +847,130 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
     if (idx >= 0) { a.sh_o[1][idx] = s_o; a.sh_d[1][idx] = s_d; a.sh_c[1][idx] = s_c; }
   }
   if constexpr (kNet) xbg::mma_teardown(m.tmem);
+}
+
+// ── guided directions, two-kernel form: the network pass over the deferred vertices ───────
+// Given a guide queue, the bounce kernel (guided_shade_kernel<false>) does all of a bounce but
+// the next direction of the guided vertices, which it queues with their state after next-event
+// estimation and roulette. This persistent kernel runs the network on dense 128-vertex tiles of
+// that queue and samples each direction as the fused kernel does: the same draws from the same
+// PCG state, the same proposal, importance ratio and records — and a row's network output does
+// not depend on the rest of its tile — so the two forms render the same image. The bounce
+// kernel then launches like the plain bounce (no barriers or network state), beside the other
+// wave lanes' kernels.
+__global__ void __launch_bounds__(128, 4) guide_sample_kernel(ShadeArgs a, GuideShadeArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* sW = smem;
+  uint8_t* sA = smem + xbg::kFwdWeightBytes;
+  float* sLob = reinterpret_cast<float*>(sA);
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ float sBias[xbg::kBiasFloats];
+  const int n = a.cnt[CNT_GUIDE];
+  if ((int)blockIdx.x * 128 >= n) return;
+  const DevScene& sc = a.sc;
+  const bool training = g.recs != nullptr;
+  xbg::load_forward_weights(sW, sBias, g.wf, g.master);
+  xbg::mma_setup(&tmem_slot, &mbar);
+  xbg::Mma m{tmem_slot, &mbar, 0u, g.err, true};
+  float* lob = sLob + threadIdx.x * kLobStride;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int slot = base + threadIdx.x;
+    const bool valid = slot < n;
+    float4 q[5];
+    for (int k = 0; k < 5; ++k) q[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    Pcg rng{0};
+    float feat[9] = {0.5f, 0.5f, 0.5f, 0.f, 0.f, 1.f, 0.f, 0.f, 1.f};
+    if (valid) {
+      for (int k = 0; k < 5; ++k) q[k] = g.gq[k][slot];
+      rng.state = g.gq_rng[slot];
+      feat[0] = fminf(fmaxf((q[0].x - g.bmin[0]) * g.binv[0], 0.f), 1.f);
+      feat[1] = fminf(fmaxf((q[0].y - g.bmin[1]) * g.binv[1], 0.f), 1.f);
+      feat[2] = fminf(fmaxf((q[0].z - g.bmin[2]) * g.binv[2], 0.f), 1.f);
+      feat[3] = q[1].x; feat[4] = q[1].y; feat[5] = q[1].z;
+      feat[6] = q[3].x; feat[7] = q[3].y; feat[8] = q[3].z;
+    }
+    __syncthreads();   // the previous tile's lobes, in the same shared memory, are all read
+    xbg::encode_row<true>(feat, sA, threadIdx.x);
+    float alpha;
+    {
+      float raw[xbg::kOut];
+      xbg::forward_tile(m, sA, sW, sBias, raw);
+      if (!m.ok) break;   // uniform: every thread saw the same failed wait
+      xbg::raw_to_lobes<true>(raw, lob);
+      alpha = g.alpha >= 0.f ? g.alpha : xbg::selection<true>(raw);
+    }
+    bool emit_next = false, emit_rec = false;
+    float4 n_o, n_d, n_tp;
+    float4 rec[6];
+    uint64_t n_rng = 0;
+    float n_ratio = 1.f;
+    const int32_t pid = __float_as_int(q[1].w);
+    if (valid) do {
+      const DevMaterial& mat = sc.mats[__float_as_int(q[0].w)];
+      const V3 pos = v3(q[0].x, q[0].y, q[0].z), gn = v3(q[2].x, q[2].y, q[2].z);
+      const float ratio = q[2].w;
+      V3 tp = v3(q[4].x, q[4].y, q[4].z);
+      const Onb onb(v3(q[1].x, q[1].y, q[1].z));
+      const V3 wo_l = onb.to_local(v3(q[3].x, q[3].y, q[3].z));
+      BsdfSample s;
+      V3 wiw;
+      float pb;
+      if (rng.next_float() < alpha) {
+        const float u0 = rng.next_float(), u1 = rng.next_float(), u2 = rng.next_float();
+        float d[3];
+        xbg::mix_sample(lob, u0, u1, u2, d);
+        wiw = v3(d[0], d[1], d[2]);
+        s.wi = onb.to_local(wiw);
+        s.delta = false;
+        if (!bsdf_lobe_for_direction(wo_l, s.wi, mat, rng.next_float(), s.f, s.pdf, pb)) break;
+      } else {
+        if (!bsdf_sample(wo_l, mat, rng, s)) break;
+        wiw = onb.to_world(s.wi);
+        pb = bsdf_density(wo_l, s.wi, mat);
+      }
+      const float pm = alpha * xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) + (1.f - alpha) * pb;
+      if (!(pm > 0.f)) break;
+      n_ratio = ratio * (pb / pm);
+      if (training && (pid % g.rec_stride) == 0) {
+        const V3 tb = tp * ratio;   // actual throughput before the vertex's scattering
+        rec[0] = make_float4(feat[0], feat[1], feat[2], feat[3]);
+        rec[1] = make_float4(feat[4], feat[5], feat[6], feat[7]);
+        rec[2] = make_float4(feat[8], wiw.x, wiw.y, wiw.z);
+        rec[3] = make_float4(0.f, __int_as_float(pid), tb.x, tb.y);
+        rec[4] = make_float4(tb.z, kNaN, kNaN, kNaN);   // baseline: set by the next bounce
+        rec[5] = make_float4(pb, 0.f, 0.f, 0.f);
+        emit_rec = true;
+      }
+      // cpu_tiled.cpp:197-216 (the guided lobes are never delta)
+      const float ci = fabsf(s.wi.z);
+      if (s.pdf < 1e-8f || ci < 1e-8f) { emit_rec = false; break; }
+      tp = tp * (s.f * ci / s.pdf);
+      const V3 org = offset_origin(pos, gn, wiw, kRayEps);
+      n_o = make_float4(org.x, org.y, org.z, kRayEps);
+      n_d = make_float4(wiw.x, wiw.y, wiw.z, kInf);
+      n_tp = make_float4(tp.x, tp.y, tp.z, s.pdf);
+      n_rng = rng.state;
+      emit_next = true;
+    } while (false);
+    if (!emit_next) emit_rec = false;
+    int ridx = -1;
+    if (training) {
+      ridx = warp_append(g.rec_count, emit_rec, g.rec_cap, a.stats + STAT_REC_DROPPED);
+      if (ridx >= 0) {
+        float4* R = reinterpret_cast<float4*>(g.recs + (size_t)ridx * xbg::kRecFloats);
+        for (int i = 0; i < 6; ++i) R[i] = rec[i];
+      }
+    }
+    const int idx = warp_append(a.cnt_next + CNT_RAYS, emit_next, a.capacity, a.stats + STAT_OVERFLOW);
+    if (idx >= 0) {
+      a.nray_o[idx] = n_o; a.nray_d[idx] = n_d; a.ntp[idx] = n_tp; a.nrng[idx] = n_rng;
+      a.npath[idx] = pid;
+      g.ratio_out[idx] = n_ratio;
+      if (g.rec_out) g.rec_out[idx] = ridx;
+    }
+  }
+  xbg::mma_teardown(m.tmem);
 }
 
 // ── many views: raygen and accumulation over a table of pieces ────────────────────
@@ -1163,7 +1315,7 @@ void free_wave_buffers(WaveBuffers& w) {
   void* ptrs[] = {w.ray_o[0], w.ray_o[1], w.ray_d[0], w.ray_d[1], w.tp[0], w.tp[1], w.rng[0],
                   w.rng[1], w.path[0], w.path[1], w.hit, w.hit_inst, w.sh_o[0], w.sh_o[1],
                   w.sh_d[0], w.sh_d[1], w.sh_c[0], w.sh_c[1], w.L, w.cnt, w.rec[0], w.rec[1],
-                  w.ratio[0], w.ratio[1], w.maxd};
+                  w.ratio[0], w.ratio[1], w.maxd, w.gq[0], w.gq[1], w.gq[2], w.gq[3], w.gq[4], w.gq_rng};
   for (void* p : ptrs) if (p) cudaFree(p);
   w = WaveBuffers();
 }
@@ -1218,6 +1370,8 @@ bool alloc_wave_buffers(WaveBuffers& w, int64_t cap) {
   ok &= A(&w.hit_inst, cap * sizeof(int32_t));
   ok &= A(&w.L, cap * sizeof(float4));
   ok &= A(&w.cnt, (kMaxDepth + 1) * kCntStride * sizeof(int32_t));
+  for (int k = 0; k < 5; ++k) ok &= A(&w.gq[k], cap * sizeof(float4));
+  ok &= A(&w.gq_rng, cap * sizeof(uint64_t));
   return ok;
 }
 
@@ -1257,6 +1411,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.waves = std::min(kMaxLanes, pick(t.waves, c.waves, 2));
   c.lane_stagger = std::min(kMaxDepth, pick(t.lane_stagger, c.lane_stagger, 1));
   c.graph = std::min(2, pick(t.graph, c.graph, 1));
+  c.guided_form = std::min(2, pick(t.guided_form, c.guided_form, 1));
   drop_graphs(r);
   r->ext_persistent_from = c.extend_persistent_from_depth;
   r->shadow_persistent = c.shadow_persistent == 1;
@@ -1420,8 +1575,9 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
     sa.path_maxd = path_maxd;
     sa.capacity = (int)w.capacity;
     sa.stats = r->stats;
+    bool network_pass = false;
+    GuideShadeArgs ga{};
     if (gd) {
-      GuideShadeArgs ga;
       ga.wf = xbg::guide_weights_bf16(gd);
       ga.master = xbg::guide_master(gd);
       ga.alpha = r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f;
@@ -1436,15 +1592,26 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
       ga.rec_out = train ? w.rec[nq] : nullptr;
       ga.err = xbg::guide_error(gd);
       StageTimer t(r, STAGE_SHADE, L.s);
-      if (d < r->gcfg.guided_bounces)
+      const bool net = d < r->gcfg.guided_bounces;
+      if (net && r->tune.guided_form == 2) {
         guided_shade_kernel<true><<<r->grid_gshade, 128, kGuidedShadeSmem, L.s>>>(sa, ga);
-      else
+      } else {
+        if (net) {   // two-kernel form: the guided vertices' directions come from the network pass
+          for (int k = 0; k < 5; ++k) ga.gq[k] = w.gq[k];
+          ga.gq_rng = w.gq_rng;
+          network_pass = true;
+        }
         guided_shade_kernel<false><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
+      }
     } else {
       StageTimer t(r, STAGE_SHADE, L.s);
       shade_kernel<<<r->grid_shade, 128, 0, L.s>>>(sa);
     }
     CK(cudaEventRecord(L.ev_shade[d], L.s));
+    if (network_pass) {   // beside the shadow rays of this bounce, before the next closest hits
+      StageTimer t(r, STAGE_SHADE, L.s);
+      guide_sample_kernel<<<r->grid_gshade, 128, kGuidedShadeSmem, L.s>>>(sa, ga);
+    }
     if (!ov) {
       launch_shadows(r, L, d, count, L.s);
       continue;
@@ -1780,6 +1947,9 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   r->occ_shade = std::max(occ, 1);
   // guided shade: dynamic shared memory for the weights, one activation tile and the lobes; at
   // most 4 CTAs per SM so their TMEM (64 columns each) always fits the SM's 512 columns
+  if (cudaFuncSetAttribute(guide_sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kGuidedShadeSmem) != cudaSuccess)
+    return bail(xb::fail(XB_E_CUDA, "guide sample kernel attribute failed"));
   if (cudaFuncSetAttribute(guided_shade_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kGuidedShadeSmem) != cudaSuccess)
     return bail(xb::fail(XB_E_CUDA, "guided shade kernel attribute failed"));
