@@ -588,7 +588,7 @@ def main():
     # themselves, while in the timed region the other lane's kernels run beside them
     lanes = r.tuning()["waves"]
     one_lane = None
-    if lanes == 2:
+    if lanes > 1:
         r.set_tuning(waves=1)
         r.reset_profile()
         r.reset_stats()
@@ -601,18 +601,19 @@ def main():
         a1 = ext_bytes_per_ray * r.stats().rays_closest / max(p1.extend_ms * 1e-3, 1e-12) / 1e9
         one_lane = {"achieved": a1, "frac": a1 / peaks["hbm_gbs"], "extend_ms_per_launch":
                     p1.extend_ms / max(p1.extend_launches, 1)}
-        r.set_tuning(waves=2)
+        r.set_tuning(waves=lanes)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                 "peak_source": peaks["source"], "kernel": "extend_kernel (closest-hit traversal)",
                 "algorithmic_bytes_per_ray": ext_bytes_per_ray,
                 "extend_launch_ms_per_step": prof.extend_ms / n_prof, "waves_in_flight": lanes,
                 "timing": f"events around each launch over {n_prof} steps of the timed workload run again "
-                          "with stage timing (the timed steps replay captured graphs); with two waves in "
-                          "flight each extend launch shares the GPU with the other lane's kernels, so its "
-                          "duration includes that sharing; one_lane is the same kernel with one wave in "
-                          f"flight; the profiled steps took {prof_ms / n_prof:.3f} ms each against "
-                          f"{dev_ms / args.steps:.3f} in the timed region",
+                          "with stage timing (the timed steps replay captured graphs); the profiled steps "
+                          f"took {prof_ms / n_prof:.3f} ms each against {dev_ms / args.steps:.3f} in the "
+                          "timed region" + (f"; with {lanes} waves in flight each extend launch shares the "
+                                            "GPU with the other lanes' kernels, so its duration includes "
+                                            "that sharing; one_lane is the same kernel with one wave in "
+                                            "flight" if lanes > 1 else ""),
                 "one_lane": one_lane, **work}
 
     # e2e through the public API with host buffers: render + resolve to pinned host memory
