@@ -8,9 +8,10 @@ two passes), and keeps the fastest setting:
   shadow_persistent              persistent warps or one ray per thread for shadow rays
   shadow_order                   nearer or farther child first for shadow (any-hit) rays
   overlap                        shadow rays of a bounce concurrent with the next bounce's closest hits
-  waves                          waves in flight (two stream lanes or one)
-  lane_stagger                   bounces the first lane shades before the second lane starts
-  graph                          captured CUDA graph of a wave's bounce loop, or direct launches
+  waves                          waves in flight (stream lanes, 1-4)
+  lane_stagger                   bounces a lane's first wave shades before the next lane's starts
+  graph                          captured CUDA graphs of the bounce loop, or direct launches
+  guided_form                    guided bounce as a bounce kernel + network pass, or one fused kernel
   refill                         idle lanes that trigger a warp refill
   extend/shadow/shade_blocks_per_sm   blocks per SM in the grids (persistent kernels: at most
                                       those resident at once)
@@ -68,7 +69,7 @@ def load_tuning(workload: str, gpu: str | None = None) -> dict | None:
 
 def measure(renderer, cam, calls: int, spp_per_call: int, first: int) -> float:
     """Device ms per sample over `calls` xb_render calls of `spp_per_call` samples each (after
-    one warm-up call); several waves per call, so two waves in flight are measured as used."""
+    one warm-up call); several waves per call, so waves in flight are measured as used."""
     renderer.render_range(cam, first, spp_per_call)
     ms = 0.0
     for k in range(calls):

@@ -117,7 +117,6 @@ struct xb_renderer {
   cudaStream_t stream2 = nullptr;         // shadow rays, concurrent with the next bounce's hits
   cudaEvent_t ev_shade[kMaxDepth] = {};   // bounce d's shading done (its shadow queues are full)
   cudaEvent_t ev_shadow[kMaxDepth] = {};  // bounce d's shadow rays done (path radiance final)
-  // the second wave lane (two waves in flight): its own queues, streams and per-bounce events
   // wave lanes 1 .. kMaxLanes - 1 (several waves in flight; lane 0 is the fields above): each
   // with its own queues, streams and per-bounce events
   struct ExtraLane {
@@ -1375,7 +1374,7 @@ bool alloc_wave_buffers(WaveBuffers& w, int64_t cap) {
   return ok;
 }
 
-// Queues for `cap` paths per wave, in both lanes when two waves run at once.
+// Queues for `cap` paths per wave, in each of the `waves` lanes.
 int alloc_wave(xb_renderer* r, int64_t cap) {
   free_wave(r);
   bool ok = alloc_wave_buffers(r->wb, cap);
