@@ -7,6 +7,9 @@
     python -m xenon_b200.profile_cases guided_room [W H]    config-4 room, guided bounces with an
                                                             untrained network (no training launches)
     python -m xenon_b200.profile_cases plain_room [W H]     the same renders with plain sampling
+    python -m xenon_b200.profile_cases config2 [W H SPP]    config-2 scene, its tuning, SPP samples
+                                                            (default 640x360, 2): prints the rays
+    python -m xenon_b200.profile_cases config3 [SPP]        config-3 scene at full size, its tuning
 
 Each case prints one line and exits 0; it renders a handful of samples so a capture of one
 launch ends quickly.
@@ -63,8 +66,31 @@ def plain_room(w: int = 320, h: int = 180) -> None:
     guided_room(w, h, guided=False)
 
 
+def config2(w: int = 640, h: int = 360, spp: int = 2) -> None:
+    xb, autotune, scenes = _lib()
+    desc = scenes.icosphere_scene(level=8, width=w, height=h)
+    r = xb.Renderer(w, h, desc.max_bounces, desc.min_bounces)
+    r.upload_scene(xb.HostScene.from_desc(desc))
+    r.set_tuning(**autotune.load_tuning("config2"))
+    r.render_frame(xb.camera(desc.eye, desc.target, desc.fov, w / h), spp)
+    st = r.stats()
+    print("config2", w, h, "spp", spp, "rays_closest", st.rays_closest, "rays_shadow", st.rays_shadow,
+          "ms", st.last_ms)
+
+
+def config3(spp: int = 8) -> None:
+    xb, autotune, scenes = _lib()
+    desc = scenes.instanced_grid()
+    r = xb.Renderer(desc.width, desc.height, desc.max_bounces, desc.min_bounces)
+    r.upload_scene(xb.HostScene.from_desc(desc))
+    r.set_tuning(**autotune.load_tuning("config3"))
+    r.render_frame(xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height), spp)
+    st = r.stats()
+    print("config3 spp", spp, "rays_closest", st.rays_closest, "rays_shadow", st.rays_shadow, "ms", st.last_ms)
+
+
 CASES = {"shadow_d0": shadow_d0, "guide_small": guide_small, "guided_room": guided_room,
-         "plain_room": plain_room}
+         "plain_room": plain_room, "config2": config2, "config3": config3}
 
 if __name__ == "__main__":
     if len(sys.argv) < 2 or sys.argv[1] not in CASES:
