@@ -346,6 +346,9 @@ typedef struct xb_tuning {
   int32_t guided_form;                  /* guided bounces: 1 (default) a plain-form bounce kernel
                                            plus a network pass over the guided vertices; 2 one
                                            fused kernel. Same image either way. */
+  int32_t shade_occupancy;              /* shading kernels compiled to fit 4, 8 (default) or 12
+                                           blocks of 128 threads per SM: fewer registers per
+                                           thread, the rest spilled to L1 (other values: 8) */
 } xb_tuning;
 int  xb_set_tuning(xb_renderer *r, const xb_tuning *t);
 int  xb_get_tuning(const xb_renderer *r, xb_tuning *out);

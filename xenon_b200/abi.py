@@ -154,7 +154,8 @@ class Tuning(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int32) for k in ("extend_persistent_from_depth", "shadow_persistent", "refill",
                                               "extend_blocks_per_sm", "shadow_blocks_per_sm",
                                               "shade_blocks_per_sm", "wave_paths", "shadow_order", "overlap",
-                                              "waves", "lane_stagger", "graph", "guided_form")]
+                                              "waves", "lane_stagger", "graph", "guided_form",
+                                              "shade_occupancy")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

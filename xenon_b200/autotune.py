@@ -12,6 +12,7 @@ two passes), and keeps the fastest setting:
   lane_stagger                   bounces a lane's first wave shades before the next lane's starts
   graph                          captured CUDA graphs of the bounce loop, or direct launches
   guided_form                    guided bounce as a bounce kernel + network pass, or one fused kernel
+  shade_occupancy                blocks per SM the shading kernels are compiled to fit (registers)
   refill                         idle lanes that trigger a warp refill
   extend/shadow/shade_blocks_per_sm   blocks per SM in the grids (persistent kernels: at most
                                       those resident at once)
@@ -39,6 +40,7 @@ SPACE = {
     "lane_stagger": [1, 2, 3],
     "graph": [1, 2],
     "guided_form": [1, 2],
+    "shade_occupancy": [4, 8, 12],
     "refill": [2, 4, 8, 16, 24],
     "extend_blocks_per_sm": [2, 4, 8, 16, 64],
     "shadow_blocks_per_sm": [2, 4, 8, 16, 64],

@@ -164,7 +164,7 @@ struct xb_renderer {
   int refill = 8;                // persistent traversal: refill a warp when this many lanes idle
   int ext_persistent_from = 0;   // bounces >= this trace closest hits with persistent warps
   bool shadow_persistent = true;
-  int occ_ext = 1, occ_pext = 1, occ_shadow = 1, occ_pshadow = 1, occ_shade = 1;  // limits
+  int occ_ext = 1, occ_pext = 1, occ_shadow = 1, occ_pshadow = 1;  // limits
   xb_tuning tune{};
   // profiling
   int prof_flags = 0;
@@ -363,7 +363,11 @@ __device__ __forceinline__ void add_L(float4* L, int p, V3 c) {
   L[p] = l;
 }
 
-__global__ void __launch_bounds__(128) shade_kernel(ShadeArgs a) {
+// kOcc: the blocks of 128 threads the kernel is compiled to fit on one SM (xb_tuning
+// shade_occupancy): 4 keeps every value in registers (108), 8 and 12 cap them at 64 and 40 and
+// spill the rest to L1; the bounce is latency-bound, so more resident warps usually win.
+template <int kOcc>
+__global__ void __launch_bounds__(128, kOcc) shade_kernel(ShadeArgs a) {
   const int n = a.cnt[CNT_RAYS];
   const DevScene& sc = a.sc;
   const bool last_all = (a.depth + 1 >= a.max_bounces);
@@ -559,12 +563,13 @@ constexpr size_t kLobBytes = (size_t)xbg::kTile * kLobStride * 4;
 constexpr size_t kGuidedShadeSmem =
     xbg::kFwdWeightBytes + (kLobBytes > xbg::kTileBytes ? kLobBytes : xbg::kTileBytes) + 1024;
 
-// 128 registers and 55 KB of shared memory: four CTAs (16 warps) per SM. kNet = false is the
+// 128 registers and 55 KB of shared memory: four CTAs (16 warps) per SM (kOcc applies to the
+// network-free form only, as for shade_kernel). kNet = false is the
 // same bounce past the bounces the network serves (xb_guiding.guided_bounces): every vertex
 // samples its BSDF, the importance ratio of the path's earlier guided vertices is carried on, and
 // there is no network, shared memory or barrier, so it launches like the plain bounce.
-template <bool kNet>
-__global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, GuideShadeArgs g) {
+template <bool kNet, int kOcc>
+__global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(ShadeArgs a, GuideShadeArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sW = smem;
   uint8_t* sA = smem + xbg::kFwdWeightBytes;
@@ -849,7 +854,7 @@ __global__ void __launch_bounds__(128, 4) guided_shade_kernel(ShadeArgs a, Guide
 }
 
 // ── guided directions, two-kernel form: the network pass over the deferred vertices ───────
-// Given a guide queue, the bounce kernel (guided_shade_kernel<false>) does all of a bounce but
+// Given a guide queue, the bounce kernel (guided_shade_kernel<false, *>) does all of a bounce but
 // the next direction of the guided vertices, which it queues with their state after next-event
 // estimation and roulette. This persistent kernel runs the network on dense 128-vertex tiles of
 // that queue and samples each direction as the fused kernel does: the same draws from the same
@@ -1411,6 +1416,8 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.lane_stagger = std::min(kMaxDepth, pick(t.lane_stagger, c.lane_stagger, 1));
   c.graph = std::min(2, pick(t.graph, c.graph, 1));
   c.guided_form = std::min(2, pick(t.guided_form, c.guided_form, 1));
+  c.shade_occupancy = pick(t.shade_occupancy, c.shade_occupancy, 8);
+  if (c.shade_occupancy != 4 && c.shade_occupancy != 8 && c.shade_occupancy != 12) c.shade_occupancy = 8;
   drop_graphs(r);
   r->ext_persistent_from = c.extend_persistent_from_depth;
   r->shadow_persistent = c.shadow_persistent == 1;
@@ -1593,18 +1600,23 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
       StageTimer t(r, STAGE_SHADE, L.s);
       const bool net = d < r->gcfg.guided_bounces;
       if (net && r->tune.guided_form == 2) {
-        guided_shade_kernel<true><<<r->grid_gshade, 128, kGuidedShadeSmem, L.s>>>(sa, ga);
+        guided_shade_kernel<true, 4><<<r->grid_gshade, 128, kGuidedShadeSmem, L.s>>>(sa, ga);
       } else {
         if (net) {   // two-kernel form: the guided vertices' directions come from the network pass
           for (int k = 0; k < 5; ++k) ga.gq[k] = w.gq[k];
           ga.gq_rng = w.gq_rng;
           network_pass = true;
         }
-        guided_shade_kernel<false><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
+        if (r->tune.shade_occupancy == 4)
+          guided_shade_kernel<false, 4><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
+        else
+          guided_shade_kernel<false, 8><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
       }
     } else {
       StageTimer t(r, STAGE_SHADE, L.s);
-      shade_kernel<<<r->grid_shade, 128, 0, L.s>>>(sa);
+      if (r->tune.shade_occupancy == 4) shade_kernel<4><<<r->grid_shade, 128, 0, L.s>>>(sa);
+      else if (r->tune.shade_occupancy == 12) shade_kernel<12><<<r->grid_shade, 128, 0, L.s>>>(sa);
+      else shade_kernel<8><<<r->grid_shade, 128, 0, L.s>>>(sa);
     }
     CK(cudaEventRecord(L.ev_shade[d], L.s));
     if (network_pass) {   // beside the shadow rays of this bounce, before the next closest hits
@@ -1942,14 +1954,12 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   r->occ_ext = std::max(occ, 1);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_kernel<false>, 128, 0);
   r->occ_shadow = std::max(occ, 1);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel, 128, 0);
-  r->occ_shade = std::max(occ, 1);
   // guided shade: dynamic shared memory for the weights, one activation tile and the lobes; at
   // most 4 CTAs per SM so their TMEM (64 columns each) always fits the SM's 512 columns
   if (cudaFuncSetAttribute(guide_sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kGuidedShadeSmem) != cudaSuccess)
     return bail(xb::fail(XB_E_CUDA, "guide sample kernel attribute failed"));
-  if (cudaFuncSetAttribute(guided_shade_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(guided_shade_kernel<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kGuidedShadeSmem) != cudaSuccess)
     return bail(xb::fail(XB_E_CUDA, "guided shade kernel attribute failed"));
   {
@@ -1960,7 +1970,7 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, cfg->device);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, cfg->device);
     cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, cfg->device);
-    if (cudaFuncGetAttributes(&fa, guided_shade_kernel<true>) != cudaSuccess)
+    if (cudaFuncGetAttributes(&fa, guided_shade_kernel<true, 4>) != cudaSuccess)
       return bail(xb::fail(XB_E_CUDA, "guided shade kernel attributes failed"));
     const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;
     const int by_regs = regs_sm / std::max(1, warp_regs * 4);
