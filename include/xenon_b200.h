@@ -301,6 +301,33 @@ int  xb_resolve_async(xb_renderer *r, float *out_rgb);
 int  xb_sync(xb_renderer *r);
 /* FP64 per-pixel sums and Welford M2 (needs XB_FLAG_FP64_ACCUM); each double[W*H*3]. */
 int  xb_resolve_fp64(xb_renderer *r, double *sum_rgb, double *m2_rgb);
+
+/* Output stage, on the host over an image as xb_resolve returns it (float[W*H*3], first row the
+ * bottom of the image as in the reference's framebuffer). The reference does this inside its
+ * main() when a render ends (save_image, src/main.cpp:24-52).
+ *   xb_image_to_rgb8: the PNG's 8-bit pixels, top row first: each channel clamped to [0, 1],
+ *     raised to 1/2.2, times 255.99, truncated (src/main.cpp:26-30) — uint8[W*H*3].
+ *   xb_write_png: those pixels as an 8-bit RGB PNG file (uncompressed deflate blocks).
+ *   xb_image_noise_stats: ImageNoiseEstimator::computeResidualNoiseStats
+ *     (src/math/image.h:35-118): luminance minus its 3x3 blur, relative to the blur, over the
+ *     interior pixels whose luminance gradient is below a tenth of the mean luminance. */
+typedef struct xb_noise_stats {
+  float mean_squared_score;   /* mean of residual^2 / (blur^2 + epsilon) */
+  float rms_score;
+  float mean_absolute;        /* mean, median, 95th percentile and maximum of |residual| / */
+  float median_absolute;      /* sqrt(blur^2 + epsilon) */
+  float p95_absolute;
+  float max_absolute;
+  float avg_luminance;
+  float edge_threshold;       /* max(1e-6, avg_luminance / 10) */
+  float epsilon;              /* max(1e-8, 1e-4 avg_luminance^2) */
+  int32_t valid_pixel_count;
+  int32_t total_interior_pixel_count;
+  float valid_pixel_ratio;
+} xb_noise_stats;
+int  xb_image_to_rgb8(const float *rgb, int32_t width, int32_t height, uint8_t *out_rgb8);
+int  xb_write_png(const char *path, const float *rgb, int32_t width, int32_t height);
+int  xb_image_noise_stats(const float *rgb, int32_t width, int32_t height, xb_noise_stats *out);
 int  xb_get_spp(const xb_renderer *r);
 int  xb_reset(xb_renderer *r);
 /* Renders samples [spp_first, spp_first + spp_count) of the sequence (1-based), e.g. one shard

@@ -44,6 +44,8 @@ _SIGS = {
     "xr_renderer_free": ([_P], None),
     "xr_render": ([_P, _P, _P, _I, _I, _P], ctypes.c_double),
     "xr_hardware_threads": ([], _I),
+    "xr_noise_stats": ([_P, _I, _I, _P, _P], None),
+    "xr_image_rgb8": ([_P, _I64, _P], None),
 }
 
 _LIBS: dict[str, ctypes.CDLL] = {}
@@ -194,4 +196,22 @@ def camera(eye, target, fov, aspect) -> np.ndarray:
     out = np.zeros(12, np.float32)
     lib("strict").xr_camera(ptr(np.asarray(eye, np.float32)), ptr(np.asarray(target, np.float32)),
                             float(fov), float(aspect), ptr(out))
+    return out
+
+
+def noise_stats(rgb: np.ndarray):
+    """The reference's ImageNoiseEstimator on an (h, w, 3) float32 image: (10 floats, 2 counts)."""
+    img = np.ascontiguousarray(rgb, np.float32)
+    h, w = img.shape[:2]
+    out = np.zeros(10, np.float32)
+    counts = np.zeros(2, np.int32)
+    lib().xr_noise_stats(ptr(img), w, h, ptr(out), ptr(counts))
+    return out, counts
+
+
+def image_rgb8(rgb: np.ndarray) -> np.ndarray:
+    """save_image's 8-bit values of an (h, w, 3) float32 image (before its vertical flip)."""
+    img = np.ascontiguousarray(rgb, np.float32)
+    out = np.zeros(img.shape, np.uint8)
+    lib().xr_image_rgb8(ptr(img), img.size, ptr(out))
     return out

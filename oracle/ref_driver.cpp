@@ -46,6 +46,7 @@
 #include "render/wavefront.h"
 #include "scene/scene_file.h"
 #include "material/bsdf.h"
+#include "math/image.h"
 #undef private
 
 #include "../include/xenon_b200.h"
@@ -550,5 +551,25 @@ double xr_render(void* rp, void* sp, const float* eye_target_fov, int spp_first,
 }
 
 int xr_hardware_threads() { return (int)std::thread::hardware_concurrency(); }
+
+// The reference's output stage (src/main.cpp:24-52). Noise statistics: its own
+// ImageNoiseEstimator (src/math/image.h:35-118) on an RGB float image; out receives the ten
+// float fields of NoiseStats (meanSquaredScore, rmsScore, meanAbsolute, medianAbsolute,
+// p95Absolute, maxAbsolute, avgLuminance, edgeThreshold, epsilon, validPixelRatio), counts the
+// valid and interior pixel counts.
+void xr_noise_stats(const float* rgb, int w, int h, float* out, int* counts) {
+  const xn::NoiseStats s = xn::ImageNoiseEstimator::computeResidualNoiseStats(rgb, w, h);
+  const float f[10] = {s.meanSquaredScore, s.rmsScore, s.meanAbsolute, s.medianAbsolute, s.p95Absolute,
+                       s.maxAbsolute, s.avgLuminance, s.edgeThreshold, s.epsilon, s.validPixelRatio};
+  for (int i = 0; i < 10; ++i) out[i] = f[i];
+  counts[0] = s.validPixelCount;
+  counts[1] = s.totalInteriorPixelCount;
+}
+
+// save_image's 8-bit values (src/main.cpp:27-30 lives in main(), so it is restated here): each
+// channel clamped to [0, 1], raised to 1/2.2, times 255.99, truncated; n values, no flip.
+void xr_image_rgb8(const float* rgb, int64_t n, uint8_t* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = (uint8_t)(255.99f * std::pow(std::clamp(rgb[i], 0.f, 1.f), 1.f / 2.2f));
+}
 
 }  // extern "C"

@@ -4,7 +4,9 @@
 Run where the reference sources exist (`make -C oracle ref` first): every expected value here
 is computed by the reference itself (oracle/_ref/libxnref_strict.so: its BLAS/TLAS build,
 Scene::intersect / intersects, bsdf_eval_for_nee / bsdf_pdf_for_nee / bsdf_sample,
-Camera::look_at, material_prepare, the .xenon / .mat loaders and render_frame_tiled).
+Camera::look_at, material_prepare, the .xenon / .mat loaders and render_frame_tiled), and for
+the output stage its ImageNoiseEstimator and save_image's 8-bit conversion (output.npz; run
+`python tests/golden/gen_golden.py output` to write that file alone).
 Inputs are this repo's seeded procedural scenes (xenon_b200/scenes.py), so the files are
 reproducible: `python tests/golden/gen_golden.py`.
 """
@@ -150,5 +152,33 @@ def main():
     print("golden vectors written to", HERE)
 
 
+def output_stage():
+    """The output stage: noise statistics and 8-bit values of seeded images, edge cases and the
+    reference's converged 64x64 config-1 render (render.npz)."""
+    rng = np.random.default_rng(11)
+    yy, xx = np.mgrid[0:48, 0:64].astype(np.float32)
+    smooth = np.stack([xx / 64, yy / 48, 0.5 + 0.0 * xx], -1)
+    imgs = {
+        "noisy_gradient": smooth * (1 + 0.2 * rng.normal(size=smooth.shape)),
+        "hdr_edges": np.where((xx[..., None] // 8 + yy[..., None] // 8) % 2 == 0, 3.0, 0.2)
+                     * (1 + 0.05 * rng.normal(size=smooth.shape)) - 0.01,
+        "tiny_3x3": rng.random((3, 3, 3)),
+        "no_interior_2x5": rng.random((2, 5, 3)),
+        "black": np.zeros((9, 7, 3)),
+        "cornell64": np.load(os.path.join(HERE, "render.npz"))["cornell64_mean"],
+    }
+    out = {}
+    for name, img in imgs.items():
+        img = np.ascontiguousarray(img, np.float32)
+        f, c = ref.noise_stats(img)
+        out[f"{name}_image"] = img
+        out[f"{name}_stats"], out[f"{name}_counts"] = f, c
+        out[f"{name}_rgb8"] = ref.image_rgb8(img)
+    np.savez_compressed(os.path.join(HERE, "output.npz"), **out)
+    print("output-stage vectors written to", HERE)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] != ["output"]:
+        main()
+    output_stage()

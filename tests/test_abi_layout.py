@@ -18,6 +18,7 @@ STRUCTS = {
     "RenderStats": "xb_render_stats", "Tuning": "xb_tuning", "Profile": "xb_profile",
     "Guiding": "xb_guiding", "GuidingStats": "xb_guiding_stats", "SceneConfig": "xb_scene_config",
     "View": "xb_view", "CameraDesc": "xb_camera_desc", "MaterialDerived": "xb_material_derived",
+    "NoiseStats": "xb_noise_stats",
 }
 DTYPES = {"PRIM_DTYPE": "xb_prim", "RAY_DTYPE": "xb_ray", "HIT_DTYPE": "xb_hit", "NODE_DTYPE": "xb_bvh_node"}
 

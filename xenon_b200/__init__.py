@@ -275,6 +275,31 @@ class Renderer:
                                                ctypes.c_void_p(stream) if stream else None))
 
 
+def image_to_rgb8(rgb: np.ndarray) -> np.ndarray:
+    """xb_image_to_rgb8: the PNG's 8-bit pixels (top row first) of an image as resolve() returns it."""
+    img = np.ascontiguousarray(rgb, np.float32)
+    h, w = img.shape[:2]
+    out = np.empty((h, w, 3), np.uint8)
+    check(lib().xb_image_to_rgb8(_p(img), w, h, _p(out)))
+    return out
+
+
+def write_png(path: str, rgb: np.ndarray) -> None:
+    """xb_write_png: an image as resolve() returns it, written as the reference's save_image does."""
+    img = np.ascontiguousarray(rgb, np.float32)
+    h, w = img.shape[:2]
+    check(lib().xb_write_png(str(path).encode(), _p(img), w, h))
+
+
+def noise_stats(rgb: np.ndarray) -> dict:
+    """xb_image_noise_stats: the reference's blur-residual noise statistics of an image."""
+    img = np.ascontiguousarray(rgb, np.float32)
+    h, w = img.shape[:2]
+    st = abi.NoiseStats()
+    check(lib().xb_image_noise_stats(_p(img), w, h, ctypes.byref(st)))
+    return st.as_dict()
+
+
 def bsdf_eval(mat: np.ndarray, wo: np.ndarray, wi: np.ndarray):
     """GPU eval/pdf for NEE (bsdf_eval_for_nee / bsdf_pdf_for_nee)."""
     wo = np.ascontiguousarray(wo, np.float32)

@@ -196,6 +196,18 @@ class Guiding(ctypes.Structure):
         return d
 
 
+class NoiseStats(ctypes.Structure):
+    """xb_noise_stats: the reference's blur-residual noise statistics of an image."""
+    _fields_ = [(k, ctypes.c_float) for k in ("mean_squared_score", "rms_score", "mean_absolute",
+                                              "median_absolute", "p95_absolute", "max_absolute",
+                                              "avg_luminance", "edge_threshold", "epsilon")] + \
+               [("valid_pixel_count", ctypes.c_int32), ("total_interior_pixel_count", ctypes.c_int32),
+                ("valid_pixel_ratio", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GuidingStats(ctypes.Structure):
     _fields_ = [("adam_steps", ctypes.c_int64), ("records", ctypes.c_int64), ("records_dropped", ctypes.c_int64),
                 ("last_loss", ctypes.c_float), ("training", ctypes.c_int32)]

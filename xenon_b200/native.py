@@ -64,6 +64,9 @@ SIGNATURES = {
     "xb_render_views": ([_P, _P, _I32], _I),
     "xb_resolve_async": ([_P, _P], _I),
     "xb_sync": ([_P], _I),
+    "xb_image_to_rgb8": ([_P, _I, _I, _P], _I),
+    "xb_write_png": ([ctypes.c_char_p, _P, _I, _I], _I),
+    "xb_image_noise_stats": ([_P, _I, _I, _P], _I),
     "xb_set_guiding": ([_P, _P], _I),
     "xb_get_guiding": ([_P, _P], _I),
     "xb_get_guiding_stats": ([_P, _P], _I),
