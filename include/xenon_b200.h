@@ -253,6 +253,10 @@ typedef struct xb_renderer xb_renderer;
 
 #define XB_FLAG_FP64_ACCUM      1   /* FP64 per-pixel sum + Welford M2 (oracle renders) */
 #define XB_FLAG_THREAD_PER_RAY  2   /* one-ray-per-thread traversal instead of persistent warps */
+#define XB_FLAG_SUN_NEE         4   /* directional lights as delta lights in next-event estimation:
+                                       contribution f cos E / P(pick), MIS weight 1. Off (parity):
+                                       the reference's 1e8 divisor (src/render/cpu_tiled.cpp:166-183),
+                                       with which a sun adds about 1e-8 of its light */
 
 typedef struct xb_config {
   int32_t width, height;

@@ -191,6 +191,31 @@ def test_captured_bounce_loops_render_identically():
 
 
 @pytest.mark.gpu
+def test_sun_nee_flag_lights_a_lambertian_ground():
+    """XB_FLAG_SUN_NEE: a Lambertian ground of albedo a under a sun of irradiance E at angle t
+    and no sky shows a E cos t / pi in every pixel at one bounce; without the flag (the
+    reference's 1e8 divisor) it shows 1e-8 of that."""
+    from xenon_b200 import abi
+    d = scenes.SceneDesc(name="sun", width=32, height=24, spp=1, max_bounces=1)
+    ground = d.add_material("g", abi.material(base_color=(0.5, 0.4, 0.3), roughness=1.0, ior=1.0))
+    d.add_mesh(scenes.quad_mesh((-50, 0, 50), (100, 0, 0), (0, 0, -100), ground))
+    sun = np.array([0.3, 0.8, -0.2])
+    sun /= np.linalg.norm(sun)
+    d.suns.append((tuple(sun), (1.0, 0.9, 0.8), 2.0))
+    d.sky = scenes.sky_array(intensity=0.0)
+    d.eye, d.target, d.fov = (0.0, 10.0, 10.0), (0.0, 0.0, 0.0), 20.0
+    hs = HostScene.from_desc(d)
+    want = np.array([0.5, 0.4, 0.3]) * np.array([1.0, 0.9, 0.8]) * 2.0 * sun[1] / np.pi
+    for flags, scale in ((abi.XB_FLAG_SUN_NEE, 1.0), (0, 1e-8)):
+        r = Renderer(32, 24, 1, 3, flags=flags)
+        r.upload_scene(hs)
+        r.render_frame(camera(d.eye, d.target, d.fov, 32 / 24), 4)
+        img = r.resolve()
+        r.close()
+        assert np.allclose(img.reshape(-1, 3), want * scale, rtol=1e-4, atol=0), (img.reshape(-1, 3)[:3], want * scale)
+
+
+@pytest.mark.gpu
 def test_converged_cornell_matches_cpu_render(ref):
     desc = scenes.cornell(max_bounces=8)
     w = h = 64

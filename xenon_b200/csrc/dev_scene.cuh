@@ -92,7 +92,7 @@ struct DevScene {
   float sky_zenith[3], sky_horizon[3], sky_ground[3];
   float sky_inv_sharpness;
   float sky_intensity;
-  int32_t overflow_pad;
+  int32_t sun_nee;   // XB_FLAG_SUN_NEE: directional lights weighted as delta lights (else the reference's 1e8)
 };
 
 struct Ray {

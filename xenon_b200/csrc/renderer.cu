@@ -476,8 +476,11 @@ __global__ void __launch_bounds__(128, kOcc) shade_kernel(ShadeArgs a) {
               const V3 f = bsdf_eval(wo_l, wi_l, mat);
               const float bp = bsdf_pdf(wo_l, wi_l, mat);
               const float cs = wi_l.z;
-              const float lpdf = 1e8f * dpick;
-              const float mis = mis_power2(lpdf, bp);
+              // cpu_tiled.cpp:166-183 divides by a 1e8 "pdf" (the sun then adds ~1e-8 of its
+              // light); XB_FLAG_SUN_NEE weighs the delta light by its pick probability alone,
+              // with MIS weight 1 (no BSDF sample can hit a direction)
+              const float lpdf = sc.sun_nee ? dpick : 1e8f * dpick;
+              const float mis = sc.sun_nee ? 1.f : mis_power2(lpdf, bp);
               const V3 org = offset_origin(fh.pos, fh.geo_normal, sdir, kShadowEps);
               const V3 em = v3(sun.emission[0], sun.emission[1], sun.emission[2]);
               const V3 c = tp * f * cs * (em / lpdf) * mis;
@@ -735,8 +738,8 @@ __global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(Shad
         if (wi_l.z > 1e-6f) {
           const V3 f = bsdf_eval(wo_l, wi_l, mat);
           const float bp = bsdf_pdf(wo_l, wi_l, mat);
-          const float lpdf = 1e8f * dpick;
-          const float mis = mis_power2(lpdf, bp);
+          const float lpdf = sc.sun_nee ? dpick : 1e8f * dpick;   // as in shade_kernel
+          const float mis = sc.sun_nee ? 1.f : mis_power2(lpdf, bp);
           const V3 org = offset_origin(fh.pos, fh.geo_normal, sdir, kShadowEps);
           const V3 em = v3(sun.emission[0], sun.emission[1], sun.emission[2]);
           const V3 c = (tp * ratio) * f * wi_l.z * (em / lpdf) * mis;
@@ -2216,6 +2219,7 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   std::memcpy(sc.sky_ground, v->sky.ground, sizeof(sc.sky_ground));
   sc.sky_inv_sharpness = 1.0f / v->sky.sharpness;
   sc.sky_intensity = v->sky.intensity;
+  sc.sun_nee = (r->cfg.flags & XB_FLAG_SUN_NEE) != 0;
   r->has_scene = true;
   return XB_OK;
 }
