@@ -161,3 +161,47 @@ def test_scene_generators_are_deterministic():
         digest(scenes.instanced_grid(grid=2, levels=(2, 2, 2, 2)))
     v, f = scenes.icosphere(8)
     assert len(f) == 1310720 and len(v) == 655362
+
+
+def test_xenon_instance_command(tmp_path, monkeypatch):
+    """`instance` (this library's addition to the .xenon format): the loaded scene's TLAS and
+    instances equal those of the same scene built through xb_scene_add_instance."""
+    obj = tmp_path / "tri.obj"
+    obj.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0.5\nf 1 2 3\nf 2 4 3\n")
+    (tmp_path / "s.xenon").write_text(
+        "config 64 48 4\ncamera 0 3 10  0 0 0  45\n"
+        "material m 0.7 0.6 0.5 0.0 0.9\n"
+        "mesh tri.obj\nmesh tri.obj\n"
+        "light 1 0 5 5 5 0.5\n"
+        "instance 0  -2 0 0  1.0  0 30 0\n"
+        "instance 0   2 0 0  0.5  0 -45 10  77\n"
+        "instance 1   0 4 0  1.0  0 0 0\n"
+        "sphere 0 1 0 0.5 m\n"
+        "instance prims  0 0 1  1.0  0 0 0\n"
+        "instance 5  0 0 0  1 0 0 0\n"        # no such mesh: skipped with a warning
+        "instance 0  0 0 0  0 0 0 0\n")       # zero scale: skipped
+    monkeypatch.chdir(tmp_path)                # mesh paths are relative to the working directory
+    loaded = HostScene.load("s.xenon")
+    got = abi.view_arrays(loaded.view())
+
+    d = scenes.SceneDesc()
+    d.add_material("m", abi.material(base_color=(0.7, 0.6, 0.5), roughness=0.9))
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0.5]], np.float32)
+    idx = np.array([[0, 1, 2], [1, 3, 2]], np.int32)
+    for _ in range(2):
+        d.add_mesh(scenes.MeshDesc(pos, idx, None, None, 0))
+    d.lights.append((1, 0, (5.0, 5.0, 5.0), 0.5))
+    p = np.zeros(1, abi.PRIM_DTYPE)
+    p["type"], p["mat_id"], p["p"][0, :4] = abi.XB_PRIM_SPHERE, 0, (0, 1, 0, 0.5)
+    d.prims.append(p)
+    d.instances += [(0, (-2, 0, 0), 1.0, (0, 30, 0), 0), (0, (2, 0, 0), 0.5, (0, -45, 10), 77),
+                    (1, (0, 4, 0), 1.0, (0, 0, 0), 1), (abi.XB_GEOM_PRIMS, (0, 0, 1), 1.0, (0, 0, 0), 2)]
+    want = abi.view_arrays(HostScene.from_desc(d).view())
+
+    assert [(g, i) for g, i, *_ in got["instances"]] == [(0, 0), (0, 77), (1, 1), (-1, 2)]
+    for a, b in zip(got["instances"], want["instances"]):
+        assert a[0] == b[0] and a[1] == b[1]
+        for x, y in zip(a[2:], b[2:]):
+            assert np.array_equal(x, y)
+    assert np.array_equal(got["tlas_nodes"], want["tlas_nodes"])
+    assert np.array_equal(got["tlas_inst"], want["tlas_inst"])

@@ -2,12 +2,14 @@
 //
 //   .mat   key/value material files        (src/material/material.cpp:31-104)
 //   .obj   v / vn / f / usemtl, fan faces   (src/geometry/mesh.cpp:42-150)
-//   .xenon scene description               (src/scene/scene_file.cpp:49-231)
+//   .xenon scene description               (src/scene/scene_file.cpp:49-231), plus one
+//                                           command of this library's: `instance` (below)
 //
 // The parser is the source of truth for the syntax (docs/MAT_FORMAT.md disagrees with it in
 // places: `anisotropic` / `transmissionRoughness` are not keys the reference reads).
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <filesystem>
 #include <fstream>
@@ -229,6 +231,39 @@ bool load_xenon(const std::string& path, HostScene& sc, xb_scene_config* cfg, xb
         k.intensity = inten;
         k.sharpness = sharp;
       }
+    } else if (cmd == "instance") {
+      // Not a reference command (its parser has no instancing; a `mesh` line bakes its transform
+      // into the vertices): `instance <mesh> tx ty tz scale rx ry rz [id]` places the mesh of
+      // the <mesh>-th loaded `mesh` line (0-based), or the analytic primitives (`prims`), with
+      // a mesh line's transform convention (rotations in degrees). Once a file has one, the
+      // TLAS holds exactly the instances listed. The id defaults to the mesh's index (the
+      // number of meshes for `prims`), which keeps `light` entries matching their meshes.
+      std::string what;
+      ss >> what;
+      F3 t(0, 0, 0), rot(0, 0, 0);
+      float scale = 1.f;
+      if (!(ss >> t.x >> t.y >> t.z >> scale >> rot.x >> rot.y >> rot.z) || scale == 0.f) {
+        std::fprintf(stderr, "[xenon_b200] instance: needs tx ty tz scale rx ry rz, scale not 0 (skipped)\n");
+        continue;
+      }
+      HostInstance in;
+      if (what == "prims") {
+        in.geom = XB_GEOM_PRIMS;
+        in.instance_id = (int32_t)sc.meshes.size();
+      } else {
+        char* end = nullptr;
+        const long g = std::strtol(what.c_str(), &end, 10);
+        if (what.empty() || *end != '\0' || g < 0 || g >= (long)sc.meshes.size()) {
+          std::fprintf(stderr, "[xenon_b200] instance: no mesh '%s' (skipped)\n", what.c_str());
+          continue;
+        }
+        in.geom = (int32_t)g;
+        in.instance_id = (int32_t)g;
+      }
+      int32_t id;
+      if (ss >> id) in.instance_id = id;
+      in.l2w = affine_from_trs(t, scale, rot, &in.w2l);
+      sc.explicit_instances.push_back(in);
     } else if (cmd == "sphere" || cmd == "box" || cmd == "disk" || cmd == "quad" || cmd == "plane") {
       xb_prim q{};
       std::string mname;
