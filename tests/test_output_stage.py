@@ -69,3 +69,43 @@ def test_bad_arguments_and_paths_fail_loudly(tmp_path):
         xb.write_png(str(tmp_path / "missing_dir" / "x.png"), img)
     with pytest.raises(xb.XenonError):
         xb.noise_stats(np.zeros((0, 4, 3), np.float32))
+
+
+def test_cpp_face_save_image(tmp_path):
+    """csrc/b200_renderer.h compiles as C++17 against the library, and its save_image writes the
+    same file and statistics as the C entry points (host code only: no renderer is created)."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("needs g++")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    img = GOLD["noisy_gradient_image"]
+    h, w = img.shape[:2]
+    (tmp_path / "img.bin").write_bytes(np.ascontiguousarray(img, np.float32).tobytes())
+    (tmp_path / "t.cpp").write_text(f"""
+#include <cstdio>
+#include <fstream>
+#include <vector>
+#include "b200_renderer.h"
+int main() {{
+  std::vector<float> img({w} * {h} * 3);
+  std::ifstream("img.bin", std::ios::binary).read(reinterpret_cast<char*>(img.data()), img.size() * 4);
+  const xb_noise_stats s = xb::B200Renderer::save_image("cpp.png", img.data(), {w}, {h});
+  std::printf("%a %d\\n", s.mean_squared_score, s.valid_pixel_count);
+  try {{
+    xb::B200Renderer::save_image("no_such_dir/x.png", img.data(), {w}, {h});
+  }} catch (const xb::Error& e) {{
+    std::printf("error %d\\n", e.code);
+  }}
+  return 0;
+}}
+""")
+    lib = os.path.join(root, "xenon_b200", "lib")
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(root, "xenon_b200", "csrc"), "t.cpp", "-o", "t",
+                    "-L", lib, "-lxenon_b200", f"-Wl,-rpath,{lib}"], cwd=tmp_path, check=True)
+    out = subprocess.run(["./t"], cwd=tmp_path, check=True, capture_output=True, text=True).stdout.split()
+    stats = xb.noise_stats(img)
+    assert float.fromhex(out[0]) == float(np.float32(stats["mean_squared_score"])) and int(out[1]) == stats["valid_pixel_count"]
+    assert out[2:] == ["error", str(-5)]                    # XB_E_IO
+    xb.write_png(str(tmp_path / "py.png"), img)
+    assert (tmp_path / "cpp.png").read_bytes() == (tmp_path / "py.png").read_bytes()

@@ -69,6 +69,15 @@ class B200Renderer {
   int height() const { return h_; }
   xb_renderer* handle() { return r_; }
 
+  // The reference's save_image (src/main.cpp:24-52) on a framebuffer as render_frame fills it:
+  // the PNG file, and the noise statistics it prints (host code, no device needed).
+  static xb_noise_stats save_image(const std::string& path, const float* framebuffer, int width, int height) {
+    check(xb_write_png(path.c_str(), framebuffer, width, height));
+    xb_noise_stats s{};
+    check(xb_image_noise_stats(framebuffer, width, height, &s));
+    return s;
+  }
+
  private:
   xb_renderer* r_ = nullptr;
   int w_ = 0, h_ = 0;
