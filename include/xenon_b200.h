@@ -244,6 +244,10 @@ int  xb_scene_set_sky(xb_scene *s, const xb_sky *sky);
 int  xb_scene_add_instance(xb_scene *s, int32_t geom, const float translation[3], float scale,
                            const float rot_deg[3], int32_t instance_id);
 int  xb_scene_build(xb_scene *s);
+/* Threads of the BVH builds (0, the default: the machine's hardware threads; 1: one). Meshes are
+ * built side by side and large subtrees split across threads; the node arrays are the same for
+ * any count (the reference's, which builds on one thread). No reference counterpart. */
+int  xb_scene_set_build_threads(xb_scene *s, int32_t threads);
 int  xb_scene_get_view(const xb_scene *s, xb_scene_view *out);
 int  xb_scene_load(const char *path, xb_scene **out, xb_scene_config *cfg, xb_camera_desc *cam);
 

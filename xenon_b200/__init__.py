@@ -64,7 +64,9 @@ class HostScene:
             pass
 
     @classmethod
-    def from_desc(cls, desc) -> "HostScene":
+    def from_desc(cls, desc, build_threads: int = 0) -> "HostScene":
+        """Builds the scene's BVHs with `build_threads` threads (0: all hardware threads); the
+        arrays are the same for any count."""
         s = cls()
         L = lib()
         for name, m in zip(desc.material_names, desc.materials):
@@ -94,6 +96,7 @@ class HostScene:
         for (geom, t, sc, r, iid) in desc.instances:
             check(L.xb_scene_add_instance(s.h, int(geom), _p(np.asarray(t, np.float32)), float(sc),
                                           _p(np.asarray(r, np.float32)), int(iid)))
+        check(L.xb_scene_set_build_threads(s.h, int(build_threads)))
         check(L.xb_scene_build(s.h))
         return s
 

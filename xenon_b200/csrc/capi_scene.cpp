@@ -181,6 +181,13 @@ int xb_scene_add_instance(xb_scene* s, int32_t geom, const float t[3], float sca
   return (int)s->s.explicit_instances.size() - 1;
 }
 
+int xb_scene_set_build_threads(xb_scene* s, int32_t threads) {
+  SCENE_MUTABLE(s);
+  if (threads < 0) return fail(XB_E_INVALID, "xb_scene_set_build_threads: %d threads", threads);
+  s->s.build_threads = threads;
+  return XB_OK;
+}
+
 int xb_scene_build(xb_scene* s) {
   SCENE_CHECK(s);
   for (const auto& l : s->s.lights)

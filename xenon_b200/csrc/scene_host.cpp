@@ -11,8 +11,12 @@
 #include "scene_host.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <exception>
+#include <future>
+#include <thread>
 
 namespace xb {
 
@@ -187,10 +191,17 @@ struct BuildItem {
 
 // Binned-SAH BVH build in the reference's node allocation order: root 0, then each split
 // allocates its two children as a contiguous pair and recurses left before right.
+//
+// With par_depth > 0, the two subtrees of a split over at least kParallelItems items are built
+// at once (the left one on another thread), each into a node array of its own, down to
+// par_depth levels. They work on disjoint ranges of the items and of `order`, and their node
+// arrays are then placed where the one-thread build allocates them — the subtree roots in the
+// pair, then the left subtree's other nodes, then the right's, child indices shifted — so the
+// arrays are the same whatever the thread count.
 class BvhBuilder {
  public:
-  BvhBuilder(int bins, uint32_t max_leaf, bool leaf_cost)
-      : bins_(bins), max_leaf_(max_leaf), leaf_cost_(leaf_cost) {}
+  BvhBuilder(int bins, uint32_t max_leaf, bool leaf_cost, int par_depth = 0)
+      : bins_(bins), max_leaf_(max_leaf), leaf_cost_(leaf_cost), par_depth_(par_depth) {}
 
   void build(std::vector<BuildItem>& items, std::vector<xb_bvh_node>& nodes,
              std::vector<uint32_t>& order) {
@@ -205,11 +216,27 @@ class BvhBuilder {
   }
 
  private:
+  static constexpr uint32_t kParallelItems = 16384;
   int bins_;
   uint32_t max_leaf_;
   bool leaf_cost_;
+  int par_depth_;
   std::vector<xb_bvh_node>* nodes_ = nullptr;
   std::vector<uint32_t>* order_ = nullptr;
+
+  // The subtree over items [lo, hi) into `local`, its root at local index 0.
+  void build_subtree(std::vector<xb_bvh_node>& local, uint32_t lo, uint32_t hi, std::vector<BuildItem>& it) {
+    nodes_ = &local;
+    local.reserve((size_t)(hi - lo) * 2);
+    local.emplace_back();
+    split(0, lo, hi, it);
+  }
+  // Local node j >= 1 of a subtree goes to base + j - 1; interior nodes' children move along
+  // (a leaf's child is an item offset and stays).
+  static xb_bvh_node placed(xb_bvh_node n, uint32_t base) {
+    if (n.count == 0) n.child = base + n.child - 1;
+    return n;
+  }
 
   void set_box(uint32_t node, const Bounds& b) {
     xb_bvh_node& n = (*nodes_)[node];
@@ -287,6 +314,21 @@ class BvhBuilder {
     nodes_->emplace_back();
     (*nodes_)[node].child = left;
     (*nodes_)[node].count = 0;
+    if (par_depth_ > 0 && count >= kParallelItems) {
+      std::vector<xb_bvh_node> ln, rn;
+      BvhBuilder lb(bins_, max_leaf_, leaf_cost_, par_depth_ - 1), rb(lb);
+      lb.order_ = rb.order_ = order_;
+      auto done = std::async(std::launch::async, [&] { lb.build_subtree(ln, lo, mid, it); });
+      rb.build_subtree(rn, mid, hi, it);
+      done.get();
+      std::vector<xb_bvh_node>& nodes = *nodes_;
+      const uint32_t base_l = (uint32_t)nodes.size(), base_r = base_l + (uint32_t)ln.size() - 1;
+      nodes[left] = placed(ln[0], base_l);
+      nodes[left + 1] = placed(rn[0], base_r);
+      for (size_t j = 1; j < ln.size(); ++j) nodes.push_back(placed(ln[j], base_l));
+      for (size_t j = 1; j < rn.size(); ++j) nodes.push_back(placed(rn[j], base_r));
+      return;
+    }
     split(left, lo, mid, it);
     split(left + 1, mid, hi, it);
   }
@@ -302,8 +344,12 @@ Bounds node_bounds(const xb_bvh_node& n) {
 }  // namespace
 
 void HostScene::build() {
-  // Per-mesh BLAS (BLAS::build, blas.cpp:183-205)
-  for (HostMesh& m : meshes) {
+  // Per-mesh BLAS (BLAS::build, blas.cpp:183-205): meshes on a pool of threads, and the large
+  // subtrees of each mesh on threads of their own (BvhBuilder); the arrays do not depend on it.
+  const int threads = build_threads > 0 ? build_threads : std::max(1, (int)std::thread::hardware_concurrency());
+  int par_depth = 0;
+  while (par_depth < 4 && (2 << par_depth) <= threads) ++par_depth;
+  auto build_mesh = [&](HostMesh& m) {
     std::vector<BuildItem> items(m.num_triangles());
     for (int t = 0; t < m.num_triangles(); ++t) {
       Bounds b;
@@ -312,8 +358,25 @@ void HostScene::build() {
       b.grow(m.vertex(m.indices[3 * t + 2]));
       items[t] = {b, b.center(), (uint32_t)t};
     }
-    BvhBuilder(12, 2, true).build(items, m.nodes, m.prims);
-  }
+    BvhBuilder(12, 2, true, par_depth).build(items, m.nodes, m.prims);
+  };
+  std::atomic<size_t> next{0};
+  std::vector<std::exception_ptr> failed(meshes.size());
+  auto worker = [&] {
+    for (size_t i = next++; i < meshes.size(); i = next++) {
+      try {
+        build_mesh(meshes[i]);
+      } catch (...) {   // rethrown below, on the calling thread
+        failed[i] = std::current_exception();
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int k = 1; k < std::min<int>(threads, (int)meshes.size()); ++k) pool.emplace_back(worker);
+  worker();
+  for (std::thread& t : pool) t.join();
+  for (const std::exception_ptr& e : failed)
+    if (e) std::rethrow_exception(e);
   // PrimBLAS (prim_blas.cpp:114-134)
   prim_nodes.clear();
   prim_indices.clear();

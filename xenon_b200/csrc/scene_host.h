@@ -47,6 +47,7 @@ class HostScene {
   std::vector<xb_bvh_node> tlas_nodes;
   std::vector<uint32_t> tlas_inst;
   bool built = false;
+  int build_threads = 0;   // BVH build threads (0: the machine's hardware threads, 1: one)
 
   HostScene();
   void build();
