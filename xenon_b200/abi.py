@@ -253,7 +253,11 @@ def view_arrays(v: SceneView) -> dict:
         nrm = None
         if mv.nx:
             nrm = np.stack([np.ctypeslib.as_array(getattr(mv, k), (nv,)) for k in ("nx", "ny", "nz")], 1).copy()
-        out["meshes"].append({"nodes": nodes, "prims": prims, "pos": pos, "nrm": nrm})
+        nt = mv.num_triangles
+        idx = np.ctypeslib.as_array(mv.indices, (nt, 3)).copy() if nt else np.zeros((0, 3), np.int32)
+        mat = np.ctypeslib.as_array(mv.mat_ids, (nt,)).copy() if nt else np.zeros(0, np.int32)
+        out["meshes"].append({"nodes": nodes, "prims": prims, "pos": pos, "nrm": nrm, "indices": idx,
+                              "mat_ids": mat})
     n = v.num_tlas_nodes
     out["tlas_nodes"] = np.frombuffer((ctypes.c_char * (n * 32)).from_address(v.tlas_nodes), NODE_DTYPE).copy() if n else np.zeros(0, NODE_DTYPE)
     out["tlas_inst"] = np.ctypeslib.as_array(v.tlas_inst_indices, (v.num_instances,)).copy() if v.num_instances else np.zeros(0, np.uint32)
