@@ -42,7 +42,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Mrays/s; equal-time relMSE, guided vs plain GPU wavefront (1×B200)"
-WORKLOAD = "config2: displaced icosphere L8 (1,310,722 tris incl. ground) 1920x1080, depth 10"
+
+
+def workload(desc, level: int) -> str:
+    """The workload's name with its actual sizes (config 2 at the defaults: level 8,
+    1,310,722 triangles with the ground, 1920x1080, depth 10)."""
+    return (f"config2: displaced icosphere L{level} ({desc.num_triangles:,} tris incl. ground) "
+            f"{desc.width}x{desc.height}, depth {desc.max_bounces}")
 
 
 def parse():
@@ -260,7 +266,7 @@ def reference_line(args) -> dict:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": WORKLOAD, "sample_per_step": f"{w}x{h} px x {spp_per_step} spp (1/64 of the pixels)",
+            "config": {"workload": workload(desc, args.level), "sample_per_step": f"{w}x{h} px x {spp_per_step} spp (1/64 of the pixels)",
                        "rays_per_path": rpp, "msamples_per_s": msps},
             "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "reference",
                              "sample": f"{w}x{h} px x {spp_per_step} spp per step, render_frame_tiled, Release flags, {cores} threads"},
@@ -689,7 +695,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded procedural scene, seed 1)",
-                "config": {"workload": WORKLOAD, "spp_per_step": sps, "paths_per_step": npix * sps,
+                "config": {"workload": workload(desc, args.level), "spp_per_step": sps, "paths_per_step": npix * sps,
                            "rays_per_path": rays_per_path,
                            "msamples_per_s": msamples, "l2": "flushed between timed steps (256 MiB write)",
                            "parallelism": f"sample-sharded x{ws}" if ws > 1 else "1 GPU",
