@@ -248,6 +248,14 @@ int  xb_scene_build(xb_scene *s);
  * built side by side and large subtrees split across threads; the node arrays are the same for
  * any count (the reference's, which builds on one thread). No reference counterpart. */
 int  xb_scene_set_build_threads(xb_scene *s, int32_t threads);
+/* Moves the vertices of mesh `mesh` of a built scene and refits its BLAS: the tree keeps its
+ * topology and every node box is recomputed bottom-up from the new triangles (a leaf from its
+ * triangles in slot order, an interior node from its two children), then the TLAS is rebuilt
+ * over the instances' new world boxes as xb_scene_build builds it. positions: float[3 * nv]
+ * (nv = the mesh's vertex count); normals: the same, or NULL to keep the mesh's. With unchanged
+ * vertices the node boxes equal the build's. Upload the scene again to render it. No reference
+ * counterpart: the reference rebuilds (BLAS::build, src/geometry/blas.cpp:183-205). */
+int  xb_scene_refit_mesh(xb_scene *s, int32_t mesh, const float *positions, const float *normals);
 int  xb_scene_get_view(const xb_scene *s, xb_scene_view *out);
 int  xb_scene_load(const char *path, xb_scene **out, xb_scene_config *cfg, xb_camera_desc *cam);
 

@@ -113,6 +113,19 @@ class HostScene:
         s.camera_desc = cam
         return s
 
+    def refit_mesh(self, mesh: int, positions, normals=None) -> None:
+        """Moves mesh `mesh`'s vertices and refits its BLAS with the topology kept, then
+        rebuilds the TLAS (xb_scene_refit_mesh). positions, normals: (num_vertices, 3)."""
+        pos = np.ascontiguousarray(positions, np.float32)
+        nrm = None if normals is None else np.ascontiguousarray(normals, np.float32)
+        v = self.view()
+        if not 0 <= mesh < v.num_meshes:
+            raise XenonError(abi.XB_E_INVALID, f"refit_mesh: no mesh {mesh}")
+        nv = v.meshes[mesh].num_vertices
+        if pos.shape != (nv, 3) or (nrm is not None and nrm.shape != (nv, 3)):
+            raise XenonError(abi.XB_E_INVALID, f"refit_mesh: mesh {mesh} has {nv} vertices")
+        check(lib().xb_scene_refit_mesh(self.h, int(mesh), _p(pos), _p(nrm)))
+
     def view(self) -> abi.SceneView:
         """The flattened arrays; they belong to this scene, which the view keeps alive."""
         v = abi.SceneView()

@@ -1,5 +1,6 @@
 // capi_scene.cpp — C ABI of the host scene (xb_scene_*, xb_material_*, xb_camera_look_at).
 
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -197,6 +198,23 @@ int xb_scene_build(xb_scene* s) {
     s->s.build();
   } catch (const std::bad_alloc&) {
     return fail(XB_E_OOM, "xb_scene_build: out of host memory");
+  }
+  return XB_OK;
+}
+
+int xb_scene_refit_mesh(xb_scene* s, int32_t mesh, const float* positions, const float* normals) {
+  SCENE_CHECK(s);
+  if (!s->s.built) return fail(XB_E_STATE, "xb_scene_refit_mesh: call xb_scene_build first");
+  if (mesh < 0 || mesh >= (int)s->s.meshes.size() || !positions)
+    return fail(XB_E_INVALID, "xb_scene_refit_mesh: bad mesh %d or null positions", mesh);
+  const int nv = s->s.meshes[mesh].num_vertices();
+  for (int i = 0; i < 3 * nv; ++i)
+    if (!std::isfinite(positions[i]) || (normals && !std::isfinite(normals[i])))
+      return fail(XB_E_INVALID, "xb_scene_refit_mesh: non-finite value at %d", i);
+  try {
+    s->s.refit_mesh(mesh, positions, normals);
+  } catch (const std::bad_alloc&) {
+    return fail(XB_E_OOM, "xb_scene_refit_mesh: out of host memory");
   }
   return XB_OK;
 }

@@ -9,6 +9,7 @@
 // Compiled with -ffp-contract=off.
 
 #include "scene_host.h"
+#include "bvh_refit.h"
 
 #include <algorithm>
 #include <atomic>
@@ -399,26 +400,81 @@ void HostScene::build() {
       instances.push_back({(int32_t)i, id++, Affine::identity(), Affine::identity()});
     if (!prims.empty()) instances.push_back({XB_GEOM_PRIMS, id++, Affine::identity(), Affine::identity()});
   }
-  // TLAS over world AABBs of the 8 transformed root-box corners (tlas.cpp:116-128,
-  // transform.h:78-89, Instance::rebuild_world_aabb tlas.h:51-53).
-  std::vector<BuildItem> items(instances.size());
-  for (size_t i = 0; i < instances.size(); ++i) {
-    const HostInstance& in = instances[i];
-    Bounds local;
+  build_tlas();
+  built = true;
+}
+
+void HostScene::build_tlas() {
+  std::vector<Affine> l2w;
+  std::vector<const xb_bvh_node*> roots;
+  for (const HostInstance& in : instances) {
+    l2w.push_back(in.l2w);
+    const xb_bvh_node* root = nullptr;
     if (in.geom >= 0) {
-      const HostMesh& m = meshes[in.geom];
-      if (!m.nodes.empty()) local = node_bounds(m.nodes[0]);
+      if (!meshes[in.geom].nodes.empty()) root = &meshes[in.geom].nodes[0];
     } else if (!prim_nodes.empty()) {
-      local = node_bounds(prim_nodes[0]);
+      root = &prim_nodes[0];
     }
+    roots.push_back(root);
+  }
+  xb::build_tlas(l2w, roots, tlas_nodes, tlas_inst);
+}
+
+// TLAS over world AABBs of the 8 transformed root-box corners (tlas.cpp:116-128,
+// transform.h:78-89, Instance::rebuild_world_aabb tlas.h:51-53).
+void build_tlas(const std::vector<Affine>& l2w, const std::vector<const xb_bvh_node*>& roots,
+                std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order) {
+  std::vector<BuildItem> items(l2w.size());
+  for (size_t i = 0; i < l2w.size(); ++i) {
+    Bounds local;
+    if (roots[i]) local = node_bounds(*roots[i]);
     Bounds w;
     for (int c = 0; c < 8; ++c)
-      w.grow(in.l2w.point(F3((c & 1) ? local.mx.x : local.mn.x, (c & 2) ? local.mx.y : local.mn.y,
+      w.grow(l2w[i].point(F3((c & 1) ? local.mx.x : local.mn.x, (c & 2) ? local.mx.y : local.mn.y,
                              (c & 4) ? local.mx.z : local.mn.z)));
     items[i] = {w, w.center(), (uint32_t)i};
   }
-  BvhBuilder(8, 1, false).build(items, tlas_nodes, tlas_inst);
-  built = true;
+  BvhBuilder(8, 1, false).build(items, nodes, order);
+}
+
+void refit_blas(const HostMesh& m, std::vector<xb_bvh_node>& nodes) {
+  // a node's children are allocated after it, so children come before parents in reverse order
+  auto vertex = [&](uint32_t slot, int k, float* p) {
+    const int v = m.indices[3 * (size_t)m.prims[slot] + k];
+    p[0] = m.vx[v]; p[1] = m.vy[v]; p[2] = m.vz[v];
+  };
+  for (size_t i = nodes.size(); i-- > 0;) {
+    xb_bvh_node& n = nodes[i];
+    RefitBox b;
+    if (n.count > 0) {
+      b = refit_leaf(n.child, n.count, vertex);
+    } else {
+      const xb_bvh_node& l = nodes[n.child];
+      const xb_bvh_node& r = nodes[n.child + 1];
+      RefitBox lb, rb;
+      for (int k = 0; k < 3; ++k) {
+        lb.mn[k] = l.mn[k]; lb.mx[k] = l.mx[k];
+        rb.mn[k] = r.mn[k]; rb.mx[k] = r.mx[k];
+      }
+      b = refit_interior(lb, rb);
+    }
+    for (int k = 0; k < 3; ++k) { n.mn[k] = b.mn[k]; n.mx[k] = b.mx[k]; }
+  }
+}
+
+void HostScene::refit_mesh(int mesh, const float* positions, const float* normals) {
+  HostMesh& m = meshes[mesh];
+  for (int i = 0; i < m.num_vertices(); ++i) {
+    m.vx[i] = positions[3 * i]; m.vy[i] = positions[3 * i + 1]; m.vz[i] = positions[3 * i + 2];
+  }
+  if (normals) {
+    m.nx.resize(m.num_vertices()); m.ny.resize(m.num_vertices()); m.nz.resize(m.num_vertices());
+    for (int i = 0; i < m.num_vertices(); ++i) {
+      m.nx[i] = normals[3 * i]; m.ny[i] = normals[3 * i + 1]; m.nz[i] = normals[3 * i + 2];
+    }
+  }
+  refit_blas(m, m.nodes);
+  build_tlas();
 }
 
 void HostScene::view(xb_scene_view* v) {

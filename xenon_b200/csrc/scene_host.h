@@ -52,13 +52,24 @@ class HostScene {
   HostScene();
   void build();
   void view(xb_scene_view* out);
+  // Moves the vertices of a built mesh (positions: float[3 * num_vertices]; normals the same,
+  // or null to keep them), refits its BLAS with the topology kept (bvh_refit.h) and rebuilds
+  // the TLAS over the instances' new world boxes.
+  void refit_mesh(int mesh, const float* positions, const float* normals);
 
  private:
+  void build_tlas();
   std::vector<xb_mesh_view> mesh_views_;
   std::vector<xb_instance_view> inst_views_;
 };
 
 Bounds prim_bounds(const xb_prim& p);
+// The TLAS build (8 bins, one instance per leaf) over instances placed by l2w, each over the
+// box of its root node (null: an empty box), as HostScene::build makes it.
+void build_tlas(const std::vector<Affine>& l2w, const std::vector<const xb_bvh_node*>& roots,
+                std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
+// Node boxes of a mesh's BLAS recomputed from its current vertices (bvh_refit.h).
+void refit_blas(const HostMesh& m, std::vector<xb_bvh_node>& nodes);
 Affine affine_from_trs(F3 t, float s, F3 rot_deg, Affine* inverse);
 xb_material_derived prepare_material(const xb_material& m);
 void default_material(xb_material* m);
