@@ -283,6 +283,18 @@ int  xb_create(const xb_config *cfg, xb_renderer **out);
 void xb_destroy(xb_renderer *r);
 int  xb_last_error(const xb_renderer *r, char *buf, size_t len);
 int  xb_upload_scene(xb_renderer *r, const xb_scene_view *view);
+/* Moves the vertices of uploaded mesh `mesh` and refits its BLAS on the device: the triangles
+ * take the new positions, and every node box is recomputed bottom-up by one kernel in which the
+ * second child to reach a node folds both children's boxes (no thread waits for another). The
+ * folds are xb_scene_refit_mesh's, so both give the same node arrays. The TLAS is then rebuilt
+ * on the host over the instances' new world boxes and copied up. positions: host
+ * float[3 * nv] (nv = the mesh's vertex count in the uploaded view); normals: the same, or NULL
+ * to keep the uploaded ones. Meshes that carry area lights are refused (XB_E_UNSUPPORTED: their
+ * emitter geometry is built on the host at upload; refit the host scene and upload again).
+ * Synchronises the render stream; captured bounce graphs are rebuilt on the next render. The
+ * accumulated image is kept: call xb_reset for frames of a moving scene. No reference
+ * counterpart: the reference rebuilds its BLAS on the host (src/geometry/blas.cpp:183-205). */
+int  xb_refit_mesh(xb_renderer *r, int32_t mesh, const float *positions, const float *normals);
 int  xb_set_bounces(xb_renderer *r, int32_t min_bounces, int32_t max_bounces);
 /* Adds spp_to_add samples per pixel; sample k of pixel p is seeded exactly as the CPU backend
  * seeds it (seed_pcg(p + k * 0xdeadbeef), src/render/cpu_tiled.cpp:22-23). With guiding on, the

@@ -166,6 +166,13 @@ class Renderer:
         v = scene.view() if isinstance(scene, HostScene) else scene
         self._check(lib().xb_upload_scene(self.h, ctypes.byref(v)))
 
+    def refit_mesh(self, mesh: int, positions, normals=None) -> None:
+        """Moves an uploaded mesh's vertices and refits its BLAS on the device (xb_refit_mesh);
+        positions, normals: (num_vertices, 3) float32 in host memory."""
+        pos = np.ascontiguousarray(positions, np.float32)
+        nrm = None if normals is None else np.ascontiguousarray(normals, np.float32)
+        self._check(lib().xb_refit_mesh(self.h, int(mesh), _p(pos), _p(nrm)))
+
     def set_bounces(self, min_bounces: int, max_bounces: int) -> None:
         self._check(lib().xb_set_bounces(self.h, min_bounces, max_bounces))
 

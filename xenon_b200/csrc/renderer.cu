@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "../../include/xenon_b200.h"
+#include "bvh_refit.h"
 #include "capi_common.h"
 #include "dev_bsdf.cuh"
 #include "dev_math.cuh"
@@ -184,6 +185,22 @@ struct xb_renderer {
   // generic scratch for trace/bsdf helpers
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
+  // BLAS refit (xb_refit_mesh): where each mesh's nodes and triangles sit in the uploaded arrays,
+  // what the host TLAS rebuild needs (instance transforms, root boxes) and device scratch
+  struct MeshLayout {
+    int64_t node_base = 0, slot_base = 0;
+    int32_t num_nodes = 0, num_tris = 0, num_verts = 0, tri_offset = 0, vtx_offset = 0;
+    bool has_light = false, has_normals = false;
+    xb_bvh_node root{};
+  };
+  std::vector<MeshLayout> mesh_layout;
+  std::vector<int32_t> inst_geom;
+  std::vector<xb::Affine> inst_l2w;
+  xb_bvh_node prim_root{};
+  bool has_prim_root = false;
+  int64_t tlas_cap = 0;         // nodes the device TLAS array holds
+  void* refit_mem = nullptr;
+  size_t refit_bytes = 0;
 };
 
 namespace {
@@ -1885,6 +1902,98 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
   return XB_OK;
 }
 
+// ── BLAS refit (xb_refit_mesh): one mesh's triangles and node boxes, topology kept ──────────
+// The node boxes are folded by bvh_refit.h, the same code the host refit runs, so a device
+// refit and a host refit of the same vertices give the same arrays.
+struct RefitArgs {
+  float4* blas;               // all meshes' nodes, two float4 each (node_lo, node_hi)
+  float4* tris;               // all meshes' triangle slots, three float4 each
+  const int32_t* tri_index;   // global vertex ids per global triangle
+  const float* pos;           // the mesh's new positions, float[3 * num_verts]
+  int32_t* parent;            // per node of the mesh: its parent (-1: root)
+  uint32_t* arrivals;         // per node of the mesh: children whose walk reached it
+  int32_t* status;            // 0 ok; 1 an index out of range; 2 a walk longer than the node count
+  int64_t node_base, slot_base;
+  int32_t num_nodes, num_tris, num_verts, tri_offset, vtx_offset;
+};
+
+// Triangle slot s of the mesh takes its three vertices from the new positions (the .w words,
+// the triangle's indices, stay).
+__global__ void refit_tris_kernel(RefitArgs a) {
+  const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.num_tris) return;
+  float4* T = a.tris + 3 * (a.slot_base + s);
+  const int32_t t = __float_as_int(T[0].w);   // the triangle's index within its mesh
+  if (t < 0 || t >= a.num_tris) { atomicExch(a.status, 1); return; }
+  int32_t v[3];
+  for (int k = 0; k < 3; ++k) {
+    v[k] = a.tri_index[3 * (int64_t)(a.tri_offset + t) + k] - a.vtx_offset;
+    if (v[k] < 0 || v[k] >= a.num_verts) { atomicExch(a.status, 1); return; }
+  }
+  for (int k = 0; k < 3; ++k) {
+    const float* p = a.pos + 3 * (int64_t)v[k];
+    T[k] = make_float4(p[0], p[1], p[2], T[k].w);
+  }
+}
+
+// Each interior node names itself as its two children's parent; every arrival count starts at 0.
+__global__ void refit_parents_kernel(RefitArgs a) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.num_nodes) return;
+  a.arrivals[i] = 0u;
+  const float4 hi = a.blas[2 * (a.node_base + i) + 1];
+  if (__float_as_uint(hi.w) != 0u) return;   // a leaf
+  const int64_t c = (int64_t)__float_as_uint(hi.z) - a.node_base;
+  if (c < 1 || c + 1 >= a.num_nodes) { atomicExch(a.status, 1); return; }
+  a.parent[c] = i;
+  a.parent[c + 1] = i;
+}
+
+// Boxes written during the walk are read and written through L2 (other SMs write them).
+__device__ __forceinline__ xb::RefitBox refit_load_box(const float4* blas, int64_t n) {
+  const float4 lo = __ldcg(blas + 2 * n), hi = __ldcg(blas + 2 * n + 1);
+  xb::RefitBox b;
+  b.mn[0] = lo.x; b.mn[1] = lo.y; b.mn[2] = lo.z;
+  b.mx[0] = lo.w; b.mx[1] = hi.x; b.mx[2] = hi.y;
+  return b;
+}
+__device__ __forceinline__ void refit_store_box(float4* blas, int64_t n, const xb::RefitBox& b, float4 hi) {
+  __stcg(blas + 2 * n, make_float4(b.mn[0], b.mn[1], b.mn[2], b.mx[0]));
+  __stcg(blas + 2 * n + 1, make_float4(b.mx[1], b.mx[2], hi.z, hi.w));
+}
+
+// One thread per leaf: the leaf's box from its triangles, then up the tree. At each interior
+// node the first child to arrive stops and the second, which finds both boxes written, folds
+// them and goes on, so every box is written once and no thread waits for another.
+__global__ void refit_nodes_kernel(RefitArgs a) {
+  int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.num_nodes) return;
+  const float4 hi = a.blas[2 * (a.node_base + i) + 1];
+  const uint32_t count = __float_as_uint(hi.w);
+  if (count == 0u) return;
+  const int64_t first = __float_as_uint(hi.z);
+  if (first < a.slot_base || first + count > a.slot_base + a.num_tris) { atomicExch(a.status, 1); return; }
+  const float4* tris = a.tris;
+  auto vertex = [tris](uint32_t slot, int k, float* p) {
+    const float4 q = tris[3 * (int64_t)slot + k];
+    p[0] = q.x; p[1] = q.y; p[2] = q.z;
+  };
+  refit_store_box(a.blas, a.node_base + i, xb::refit_leaf((uint32_t)first, count, vertex), hi);
+  for (int32_t steps = 0; steps < a.num_nodes; ++steps) {
+    const int32_t p = a.parent[i];
+    if (p < 0) return;
+    __threadfence();                                   // this child's box before its arrival
+    if (atomicAdd(a.arrivals + p, 1u) != 1u) return;   // first arrival (or a malformed third)
+    __threadfence();
+    const float4 ph = a.blas[2 * (a.node_base + p) + 1];
+    const int64_t c = __float_as_uint(ph.z);
+    refit_store_box(a.blas, a.node_base + p,
+                    xb::refit_interior(refit_load_box(a.blas, c), refit_load_box(a.blas, c + 1)), ph);
+    i = p;
+  }
+  atomicExch(a.status, 2);
+}
+
 }  // namespace
 
 extern "C" {
@@ -2017,7 +2126,7 @@ void xb_destroy(xb_renderer* r) {
   if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
   if (r->host_ov) cudaFreeHost(r->host_ov);
   void* ptrs[] = {r->accum, r->sum64, r->m2_64, r->mean64, r->resolve_buf, r->stats, r->scratch,
-                  r->resolve_async_buf[0], r->resolve_async_buf[1]};
+                  r->resolve_async_buf[0], r->resolve_async_buf[1], r->refit_mem};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (cudaEvent_t e : r->ev_pool) cudaEventDestroy(e);
   if (r->ev0) cudaEventDestroy(r->ev0);
@@ -2069,6 +2178,7 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   std::vector<int32_t> tri_index, tri_mat, root_of(v->num_meshes, -1);
   std::vector<float> nx, ny, nz;
   std::vector<DevMesh> meshes(v->num_meshes);
+  r->mesh_layout.assign(v->num_meshes, xb_renderer::MeshLayout());
   int64_t slot_base = 0, tri_base = 0, vtx_base = 0;
   for (int m = 0; m < v->num_meshes; ++m) {
     const xb_mesh_view& mv = v->meshes[m];
@@ -2077,6 +2187,16 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
     if ((blas.size() / 2) % 2 == 0) { blas.push_back(make_float4(0, 0, 0, 0)); blas.push_back(make_float4(0, 0, 0, 0)); }
     const int64_t node_base = (int64_t)blas.size() / 2;
     if (mv.num_blas_nodes > 0) root_of[m] = (int32_t)node_base;
+    xb_renderer::MeshLayout& ml = r->mesh_layout[m];
+    ml.node_base = node_base;
+    ml.slot_base = slot_base;
+    ml.num_nodes = mv.num_blas_nodes > 0 ? mv.num_blas_nodes : 0;
+    ml.num_tris = mv.num_triangles;
+    ml.num_verts = mv.num_vertices;
+    ml.tri_offset = (int32_t)tri_base;
+    ml.vtx_offset = (int32_t)vtx_base;
+    ml.has_normals = mv.nx != nullptr;
+    if (ml.num_nodes > 0) ml.root = mv.blas_nodes[0];
     for (int i = 0; i < mv.num_blas_nodes; ++i) {
       const xb_bvh_node& nd = mv.blas_nodes[i];
       uint32_t child;
@@ -2147,8 +2267,15 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   }
   std::vector<uint32_t> tinst(v->tlas_inst_indices, v->tlas_inst_indices + v->num_instances);
   std::vector<DevInstance> insts(v->num_instances);
+  r->inst_geom.assign(v->num_instances, 0);
+  r->inst_l2w.assign(v->num_instances, xb::Affine());
+  r->has_prim_root = v->num_prim_nodes > 0;
+  if (r->has_prim_root) r->prim_root = v->prim_nodes[0];
   for (int i = 0; i < v->num_instances; ++i) {
     const xb_instance_view& iv = v->instances[i];
+    r->inst_geom[i] = iv.geom;
+    for (int c = 0; c < 4; ++c)
+      r->inst_l2w[i].c[c] = xb::F3(iv.local_to_world[3 * c], iv.local_to_world[3 * c + 1], iv.local_to_world[3 * c + 2]);
     DevInstance& d = insts[i];
     std::memcpy(d.w2l, iv.world_to_local, sizeof(d.w2l));
     d.instance_id = iv.instance_id;
@@ -2167,6 +2294,7 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   std::vector<DevLight> lights;
   for (int i = 0; i < v->num_lights; ++i) {
     const xb_light& l = v->lights[i];
+    if (l.mesh_id < (uint32_t)v->num_meshes) r->mesh_layout[l.mesh_id].has_light = true;
     xb::LightGeom g;
     if (!xb::light_geometry(*v, l, &g)) return set_err(r, XB_E_INVALID, "light %d refers to a missing triangle", i);
     DevLight d;
@@ -2213,6 +2341,7 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   sc.num_lights = v->num_lights;
   sc.num_suns = v->num_suns;
   sc.num_tlas_nodes = v->num_tlas_nodes;
+  r->tlas_cap = v->num_tlas_nodes;
   sc.num_materials = v->num_materials;
   std::memcpy(sc.sky_zenith, v->sky.zenith, sizeof(sc.sky_zenith));
   std::memcpy(sc.sky_horizon, v->sky.horizon, sizeof(sc.sky_horizon));
@@ -2221,6 +2350,124 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   sc.sky_intensity = v->sky.intensity;
   sc.sun_nee = (r->cfg.flags & XB_FLAG_SUN_NEE) != 0;
   r->has_scene = true;
+  return XB_OK;
+}
+
+int xb_refit_mesh(xb_renderer* r, int32_t mesh, const float* positions, const float* normals) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!r->has_scene) return set_err(r, XB_E_STATE, "xb_refit_mesh: no scene uploaded");
+  if (mesh < 0 || mesh >= (int)r->mesh_layout.size() || !positions)
+    return set_err(r, XB_E_INVALID, "xb_refit_mesh: bad mesh %d or null positions", mesh);
+  xb_renderer::MeshLayout& ml = r->mesh_layout[mesh];
+  if (ml.has_light)
+    return set_err(r, XB_E_UNSUPPORTED, "xb_refit_mesh: mesh %d carries area lights (refit the host scene "
+                   "with xb_scene_refit_mesh and upload it again)", mesh);
+  if (normals && !ml.has_normals)
+    return set_err(r, XB_E_INVALID, "xb_refit_mesh: mesh %d was uploaded without normals", mesh);
+  const int64_t nv = ml.num_verts;
+  for (int64_t i = 0; i < 3 * nv; ++i)
+    if (!std::isfinite(positions[i]) || (normals && !std::isfinite(normals[i])))
+      return set_err(r, XB_E_INVALID, "xb_refit_mesh: non-finite value at %lld", (long long)i);
+  if (ml.num_nodes == 0 || ml.num_tris == 0) return XB_OK;
+  sync_lanes(r);                          // no wave may read the scene while it changes
+  CK(cudaStreamSynchronize(r->stream));
+  // scratch: positions, normals, parents, arrival counts, status (256-byte aligned pieces)
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t b_pos = up(12 * (size_t)nv), b_nodes = up(4 * (size_t)ml.num_nodes);
+  const size_t need = b_pos * (normals ? 2 : 1) + 2 * b_nodes + 256;
+  if (need > r->refit_bytes) {
+    if (r->refit_mem) CK(cudaFree(r->refit_mem));
+    r->refit_mem = nullptr;
+    r->refit_bytes = 0;
+    CK(cudaMalloc(&r->refit_mem, need));
+    r->refit_bytes = need;
+  }
+  char* base = static_cast<char*>(r->refit_mem);
+  RefitArgs a;
+  a.blas = const_cast<float4*>(r->scene.blas);
+  a.tris = const_cast<float4*>(r->scene.tris);
+  a.tri_index = r->scene.tri_index;
+  float* pos_dev = reinterpret_cast<float*>(base);
+  a.pos = pos_dev;
+  float* nrm = normals ? reinterpret_cast<float*>(base + b_pos) : nullptr;
+  char* rest = base + b_pos * (normals ? 2 : 1);
+  a.parent = reinterpret_cast<int32_t*>(rest);
+  a.arrivals = reinterpret_cast<uint32_t*>(rest + b_nodes);
+  a.status = reinterpret_cast<int32_t*>(rest + 2 * b_nodes);
+  a.node_base = ml.node_base;
+  a.slot_base = ml.slot_base;
+  a.num_nodes = ml.num_nodes;
+  a.num_tris = ml.num_tris;
+  a.num_verts = ml.num_verts;
+  a.tri_offset = ml.tri_offset;
+  a.vtx_offset = ml.vtx_offset;
+  cudaStream_t s = r->stream;
+  CK(cudaMemcpyAsync(pos_dev, positions, 12 * (size_t)nv, cudaMemcpyHostToDevice, s));
+  if (normals) {
+    // the device keeps normals as three arrays over all vertices: one copy per component
+    CK(cudaMemcpyAsync(nrm, normals, 12 * (size_t)nv, cudaMemcpyHostToDevice, s));
+    float* dst[3] = {const_cast<float*>(r->scene.nx), const_cast<float*>(r->scene.ny),
+                     const_cast<float*>(r->scene.nz)};
+    for (int k = 0; k < 3; ++k)
+      CK(cudaMemcpy2DAsync(dst[k] + ml.vtx_offset, sizeof(float), nrm + k, 3 * sizeof(float), sizeof(float),
+                           (size_t)nv, cudaMemcpyDeviceToDevice, s));
+  }
+  CK(cudaMemsetAsync(a.parent, 0xff, 4 * (size_t)ml.num_nodes, s));
+  CK(cudaMemsetAsync(a.status, 0, sizeof(int32_t), s));
+  refit_tris_kernel<<<(ml.num_tris + 255) / 256, 256, 0, s>>>(a);
+  refit_parents_kernel<<<(ml.num_nodes + 255) / 256, 256, 0, s>>>(a);
+  refit_nodes_kernel<<<(ml.num_nodes + 255) / 256, 256, 0, s>>>(a);
+  CK(cudaGetLastError());
+  int32_t status = 0;
+  float4 root[2];
+  CK(cudaMemcpyAsync(&status, a.status, sizeof(status), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(root, a.blas + 2 * ml.node_base, sizeof(root), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  drop_graphs(r);
+  if (status != 0)
+    return set_err(r, XB_E_INVALID, "xb_refit_mesh: mesh %d's BLAS is malformed (%s)", mesh,
+                   status == 1 ? "an index out of range" : "a cycle");
+  ml.root.mn[0] = root[0].x; ml.root.mn[1] = root[0].y; ml.root.mn[2] = root[0].z;
+  ml.root.mx[0] = root[0].w; ml.root.mx[1] = root[1].x; ml.root.mx[2] = root[1].y;
+  // the TLAS over the instances' new world boxes, built on the host as xb_scene_build builds it
+  std::vector<const xb_bvh_node*> roots(r->inst_geom.size(), nullptr);
+  for (size_t i = 0; i < roots.size(); ++i) {
+    const int32_t g = r->inst_geom[i];
+    if (g >= 0 && g < (int32_t)r->mesh_layout.size() && r->mesh_layout[g].num_nodes > 0) roots[i] = &r->mesh_layout[g].root;
+    else if (g == XB_GEOM_PRIMS && r->has_prim_root) roots[i] = &r->prim_root;
+  }
+  std::vector<xb_bvh_node> nodes;
+  std::vector<uint32_t> order;
+  try {
+    xb::build_tlas(r->inst_l2w, roots, nodes, order);
+  } catch (const std::bad_alloc&) {
+    return set_err(r, XB_E_OOM, "xb_refit_mesh: out of host memory");
+  }
+  std::vector<float4> tlas;
+  for (const xb_bvh_node& n : nodes) {
+    tlas.push_back(node_lo(n));
+    tlas.push_back(node_hi(n, n.child));
+  }
+  DevScene& sc = r->scene;
+  if ((int64_t)nodes.size() > r->tlas_cap) {
+    const float4* fresh;
+    if ((rc = dev_upload(r, tlas, &fresh))) return rc;
+    sc.tlas = fresh;
+    r->tlas_cap = (int64_t)nodes.size();
+  } else if (!tlas.empty()) {
+    CK(cudaMemcpy(const_cast<float4*>(sc.tlas), tlas.data(), tlas.size() * sizeof(float4), cudaMemcpyHostToDevice));
+  }
+  if (!order.empty())
+    CK(cudaMemcpy(const_cast<uint32_t*>(sc.tlas_inst), order.data(), order.size() * sizeof(uint32_t),
+                  cudaMemcpyHostToDevice));
+  sc.num_tlas_nodes = (int32_t)nodes.size();
+  if (!nodes.empty()) {
+    for (int k = 0; k < 3; ++k) {
+      r->scene_lo[k] = nodes[0].mn[k];
+      r->scene_hi[k] = nodes[0].mx[k];
+    }
+  }
   return XB_OK;
 }
 

@@ -42,6 +42,7 @@ SIGNATURES = {
     "xb_destroy": ([_P], None),
     "xb_last_error": ([_P, ctypes.c_char_p, ctypes.c_size_t], _I),
     "xb_upload_scene": ([_P, _P], _I),
+    "xb_refit_mesh": ([_P, _I, _P, _P], _I),
     "xb_set_bounces": ([_P, _I32, _I32], _I),
     "xb_render": ([_P, _P, _I32], _I),
     "xb_render_range": ([_P, _P, _I32, _I32], _I),
