@@ -116,3 +116,18 @@ def test_refit_errors():
     with pytest.raises(xb.XenonError) as e:
         s.refit_mesh(0, bad)
     assert e.value.code == abi.XB_E_INVALID
+
+
+def test_refit_signed_zero_ties_differ_only_in_sign():
+    """Where a box coordinate's extreme is reached by both +0 and -0, an interior node's refit
+    box can keep the other zero than the build's (bvh_refit.h): equal values, leaves identical."""
+    from tests.test_bvh_levels import _signed_zero_mesh
+    d = _signed_zero_mesh()
+    built = abi.view_arrays(HostScene.from_desc(d).view())["meshes"][0]["nodes"]
+    s = HostScene.from_desc(d)
+    s.refit_mesh(0, d.meshes[0].positions)
+    refit = abi.view_arrays(s.view())["meshes"][0]["nodes"]
+    assert np.array_equal(_boxes(refit), _boxes(built))
+    leaves = built["count"] > 0
+    assert refit[leaves].tobytes() == built[leaves].tobytes()
+    assert np.array_equal(refit["child"], built["child"]) and np.array_equal(refit["count"], built["count"])

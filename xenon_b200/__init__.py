@@ -64,9 +64,10 @@ class HostScene:
             pass
 
     @classmethod
-    def from_desc(cls, desc, build_threads: int = 0) -> "HostScene":
-        """Builds the scene's BVHs with `build_threads` threads (0: all hardware threads); the
-        arrays are the same for any count."""
+    def from_desc(cls, desc, build_threads: int = 0, build_mode: int = abi.XB_BUILD_RECURSIVE) -> "HostScene":
+        """Builds the scene's BVHs with `build_threads` threads (0: all hardware threads), in the
+        recursive or the level-synchronous form (build_mode); the arrays are the same for any
+        count and either form."""
         s = cls()
         L = lib()
         for name, m in zip(desc.material_names, desc.materials):
@@ -97,6 +98,7 @@ class HostScene:
             check(L.xb_scene_add_instance(s.h, int(geom), _p(np.asarray(t, np.float32)), float(sc),
                                           _p(np.asarray(r, np.float32)), int(iid)))
         check(L.xb_scene_set_build_threads(s.h, int(build_threads)))
+        check(L.xb_scene_set_build_mode(s.h, int(build_mode)))
         check(L.xb_scene_build(s.h))
         return s
 

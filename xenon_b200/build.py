@@ -19,7 +19,7 @@ BUILDDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libxenon_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-CXX_SRCS = ["scene_host.cpp", "loaders.cpp", "capi_scene.cpp", "image_out.cpp"]
+CXX_SRCS = ["scene_host.cpp", "bvh_levels.cpp", "loaders.cpp", "capi_scene.cpp", "image_out.cpp"]
 CU_STRICT = ["renderer.cu"]
 CU_FAST = ["guide.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -189,6 +189,14 @@ int xb_scene_set_build_threads(xb_scene* s, int32_t threads) {
   return XB_OK;
 }
 
+int xb_scene_set_build_mode(xb_scene* s, int32_t mode) {
+  SCENE_MUTABLE(s);
+  if (mode != XB_BUILD_RECURSIVE && mode != XB_BUILD_LEVELS)
+    return fail(XB_E_INVALID, "xb_scene_set_build_mode: unknown mode %d", mode);
+  s->s.build_mode = mode;
+  return XB_OK;
+}
+
 int xb_scene_build(xb_scene* s) {
   SCENE_CHECK(s);
   for (const auto& l : s->s.lights)

@@ -9,6 +9,7 @@
 // Compiled with -ffp-contract=off.
 
 #include "scene_host.h"
+#include "bvh_build.h"
 #include "bvh_refit.h"
 
 #include <algorithm>
@@ -182,13 +183,36 @@ Bounds prim_bounds(const xb_prim& q) {
   return b;
 }
 
-namespace {
+// The SAH sweep over the bins of a split (src/geometry/blas.cpp:128-146): prefix and suffix
+// counts and areas, cost (A_l N_l + A_r N_r) / A_node per plane, the first minimum.
+int sah_best_split(const Bounds* bin_box, const int* bin_cnt, int bins, const Bounds& node_box,
+                   float* best_cost) {
+  float l_area[16], r_area[16];
+  int l_cnt[16], r_cnt[16];
+  Bounds acc;
+  int run = 0;
+  for (int i = 0; i < bins - 1; ++i) {
+    run += bin_cnt[i]; l_cnt[i] = run;
+    acc.grow(bin_box[i]); l_area[i] = acc.area();
+  }
+  acc = Bounds();
+  run = 0;
+  for (int i = bins - 1; i > 0; --i) {
+    run += bin_cnt[i]; r_cnt[i - 1] = run;
+    acc.grow(bin_box[i]); r_area[i - 1] = acc.area();
+  }
+  const float parent = node_box.area();
+  float best = kInf;
+  int best_bin = -1;
+  for (int i = 0; i < bins - 1; ++i) {
+    const float c = (l_area[i] * l_cnt[i] + r_area[i] * r_cnt[i]) / parent;
+    if (c < best) { best = c; best_bin = i; }
+  }
+  *best_cost = best;
+  return best_bin;
+}
 
-struct BuildItem {
-  Bounds box;
-  F3 centroid;
-  uint32_t index;
-};
+namespace {
 
 // Binned-SAH BVH build in the reference's node allocation order: root 0, then each split
 // allocates its two children as a contiguous pair and recurses left before right.
@@ -276,27 +300,8 @@ class BvhBuilder {
       bin_cnt[b]++;
       bin_box[b].grow(it[i].box);
     }
-    float l_area[16], r_area[16];
-    int l_cnt[16], r_cnt[16];
-    Bounds acc;
-    int run = 0;
-    for (int i = 0; i < bins_ - 1; ++i) {
-      run += bin_cnt[i]; l_cnt[i] = run;
-      acc.grow(bin_box[i]); l_area[i] = acc.area();
-    }
-    acc = Bounds();
-    run = 0;
-    for (int i = bins_ - 1; i > 0; --i) {
-      run += bin_cnt[i]; r_cnt[i - 1] = run;
-      acc.grow(bin_box[i]); r_area[i - 1] = acc.area();
-    }
-    const float parent = nb.area();
-    float best = kInf;
-    int best_bin = -1;
-    for (int i = 0; i < bins_ - 1; ++i) {
-      const float c = (l_area[i] * l_cnt[i] + r_area[i] * r_cnt[i]) / parent;
-      if (c < best) { best = c; best_bin = i; }
-    }
+    float best;
+    const int best_bin = sah_best_split(bin_box, bin_cnt, bins_, nb, &best);
     if ((leaf_cost_ && best >= (float)count) || best_bin < 0) { leaf(node, lo, hi, it); return; }
 
     auto mid_it = std::partition(it.begin() + lo, it.begin() + hi, [&](const BuildItem& p) {
@@ -359,7 +364,8 @@ void HostScene::build() {
       b.grow(m.vertex(m.indices[3 * t + 2]));
       items[t] = {b, b.center(), (uint32_t)t};
     }
-    BvhBuilder(12, 2, true, par_depth).build(items, m.nodes, m.prims);
+    if (build_mode == 1) build_bvh_levels(items, 12, 2, true, m.nodes, m.prims);
+    else BvhBuilder(12, 2, true, par_depth).build(items, m.nodes, m.prims);
   };
   std::atomic<size_t> next{0};
   std::vector<std::exception_ptr> failed(meshes.size());
@@ -387,7 +393,8 @@ void HostScene::build() {
       Bounds b = prim_bounds(prims[i]);
       items[i] = {b, b.center(), (uint32_t)i};
     }
-    BvhBuilder(12, 2, true).build(items, prim_nodes, prim_indices);
+    if (build_mode == 1) build_bvh_levels(items, 12, 2, true, prim_nodes, prim_indices);
+    else BvhBuilder(12, 2, true).build(items, prim_nodes, prim_indices);
   }
   // Instances: explicit ones, or one identity instance per mesh + one for the prim group
   // (Scene::build_acceleration, scene.h:79-121).
@@ -417,13 +424,13 @@ void HostScene::build_tlas() {
     }
     roots.push_back(root);
   }
-  xb::build_tlas(l2w, roots, tlas_nodes, tlas_inst);
+  xb::build_tlas(l2w, roots, tlas_nodes, tlas_inst, build_mode);
 }
 
 // TLAS over world AABBs of the 8 transformed root-box corners (tlas.cpp:116-128,
 // transform.h:78-89, Instance::rebuild_world_aabb tlas.h:51-53).
 void build_tlas(const std::vector<Affine>& l2w, const std::vector<const xb_bvh_node*>& roots,
-                std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order) {
+                std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order, int mode) {
   std::vector<BuildItem> items(l2w.size());
   for (size_t i = 0; i < l2w.size(); ++i) {
     Bounds local;
@@ -434,7 +441,8 @@ void build_tlas(const std::vector<Affine>& l2w, const std::vector<const xb_bvh_n
                              (c & 4) ? local.mx.z : local.mn.z)));
     items[i] = {w, w.center(), (uint32_t)i};
   }
-  BvhBuilder(8, 1, false).build(items, nodes, order);
+  if (mode == 1) build_bvh_levels(items, 8, 1, false, nodes, order);
+  else BvhBuilder(8, 1, false).build(items, nodes, order);
 }
 
 void refit_blas(const HostMesh& m, std::vector<xb_bvh_node>& nodes) {

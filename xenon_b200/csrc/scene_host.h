@@ -48,6 +48,7 @@ class HostScene {
   std::vector<uint32_t> tlas_inst;
   bool built = false;
   int build_threads = 0;   // BVH build threads (0: the machine's hardware threads, 1: one)
+  int build_mode = 0;      // 0: recursive build, 1: level-synchronous build (same arrays)
 
   HostScene();
   void build();
@@ -67,7 +68,7 @@ Bounds prim_bounds(const xb_prim& p);
 // The TLAS build (8 bins, one instance per leaf) over instances placed by l2w, each over the
 // box of its root node (null: an empty box), as HostScene::build makes it.
 void build_tlas(const std::vector<Affine>& l2w, const std::vector<const xb_bvh_node*>& roots,
-                std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
+                std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order, int mode = 0);
 // Node boxes of a mesh's BLAS recomputed from its current vertices (bvh_refit.h).
 void refit_blas(const HostMesh& m, std::vector<xb_bvh_node>& nodes);
 Affine affine_from_trs(F3 t, float s, F3 rot_deg, Affine* inverse);

@@ -35,6 +35,7 @@ SIGNATURES = {
     "xb_scene_add_instance": ([_P, _I32, _P, _F, _P, _I32], _I),
     "xb_scene_build": ([_P], _I),
     "xb_scene_set_build_threads": ([_P, _I], _I),
+    "xb_scene_set_build_mode": ([_P, _I], _I),
     "xb_scene_refit_mesh": ([_P, _I, _P, _P], _I),
     "xb_scene_get_view": ([_P, _P], _I),
     "xb_scene_load": ([ctypes.c_char_p, ctypes.POINTER(_P), _P, _P], _I),
