@@ -30,6 +30,8 @@ int sah_best_split(const Bounds* bin_box, const int* bin_cnt, int bins, const Bo
 // bins: SAH bins per split (12 for a BLAS or the PrimBLAS, 8 for the TLAS); max_leaf: largest
 // leaf; leaf_cost: make a leaf when the best split costs no less than the node's count. Items are
 // reordered in place; order receives each leaf slot's item index.
+struct LevelItem;
+std::vector<LevelItem> to_level_items(const std::vector<BuildItem>& items);
 void build_bvh_levels(std::vector<BuildItem>& items, int bins, uint32_t max_leaf, bool leaf_cost,
                       std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
 
