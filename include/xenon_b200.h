@@ -248,13 +248,17 @@ int  xb_scene_build(xb_scene *s);
  * built side by side and large subtrees split across threads; the node arrays are the same for
  * any count (the reference's, which builds on one thread). No reference counterpart. */
 int  xb_scene_set_build_threads(xb_scene *s, int32_t threads);
-/* The form of the binned-SAH builds; both give the same node and order arrays.
+/* The form of the binned-SAH builds; all give the same node and order arrays.
  *   XB_BUILD_RECURSIVE (default): depth first, one node at a time, as the reference builds.
- *   XB_BUILD_LEVELS: level-synchronous. Every node of a depth is split in one pass, each step an
- *     ordered reduction, a prefix sum or a per-node scan: the form a device build takes.
+ *   XB_BUILD_LEVELS: level-synchronous on the host. Every node of a depth is split in one pass,
+ *     each step an ordered reduction, a prefix sum or a per-node scan.
+ *   XB_BUILD_DEVICE: the level-synchronous form run by the current CUDA device; one pass of
+ *     kernels per depth, the host reading each depth's outcome. xb_scene_build returns
+ *     XB_E_CUDA when there is no device.
  * No reference counterpart. */
 #define XB_BUILD_RECURSIVE 0
 #define XB_BUILD_LEVELS    1
+#define XB_BUILD_DEVICE    2
 int  xb_scene_set_build_mode(xb_scene *s, int32_t mode);
 /* Moves the vertices of mesh `mesh` of a built scene and refits its BLAS: the tree keeps its
  * topology and every node box is recomputed bottom-up from the new triangles (a leaf from its

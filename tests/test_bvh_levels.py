@@ -84,3 +84,14 @@ def test_bad_build_mode():
     import xenon_b200 as xb
     s = HostScene()
     assert xb.lib().xb_scene_set_build_mode(s.h, 7) == abi.XB_E_INVALID
+
+
+def test_device_build_fails_loudly_without_a_device():
+    """XB_BUILD_DEVICE has no host fallback: with no usable CUDA device the build is an error."""
+    import torch
+    import xenon_b200 as xb
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(xb.XenonError) as e:
+        HostScene.from_desc(scenes.cornell(), build_mode=abi.XB_BUILD_DEVICE)
+    assert e.value.code == abi.XB_E_CUDA and "device BVH build" in str(e.value)

@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "XB_OK", -1: "XB_E_INVALID", -2: "XB_E_CUDA", -3: "XB_E_OOM",
 
 XB_PRIM_SPHERE, XB_PRIM_PLANE, XB_PRIM_BOX, XB_PRIM_DISK, XB_PRIM_QUAD = range(5)
 XB_GEOM_PRIMS = -1
-XB_BUILD_RECURSIVE, XB_BUILD_LEVELS = 0, 1
+XB_BUILD_RECURSIVE, XB_BUILD_LEVELS, XB_BUILD_DEVICE = 0, 1, 2
 XB_TRACE_CLOSEST, XB_TRACE_ANY = 0, 1
 XB_FLAG_FP64_ACCUM = 1
 XB_FLAG_THREAD_PER_RAY = 2

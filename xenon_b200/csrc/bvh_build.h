@@ -1,17 +1,18 @@
 // bvh_build.h — the binned-SAH builds of the host scene (internal to the library).
 //
-// Two forms give the same node and order arrays:
+// Three forms give the same node and order arrays:
 //   * the recursive build in scene_host.cpp (BvhBuilder), which follows the reference's
 //     BLAS::build / PrimBLAS::build / TLAS::build step for step;
 //   * build_bvh_levels (bvh_levels.cpp), the level-synchronous form: every node of a depth is
 //     split at once, and each step is an ordered reduction, a prefix sum or a per-node scan.
-//     This is the form a device build takes.
+//     build_bvh_device (bvh_device.cu) runs this form on the device.
 #pragma once
 
 #include <cstdint>
 #include <vector>
 
 #include "../../include/xenon_b200.h"
+#include "bvh_refit.h"
 #include "host_math.h"
 
 namespace xb {
@@ -32,7 +33,22 @@ int sah_best_split(const Bounds* bin_box, const int* bin_cnt, int bins, const Bo
 // reordered in place; order receives each leaf slot's item index.
 struct LevelItem;
 std::vector<LevelItem> to_level_items(const std::vector<BuildItem>& items);
+
+// A node of the level-synchronous builds, in level order: items [lo, hi), the level-order
+// index of its left child (the right child follows it; -1 for a leaf) and its box.
+struct LevelNodeRecord {
+  uint32_t lo, hi;
+  int32_t left;
+  RefitBox box;
+};
+// The node array in the recursive build's depth-first allocation order, from level-order nodes.
+void place_level_nodes(const std::vector<LevelNodeRecord>& all, std::vector<xb_bvh_node>& nodes);
+
 void build_bvh_levels(std::vector<BuildItem>& items, int bins, uint32_t max_leaf, bool leaf_cost,
+                      std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
+// The same build run by the device (bvh_device.cu) on the current CUDA device: the same
+// arrays. Throws std::runtime_error on a CUDA error, std::invalid_argument on bad arguments.
+void build_bvh_device(std::vector<BuildItem>& items, int bins, uint32_t max_leaf, bool leaf_cost,
                       std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
 
 }  // namespace xb

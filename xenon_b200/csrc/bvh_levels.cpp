@@ -30,13 +30,6 @@
 namespace xb {
 namespace {
 
-struct LevelNode {
-  uint32_t lo, hi;
-  int32_t left;   // level-order index of the left child (the right child is left + 1); -1: a leaf
-  RefitBox box;
-  LevelNode(uint32_t l, uint32_t h) : lo(l), hi(h), left(-1) {}
-};
-
 class LevelBuilder {
  public:
   LevelBuilder(std::vector<LevelItem>& items, int bins, uint32_t max_leaf, bool leaf_cost)
@@ -46,14 +39,14 @@ class LevelBuilder {
     nodes.clear();
     if (it_.empty()) return;
     all_.clear();
-    all_.emplace_back(0u, (uint32_t)it_.size());
+    all_.push_back(LevelNodeRecord{0u, (uint32_t)it_.size(), -1, RefitBox()});
     // one pass per depth: the nodes of the depth, in the order their parents were split
     for (size_t begin = 0; begin < all_.size();) {
       const size_t end = all_.size();
       for (size_t x = begin; x < end; ++x) split(x);
       begin = end;
     }
-    place(all_, nodes);
+    place_level_nodes(all_, nodes);
   }
 
  private:
@@ -61,7 +54,7 @@ class LevelBuilder {
   int bins_;
   uint32_t max_leaf_;
   bool leaf_cost_;
-  std::vector<LevelNode> all_;   // every node, in level order
+  std::vector<LevelNodeRecord> all_;   // every node, in level order
 
   void split(size_t x) {
     const uint32_t lo = all_[x].lo, hi = all_[x].hi, count = hi - lo;
@@ -129,40 +122,40 @@ class LevelBuilder {
       }
     }
     all_[x].left = (int32_t)all_.size();
-    all_.emplace_back(lo, mid);
-    all_.emplace_back(mid, hi);
-  }
-
-  // Node x of the level order goes to index pos[x]. Its child pair, if it has one, starts at
-  // pair[x]. internal[x] counts the interior nodes of x's subtree.
-  static void place(const std::vector<LevelNode>& all, std::vector<xb_bvh_node>& nodes) {
-    const size_t n = all.size();
-    std::vector<uint32_t> internal(n, 0), pos(n, 0), pair(n, 0);
-    for (size_t x = n; x-- > 0;)
-      if (all[x].left >= 0) internal[x] = 1 + internal[all[x].left] + internal[all[x].left + 1];
-    nodes.assign(1 + 2 * (size_t)internal[0], xb_bvh_node{});
-    pair[0] = 1;
-    for (size_t x = 0; x < n; ++x) {
-      const LevelNode& d = all[x];
-      xb_bvh_node& out = nodes[pos[x]];
-      for (int k = 0; k < 3; ++k) { out.mn[k] = d.box.mn[k]; out.mx[k] = d.box.mx[k]; }
-      if (d.left < 0) {
-        out.child = d.lo;
-        out.count = d.hi - d.lo;
-        continue;
-      }
-      out.child = pair[x];
-      out.count = 0;
-      const int32_t l = d.left, r = d.left + 1;
-      pos[l] = pair[x];
-      pos[r] = pair[x] + 1;
-      pair[l] = pair[x] + 2;
-      pair[r] = pair[x] + 2 + 2 * internal[l];
-    }
+    all_.push_back(LevelNodeRecord{lo, mid, -1, RefitBox()});
+    all_.push_back(LevelNodeRecord{mid, hi, -1, RefitBox()});
   }
 };
 
 }  // namespace
+
+// Node x of the level order goes to index pos[x]. Its child pair, if it has one, starts at
+// pair[x]. internal[x] counts the interior nodes of x's subtree.
+void place_level_nodes(const std::vector<LevelNodeRecord>& all, std::vector<xb_bvh_node>& nodes) {
+  const size_t n = all.size();
+  std::vector<uint32_t> internal(n, 0), pos(n, 0), pair(n, 0);
+  for (size_t x = n; x-- > 0;)
+    if (all[x].left >= 0) internal[x] = 1 + internal[all[x].left] + internal[all[x].left + 1];
+  nodes.assign(1 + 2 * (size_t)internal[0], xb_bvh_node{});
+  pair[0] = 1;
+  for (size_t x = 0; x < n; ++x) {
+    const LevelNodeRecord& d = all[x];
+    xb_bvh_node& out = nodes[pos[x]];
+    for (int k = 0; k < 3; ++k) { out.mn[k] = d.box.mn[k]; out.mx[k] = d.box.mx[k]; }
+    if (d.left < 0) {
+      out.child = d.lo;
+      out.count = d.hi - d.lo;
+      continue;
+    }
+    out.child = pair[x];
+    out.count = 0;
+    const int32_t l = d.left, r = d.left + 1;
+    pos[l] = pair[x];
+    pos[r] = pair[x] + 1;
+    pair[l] = pair[x] + 2;
+    pair[r] = pair[x] + 2 + 2 * internal[l];
+  }
+}
 
 std::vector<LevelItem> to_level_items(const std::vector<BuildItem>& items) {
   std::vector<LevelItem> out(items.size());

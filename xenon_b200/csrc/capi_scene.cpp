@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <stdexcept>
 #include <string>
 
 #include "capi_common.h"
@@ -191,7 +192,7 @@ int xb_scene_set_build_threads(xb_scene* s, int32_t threads) {
 
 int xb_scene_set_build_mode(xb_scene* s, int32_t mode) {
   SCENE_MUTABLE(s);
-  if (mode != XB_BUILD_RECURSIVE && mode != XB_BUILD_LEVELS)
+  if (mode != XB_BUILD_RECURSIVE && mode != XB_BUILD_LEVELS && mode != XB_BUILD_DEVICE)
     return fail(XB_E_INVALID, "xb_scene_set_build_mode: unknown mode %d", mode);
   s->s.build_mode = mode;
   return XB_OK;
@@ -206,6 +207,10 @@ int xb_scene_build(xb_scene* s) {
     s->s.build();
   } catch (const std::bad_alloc&) {
     return fail(XB_E_OOM, "xb_scene_build: out of host memory");
+  } catch (const std::invalid_argument& e) {
+    return fail(XB_E_INVALID, "xb_scene_build: %s", e.what());
+  } catch (const std::runtime_error& e) {   // the device build's CUDA errors
+    return fail(XB_E_CUDA, "xb_scene_build: %s", e.what());
   }
   return XB_OK;
 }
@@ -223,6 +228,8 @@ int xb_scene_refit_mesh(xb_scene* s, int32_t mesh, const float* positions, const
     s->s.refit_mesh(mesh, positions, normals);
   } catch (const std::bad_alloc&) {
     return fail(XB_E_OOM, "xb_scene_refit_mesh: out of host memory");
+  } catch (const std::exception& e) {
+    return fail(XB_E_INVALID, "xb_scene_refit_mesh: %s", e.what());
   }
   return XB_OK;
 }

@@ -364,7 +364,8 @@ void HostScene::build() {
       b.grow(m.vertex(m.indices[3 * t + 2]));
       items[t] = {b, b.center(), (uint32_t)t};
     }
-    if (build_mode == 1) build_bvh_levels(items, 12, 2, true, m.nodes, m.prims);
+    if (build_mode == 2) build_bvh_device(items, 12, 2, true, m.nodes, m.prims);
+    else if (build_mode == 1) build_bvh_levels(items, 12, 2, true, m.nodes, m.prims);
     else BvhBuilder(12, 2, true, par_depth).build(items, m.nodes, m.prims);
   };
   std::atomic<size_t> next{0};
@@ -379,7 +380,8 @@ void HostScene::build() {
     }
   };
   std::vector<std::thread> pool;
-  for (int k = 1; k < std::min<int>(threads, (int)meshes.size()); ++k) pool.emplace_back(worker);
+  const int mesh_threads = build_mode == 2 ? 1 : threads;   // device builds: one mesh at a time
+  for (int k = 1; k < std::min<int>(mesh_threads, (int)meshes.size()); ++k) pool.emplace_back(worker);
   worker();
   for (std::thread& t : pool) t.join();
   for (const std::exception_ptr& e : failed)
@@ -393,7 +395,8 @@ void HostScene::build() {
       Bounds b = prim_bounds(prims[i]);
       items[i] = {b, b.center(), (uint32_t)i};
     }
-    if (build_mode == 1) build_bvh_levels(items, 12, 2, true, prim_nodes, prim_indices);
+    if (build_mode == 2) build_bvh_device(items, 12, 2, true, prim_nodes, prim_indices);
+    else if (build_mode == 1) build_bvh_levels(items, 12, 2, true, prim_nodes, prim_indices);
     else BvhBuilder(12, 2, true).build(items, prim_nodes, prim_indices);
   }
   // Instances: explicit ones, or one identity instance per mesh + one for the prim group
@@ -441,7 +444,8 @@ void build_tlas(const std::vector<Affine>& l2w, const std::vector<const xb_bvh_n
                              (c & 4) ? local.mx.z : local.mn.z)));
     items[i] = {w, w.center(), (uint32_t)i};
   }
-  if (mode == 1) build_bvh_levels(items, 8, 1, false, nodes, order);
+  if (mode == 2) build_bvh_device(items, 8, 1, false, nodes, order);
+  else if (mode == 1) build_bvh_levels(items, 8, 1, false, nodes, order);
   else BvhBuilder(8, 1, false).build(items, nodes, order);
 }
 
@@ -482,7 +486,10 @@ void HostScene::refit_mesh(int mesh, const float* positions, const float* normal
     }
   }
   refit_blas(m, m.nodes);
+  const int mode = build_mode;
+  build_mode = 0;   // the TLAS over the new root boxes is rebuilt on the host (same arrays)
   build_tlas();
+  build_mode = mode;
 }
 
 void HostScene::view(xb_scene_view* v) {

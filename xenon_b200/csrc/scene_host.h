@@ -48,7 +48,7 @@ class HostScene {
   std::vector<uint32_t> tlas_inst;
   bool built = false;
   int build_threads = 0;   // BVH build threads (0: the machine's hardware threads, 1: one)
-  int build_mode = 0;      // 0: recursive build, 1: level-synchronous build (same arrays)
+  int build_mode = 0;      // 0: recursive, 1: level-synchronous, 2: on the device (same arrays)
 
   HostScene();
   void build();
