@@ -255,8 +255,8 @@ def view_arrays(v: SceneView) -> dict:
         if mv.nx:
             nrm = np.stack([np.ctypeslib.as_array(getattr(mv, k), (nv,)) for k in ("nx", "ny", "nz")], 1).copy()
         nt = mv.num_triangles
-        idx = np.ctypeslib.as_array(mv.indices, (nt, 3)).copy() if nt else np.zeros((0, 3), np.int32)
-        mat = np.ctypeslib.as_array(mv.mat_ids, (nt,)).copy() if nt else np.zeros(0, np.int32)
+        idx = np.ctypeslib.as_array(mv.indices, (nt, 3)).copy() if nt and mv.indices else np.zeros((0, 3), np.int32)
+        mat = np.ctypeslib.as_array(mv.mat_ids, (nt,)).copy() if nt and mv.mat_ids else np.zeros(0, np.int32)
         out["meshes"].append({"nodes": nodes, "prims": prims, "pos": pos, "nrm": nrm, "indices": idx,
                               "mat_ids": mat})
     n = v.num_tlas_nodes
