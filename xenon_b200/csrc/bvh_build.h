@@ -33,6 +33,8 @@ int sah_best_split(const Bounds* bin_box, const int* bin_cnt, int bins, const Bo
 // reordered in place; order receives each leaf slot's item index.
 struct LevelItem;
 std::vector<LevelItem> to_level_items(const std::vector<BuildItem>& items);
+// The items back, in their built order, and each slot's item index in order.
+void from_level_items(const std::vector<LevelItem>& it, std::vector<BuildItem>& items, std::vector<uint32_t>& order);
 
 // A node of the level-synchronous builds, in level order: items [lo, hi), the level-order
 // index of its left child (the right child follows it; -1 for a leaf) and its box.

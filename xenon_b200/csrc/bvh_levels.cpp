@@ -4,7 +4,8 @@
 // src/geometry/blas.cpp:100-205) splits depth first, one node at a time. Here every node of a
 // depth is split in the same pass, and each step has the data-parallel form a device build
 // uses, chosen so that the node and order arrays come out identical to the recursive build's.
-// The per-thread steps are those of bvh_level_steps.h, which the device build runs too:
+// Its passes and its depth loop are those of bvh_level_kernels.h, which the device build
+// (bvh_device.cu) runs too; here each pass is a loop over its thread indices:
 //
 //   * Bounds (of the item boxes, of their centroids, of each bin) are folds that keep the first
 //     of equal values (std::min / std::max). Such a fold is associative, so folding fixed-size
@@ -25,105 +26,64 @@
 #include <stdexcept>
 
 #include "bvh_build.h"
-#include "bvh_level_steps.h"
+#include "bvh_level_kernels.h"
 
 namespace xb {
 namespace {
 
-class LevelBuilder {
- public:
-  LevelBuilder(std::vector<LevelItem>& items, int bins, uint32_t max_leaf, bool leaf_cost)
-      : it_(items), bins_(bins), max_leaf_(max_leaf), leaf_cost_(leaf_cost) {}
+// Runs the passes of a depth as loops over their thread indices, in host memory.
+struct HostLevelExec {
+  std::vector<LevelItem>& items;
+  std::vector<LevelTask> tasks;
+  std::vector<ChunkRef> chunks;
+  std::vector<NodeOut> out;
+  std::vector<RefitBox> chunk_box, chunk_cbox, chunk_bins;
+  std::vector<int32_t> chunk_cnt;
+  std::vector<uint32_t> chunk_pass, chunk_before;
+  std::vector<int64_t> left_of, right_of;
 
-  void build(std::vector<xb_bvh_node>& nodes) {
-    nodes.clear();
-    if (it_.empty()) return;
-    all_.clear();
-    all_.push_back(LevelNodeRecord{0u, (uint32_t)it_.size(), -1, RefitBox()});
-    // one pass per depth: the nodes of the depth, in the order their parents were split
-    for (size_t begin = 0; begin < all_.size();) {
-      const size_t end = all_.size();
-      for (size_t x = begin; x < end; ++x) split(x);
-      begin = end;
-    }
-    place_level_nodes(all_, nodes);
+  explicit HostLevelExec(std::vector<LevelItem>& it)
+      : items(it), left_of(it.size()), right_of(it.size()) {}
+
+  void run_depth(LevelArgs& a, const std::vector<LevelTask>& t, const std::vector<ChunkRef>& c,
+                 std::vector<NodeOut>& result, int32_t* error) {
+    tasks = t;
+    chunks = c;
+    out.assign(t.size(), NodeOut());
+    chunk_box.assign(c.size(), RefitBox());
+    chunk_cbox.assign(c.size(), RefitBox());
+    chunk_bins.assign(c.size() * a.bins, RefitBox());
+    chunk_cnt.assign(c.size() * a.bins, 0);
+    chunk_pass.assign(c.size(), 0);
+    chunk_before.assign(c.size(), 0);
+    std::fill(left_of.begin(), left_of.end(), -1);
+    std::fill(right_of.begin(), right_of.end(), -1);
+    a.items = items.data();
+    a.tasks = tasks.data();
+    a.chunks = chunks.data();
+    a.out = out.data();
+    a.chunk_box = chunk_box.data();
+    a.chunk_cbox = chunk_cbox.data();
+    a.chunk_bins = chunk_bins.data();
+    a.chunk_cnt = chunk_cnt.data();
+    a.chunk_pass = chunk_pass.data();
+    a.chunk_before = chunk_before.data();
+    a.left_of = left_of.data();
+    a.right_of = right_of.data();
+    a.error = error;
+    for (uint32_t i = 0; i < a.nchunks; ++i) lvl_bounds_at(a, i);
+    for (uint32_t i = 0; i < a.ntasks; ++i) lvl_plane_at(a, i);
+    for (uint32_t i = 0; i < a.nchunks; ++i) lvl_bins_at(a, i);
+    for (uint32_t i = 0; i < a.ntasks; ++i) lvl_sah_at(a, i);
+    for (uint32_t i = 0; i < a.nchunks; ++i) lvl_pass_at(a, i);
+    for (uint32_t i = 0; i < a.ntasks; ++i) lvl_prefix_at(a, i);
+    for (uint32_t i = 0; i < a.nchunks; ++i) lvl_rank_at(a, i);
+    for (uint32_t i = 0; i < a.nitems; ++i) lvl_exchange_at(a, i);
+    result = out;
   }
 
- private:
-  std::vector<LevelItem>& it_;
-  int bins_;
-  uint32_t max_leaf_;
-  bool leaf_cost_;
-  std::vector<LevelNodeRecord> all_;   // every node, in level order
-
-  void split(size_t x) {
-    const uint32_t lo = all_[x].lo, hi = all_[x].hi, count = hi - lo;
-    // node box and centroid bounds: chunk partials, folded in chunk order
-    RefitBox nb, cb;
-    refit_empty(nb);
-    refit_empty(cb);
-    for (uint32_t c = lo; c < hi; c += kLevelChunk) {
-      RefitBox pb, pc;
-      level_chunk_bounds(it_.data(), c, std::min(hi, c + kLevelChunk), pb, pc);
-      refit_grow(nb, pb);
-      refit_grow(cb, pc);
-    }
-    all_[x].box = nb;
-    if (count <= max_leaf_) return;
-    int axis;
-    float cmin, scale;
-    if (!level_plane(cb, bins_, &axis, &cmin, &scale)) return;
-    // bins: chunk partials, folded in chunk order
-    RefitBox bin_box[kLevelMaxBins];
-    int bin_cnt[kLevelMaxBins] = {};
-    for (int k = 0; k < bins_; ++k) refit_empty(bin_box[k]);
-    for (uint32_t c = lo; c < hi; c += kLevelChunk) {
-      RefitBox pbox[kLevelMaxBins];
-      int pcnt[kLevelMaxBins];
-      level_chunk_bins(it_.data(), c, std::min(hi, c + kLevelChunk), axis, cmin, scale, bins_, pbox, pcnt);
-      for (int k = 0; k < bins_; ++k) {
-        bin_cnt[k] += pcnt[k];
-        refit_grow(bin_box[k], pbox[k]);
-      }
-    }
-    float best;
-    const int best_bin = level_sah(bin_box, bin_cnt, bins_, nb, &best);
-    if ((leaf_cost_ && best >= (float)count) || best_bin < 0) return;
-    // passing items per chunk, their prefix over the node, and the total m
-    std::vector<uint32_t> chunk_before;
-    uint32_t m = 0;
-    for (uint32_t c = lo; c < hi; c += kLevelChunk) {
-      chunk_before.push_back(m);
-      for (uint32_t i = c; i < std::min(hi, c + kLevelChunk); ++i)
-        m += level_pass(it_[i], axis, cmin, scale, bins_, best_bin);
-    }
-    uint32_t mid;
-    if (m == 0 || m == count) {
-      mid = lo + count / 2;
-      std::nth_element(it_.begin() + lo, it_.begin() + mid, it_.begin() + hi,
-                       [axis](const LevelItem& a, const LevelItem& b) { return a.c[axis] < b.c[axis]; });
-    } else {
-      mid = lo + m;
-      // each moving item's exchange rank, then the exchange
-      const uint32_t moves = count - m;   // an upper bound on the exchanges
-      std::vector<int64_t> left_of(moves, -1), right_of(moves, -1);
-      for (uint32_t c = lo, ci = 0; c < hi; c += kLevelChunk, ++ci) {
-        uint32_t before = chunk_before[ci];
-        for (uint32_t i = c; i < std::min(hi, c + kLevelChunk); ++i) {
-          const bool pass = level_pass(it_[i], axis, cmin, scale, bins_, best_bin);
-          const int64_t k = level_exchange_rank(i - lo, pass, before, m);
-          if (k >= 0) (i - lo < m ? left_of : right_of)[k] = i;
-          before += pass;
-        }
-      }
-      for (uint32_t k = 0; k < moves && left_of[k] >= 0; ++k) {
-        if (right_of[k] < 0) throw std::logic_error("build_bvh_levels: exchange ranks disagree");
-        std::swap(it_[left_of[k]], it_[right_of[k]]);
-      }
-    }
-    all_[x].left = (int32_t)all_.size();
-    all_.push_back(LevelNodeRecord{lo, mid, -1, RefitBox()});
-    all_.push_back(LevelNodeRecord{mid, hi, -1, RefitBox()});
+  void median_split(uint32_t lo, uint32_t mid, uint32_t hi, int axis) {
+    level_median_split(items.data(), lo, mid, hi, axis);
   }
 };
 
@@ -157,6 +117,18 @@ void place_level_nodes(const std::vector<LevelNodeRecord>& all, std::vector<xb_b
   }
 }
 
+void from_level_items(const std::vector<LevelItem>& it, std::vector<BuildItem>& items, std::vector<uint32_t>& order) {
+  order.resize(it.size());
+  for (size_t i = 0; i < it.size(); ++i) {
+    const LevelItem& l = it[i];
+    order[i] = l.index;
+    items[i].box.mn = F3(l.mn[0], l.mn[1], l.mn[2]);
+    items[i].box.mx = F3(l.mx[0], l.mx[1], l.mx[2]);
+    items[i].centroid = F3(l.c[0], l.c[1], l.c[2]);
+    items[i].index = l.index;
+  }
+}
+
 std::vector<LevelItem> to_level_items(const std::vector<BuildItem>& items) {
   std::vector<LevelItem> out(items.size());
   for (size_t i = 0; i < items.size(); ++i) {
@@ -170,16 +142,14 @@ std::vector<LevelItem> to_level_items(const std::vector<BuildItem>& items) {
 void build_bvh_levels(std::vector<BuildItem>& items, int bins, uint32_t max_leaf, bool leaf_cost,
                       std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order) {
   if (bins < 2 || bins > kLevelMaxBins) throw std::invalid_argument("build_bvh_levels: bins");
+  if (items.size() >= (1u << 31)) throw std::invalid_argument("build_bvh_levels: too many items");
   std::vector<LevelItem> it = to_level_items(items);
-  LevelBuilder(it, bins, max_leaf, leaf_cost).build(nodes);
-  order.resize(it.size());
-  for (size_t i = 0; i < it.size(); ++i) {
-    order[i] = it[i].index;
-    const LevelItem& l = it[i];
-    items[i] = BuildItem{Bounds(), F3(l.c[0], l.c[1], l.c[2]), l.index};
-    items[i].box.mn = F3(l.mn[0], l.mn[1], l.mn[2]);
-    items[i].box.mx = F3(l.mx[0], l.mx[1], l.mx[2]);
-  }
+  HostLevelExec ex(it);
+  std::vector<LevelNodeRecord> all;
+  run_level_build(ex, (uint32_t)it.size(), bins, max_leaf, leaf_cost, all);
+  nodes.clear();
+  if (!all.empty()) place_level_nodes(all, nodes);
+  from_level_items(it, items, order);
 }
 
 }  // namespace xb
