@@ -95,8 +95,8 @@ struct DeviceLevelExec {
     n = (uint32_t)it.size();
     ck(cudaMemcpy(items.need(n, "items"), it.data(), (size_t)n * sizeof(LevelItem), cudaMemcpyHostToDevice),
        "upload items");
-    left.need(n, "rank tables");
-    right.need(n, "rank tables");
+    ck(cudaMemset(left.need(n, "rank tables"), 0xff, (size_t)n * sizeof(int64_t)), "clear rank tables");
+    ck(cudaMemset(right.need(n, "rank tables"), 0xff, (size_t)n * sizeof(int64_t)), "clear rank tables");
     error.need(1, "status");
   }
 
@@ -121,8 +121,6 @@ struct DeviceLevelExec {
     a.error = error.p;
     ck(cudaMemcpy(tasks.p, t.data(), t.size() * sizeof(LevelTask), cudaMemcpyHostToDevice), "upload tasks");
     ck(cudaMemcpy(chunks.p, c.data(), c.size() * sizeof(ChunkRef), cudaMemcpyHostToDevice), "upload chunks");
-    ck(cudaMemset(left.p, 0xff, (size_t)n * sizeof(int64_t)), "clear rank tables");
-    ck(cudaMemset(right.p, 0xff, (size_t)n * sizeof(int64_t)), "clear rank tables");
     ck(cudaMemset(error.p, 0, sizeof(int32_t)), "clear status");
     lvl_bounds<<<blocks(a.nchunks), 128>>>(a);
     lvl_plane<<<blocks(a.ntasks), 128>>>(a);

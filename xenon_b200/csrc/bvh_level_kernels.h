@@ -59,8 +59,8 @@ struct LevelArgs {
   int32_t* chunk_cnt;         // `bins` per chunk
   uint32_t* chunk_pass;
   uint32_t* chunk_before;
-  int64_t* left_of;           // per item slot lo + rank: the failing item's index (-1: none)
-  int64_t* right_of;          // per item slot lo + rank: the passing item's index (-1: none)
+  int64_t* left_of;           // per item slot lo + rank: the failing item's index (-1: none);
+  int64_t* right_of;          // the passing item's. All -1 between depths (lvl_exchange_at)
   int32_t* error;             // 0; 1 a rank outside the tables; 2 a rank with one side only
   uint32_t ntasks, nchunks, nitems, max_leaf;
   int32_t bins, leaf_cost;
@@ -170,6 +170,8 @@ XB_HD void lvl_rank_at(const LevelArgs& a, uint32_t c) {
   }
 }
 
+// Swaps the pair slot s names and clears the slot, so the tables are all -1 again for the next
+// depth (they start so).
 XB_HD void lvl_exchange_at(const LevelArgs& a, uint32_t s) {
   const int64_t l = a.left_of[s];
   if (l < 0) return;
@@ -178,6 +180,8 @@ XB_HD void lvl_exchange_at(const LevelArgs& a, uint32_t s) {
   const LevelItem t = a.items[l];
   a.items[l] = a.items[r];
   a.items[r] = t;
+  a.left_of[s] = -1;
+  a.right_of[s] = -1;
 }
 
 // The level loop over n items (already in the executor's memory). Exec provides

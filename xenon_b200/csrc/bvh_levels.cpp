@@ -43,7 +43,7 @@ struct HostLevelExec {
   std::vector<int64_t> left_of, right_of;
 
   explicit HostLevelExec(std::vector<LevelItem>& it)
-      : items(it), left_of(it.size()), right_of(it.size()) {}
+      : items(it), left_of(it.size(), -1), right_of(it.size(), -1) {}
 
   void run_depth(LevelArgs& a, const std::vector<LevelTask>& t, const std::vector<ChunkRef>& c,
                  std::vector<NodeOut>& result, int32_t* error) {
@@ -56,8 +56,6 @@ struct HostLevelExec {
     chunk_cnt.assign(c.size() * a.bins, 0);
     chunk_pass.assign(c.size(), 0);
     chunk_before.assign(c.size(), 0);
-    std::fill(left_of.begin(), left_of.end(), -1);
-    std::fill(right_of.begin(), right_of.end(), -1);
     a.items = items.data();
     a.tasks = tasks.data();
     a.chunks = chunks.data();
