@@ -206,3 +206,47 @@ def test_baked_instances_match_the_reference_parser_and_the_instanced_scene(tmp_
     lights = np.frombuffer(mine["lights"], np.uint32).reshape(-1, 6)
     for (mesh_id, tri, e, area), row in zip(desc.lights, lights):
         assert row[0] == by_id[mesh_id] and row[1] == tri
+
+
+def test_documented_but_unparsed_syntax_loads_as_the_reference_parses_it(tmp_path, monkeypatch, ref):
+    """The reference's README and material docs show syntax its parser does not read: a `sun`
+    line, `transmissionRoughness`, `anisotropic`, a `type` other than principled. There are also
+    malformed numbers, which istream extraction turns into 0 or leaves at their defaults. The
+    parser is the format's definition, so this library's loader must build what the reference's
+    builds from such a file."""
+    (tmp_path / "materials").mkdir()
+    (tmp_path / "materials" / "odd.mat").write_text(
+        "# a material with the documented-only keys\n"
+        "name odd\ntype glossy\nbaseColor 0.5 abc 0.25\nroughness 0.4\n"
+        "transmissionRoughness 0.3\nanisotropic 0.6\nmetallic\nior 1.33 extra\n"
+        "emission 1 2\n")
+    (tmp_path / "materials" / "plain.mat").write_text("name \"plain\"\nbaseColor 0.7 0.7 0.7\n")
+    obj = "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nf 1 2 3\nusemtl odd\nf 2 4 3\n"
+    (tmp_path / "quad.obj").write_text(obj)
+    (tmp_path / "odd.xenon").write_text(
+        "config 64 48\ncamera 0 1 5 0 0.5 0 35\nmatfile odd.mat\nmatfile \"plain.mat\"\n"
+        "mesh quad.obj\nlight 0 1 255 182 120 0.5\nlight 0 0 1 1\n"
+        "sun 1 -1 0.5 3.0 3.0 2.8\nsunlight 0 0 0 1 1 1\nsunlight 1 2 2 0.5 0.5 0.5 4\n"
+        "sky 0.1 0.2 0.3 0.4 0.5 0.6\nsphere 0 1 0 0.5 odd\nsphere 2 1 0 0.5 nosuchmaterial\n"
+        "disk 0 0 0 0 3 4 1 plain\nplane 0 0 2 -1 plain\nbogus line here\n")
+    monkeypatch.chdir(tmp_path)
+    mine = HostScene.load("odd.xenon")
+    h = ctypes.c_void_p()
+    cfg = np.zeros(3, np.int32)
+    cam = np.zeros(12, np.float32)
+    assert ref.lib().xr_scene_load_xenon(b"odd.xenon", ctypes.byref(h), ref.ptr(cfg), ref.ptr(cam)) == 0
+    try:
+        v = abi.SceneView()
+        assert ref.lib().xr_scene_view(h, ctypes.byref(v)) == 0
+        theirs = _summary(v)
+        got = _summary(mine.view())
+        _assert_same_scene(got, theirs, [True])
+        assert got["meshes"][0]["pos"].tobytes() == theirs["meshes"][0]["pos"].tobytes()
+        assert np.array_equal(got["meshes"][0]["mat_ids"], [0, 0])   # the first face before any usemtl: 0
+        assert list(cfg) == [mine.config.width, mine.config.height, mine.config.samples] == [64, 48, 64]
+        from xenon_b200 import camera
+        cd = mine.camera_desc
+        c = camera(list(cd.eye), list(cd.target), cd.fov_y_deg, 64 / 48).to_array()
+        assert c.tobytes() == cam.tobytes()
+    finally:
+        ref.lib().xr_scene_free(h)
