@@ -167,12 +167,19 @@ class Renderer:
         """Accepts a HostScene or an abi.SceneView (e.g. exported from another builder)."""
         v = scene.view() if isinstance(scene, HostScene) else scene
         self._check(lib().xb_upload_scene(self.h, ctypes.byref(v)))
+        self._mesh_vertices = [v.meshes[i].num_vertices for i in range(v.num_meshes)]
 
     def refit_mesh(self, mesh: int, positions, normals=None) -> None:
         """Moves an uploaded mesh's vertices and refits its BLAS on the device (xb_refit_mesh);
         positions, normals: (num_vertices, 3) float32 in host memory."""
         pos = np.ascontiguousarray(positions, np.float32)
         nrm = None if normals is None else np.ascontiguousarray(normals, np.float32)
+        counts = getattr(self, "_mesh_vertices", [])
+        if not 0 <= mesh < len(counts):
+            raise XenonError(abi.XB_E_INVALID, f"refit_mesh: no uploaded mesh {mesh}")
+        nv = counts[mesh]
+        if pos.shape != (nv, 3) or (nrm is not None and nrm.shape != (nv, 3)):
+            raise XenonError(abi.XB_E_INVALID, f"refit_mesh: mesh {mesh} has {nv} vertices")
         self._check(lib().xb_refit_mesh(self.h, int(mesh), _p(pos), _p(nrm)))
 
     def set_bounces(self, min_bounces: int, max_bounces: int) -> None:
