@@ -298,8 +298,8 @@ int  xb_upload_scene(xb_renderer *r, const xb_scene_view *view);
 /* Moves the vertices of uploaded mesh `mesh` and refits its BLAS on the device: the triangles
  * take the new positions, and every node box is recomputed bottom-up by one kernel in which the
  * second child to reach a node folds both children's boxes (no thread waits for another). The
- * folds are xb_scene_refit_mesh's, so both give the same node arrays. The TLAS is then rebuilt
- * on the host over the instances' new world boxes and copied up. positions: host
+ * passes are those xb_scene_refit_mesh runs on the host, so both give the same node arrays. The
+ * TLAS is then rebuilt on the host over the instances' new world boxes and copied up. positions: host
  * float[3 * nv] (nv = the mesh's vertex count in the uploaded view); normals: the same, or NULL
  * to keep the uploaded ones. Meshes that carry area lights are refused (XB_E_UNSUPPORTED: their
  * emitter geometry is built on the host at upload; refit the host scene and upload again).

@@ -1,7 +1,7 @@
 // bvh_refit.h — BLAS refit: node boxes recomputed from moved vertices, tree topology kept.
 //
-// Shared by the host (HostScene::refit_mesh) and the device (xb_refit_mesh in renderer.cu), so
-// that both fold the same boxes in the same order. The folds are the build's: a box starts
+// The box folds of the refit passes (refit_kernels.h), which the host (HostScene::refit_mesh)
+// and the device (xb_refit_mesh in renderer.cu) both run. The folds are the build's: a box starts
 // empty (+inf / -inf) and grows with std::min / std::max semantics, so the first of two equal
 // values is kept (Bounds::grow in host_math.h, AABB::expand in the reference's
 // src/geometry/aabb.h). A triangle's box is its three vertices folded in index order. A leaf's

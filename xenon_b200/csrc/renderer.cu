@@ -34,6 +34,7 @@
 
 #include "../../include/xenon_b200.h"
 #include "bvh_refit.h"
+#include "refit_kernels.h"
 #include "capi_common.h"
 #include "dev_bsdf.cuh"
 #include "dev_math.cuh"
@@ -1903,95 +1904,18 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
 }
 
 // ── BLAS refit (xb_refit_mesh): one mesh's triangles and node boxes, topology kept ──────────
-// The node boxes are folded by bvh_refit.h, the same code the host refit runs, so a device
-// refit and a host refit of the same vertices give the same arrays.
-struct RefitArgs {
-  float4* blas;               // all meshes' nodes, two float4 each (node_lo, node_hi)
-  float4* tris;               // all meshes' triangle slots, three float4 each
-  const int32_t* tri_index;   // global vertex ids per global triangle
-  const float* pos;           // the mesh's new positions, float[3 * num_verts]
-  int32_t* parent;            // per node of the mesh: its parent (-1: root)
-  uint32_t* arrivals;         // per node of the mesh: children whose walk reached it
-  int32_t* status;            // 0 ok; 1 an index out of range; 2 a walk longer than the node count
-  int64_t node_base, slot_base;
-  int32_t num_nodes, num_tris, num_verts, tri_offset, vtx_offset;
-};
-
-// Triangle slot s of the mesh takes its three vertices from the new positions (the .w words,
-// the triangle's indices, stay).
-__global__ void refit_tris_kernel(RefitArgs a) {
+// The passes are refit_kernels.h's, which the host refit (xb_scene_refit_mesh) runs as loops.
+__global__ void refit_tris_kernel(xb::RefitArgs a) {
   const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.num_tris) return;
-  float4* T = a.tris + 3 * (a.slot_base + s);
-  const int32_t t = __float_as_int(T[0].w);   // the triangle's index within its mesh
-  if (t < 0 || t >= a.num_tris) { atomicExch(a.status, 1); return; }
-  int32_t v[3];
-  for (int k = 0; k < 3; ++k) {
-    v[k] = a.tri_index[3 * (int64_t)(a.tri_offset + t) + k] - a.vtx_offset;
-    if (v[k] < 0 || v[k] >= a.num_verts) { atomicExch(a.status, 1); return; }
-  }
-  for (int k = 0; k < 3; ++k) {
-    const float* p = a.pos + 3 * (int64_t)v[k];
-    T[k] = make_float4(p[0], p[1], p[2], T[k].w);
-  }
+  if (s < a.num_tris) xb::refit_tris_at(a, s);
 }
-
-// Each interior node names itself as its two children's parent; every arrival count starts at 0.
-__global__ void refit_parents_kernel(RefitArgs a) {
+__global__ void refit_parents_kernel(xb::RefitArgs a) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.num_nodes) return;
-  a.arrivals[i] = 0u;
-  const float4 hi = a.blas[2 * (a.node_base + i) + 1];
-  if (__float_as_uint(hi.w) != 0u) return;   // a leaf
-  const int64_t c = (int64_t)__float_as_uint(hi.z) - a.node_base;
-  if (c < 1 || c + 1 >= a.num_nodes) { atomicExch(a.status, 1); return; }
-  a.parent[c] = i;
-  a.parent[c + 1] = i;
+  if (i < a.num_nodes) xb::refit_parents_at(a, i);
 }
-
-// Boxes written during the walk are read and written through L2 (other SMs write them).
-__device__ __forceinline__ xb::RefitBox refit_load_box(const float4* blas, int64_t n) {
-  const float4 lo = __ldcg(blas + 2 * n), hi = __ldcg(blas + 2 * n + 1);
-  xb::RefitBox b;
-  b.mn[0] = lo.x; b.mn[1] = lo.y; b.mn[2] = lo.z;
-  b.mx[0] = lo.w; b.mx[1] = hi.x; b.mx[2] = hi.y;
-  return b;
-}
-__device__ __forceinline__ void refit_store_box(float4* blas, int64_t n, const xb::RefitBox& b, float4 hi) {
-  __stcg(blas + 2 * n, make_float4(b.mn[0], b.mn[1], b.mn[2], b.mx[0]));
-  __stcg(blas + 2 * n + 1, make_float4(b.mx[1], b.mx[2], hi.z, hi.w));
-}
-
-// One thread per leaf: the leaf's box from its triangles, then up the tree. At each interior
-// node the first child to arrive stops and the second, which finds both boxes written, folds
-// them and goes on, so every box is written once and no thread waits for another.
-__global__ void refit_nodes_kernel(RefitArgs a) {
-  int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.num_nodes) return;
-  const float4 hi = a.blas[2 * (a.node_base + i) + 1];
-  const uint32_t count = __float_as_uint(hi.w);
-  if (count == 0u) return;
-  const int64_t first = __float_as_uint(hi.z);
-  if (first < a.slot_base || first + count > a.slot_base + a.num_tris) { atomicExch(a.status, 1); return; }
-  const float4* tris = a.tris;
-  auto vertex = [tris](uint32_t slot, int k, float* p) {
-    const float4 q = tris[3 * (int64_t)slot + k];
-    p[0] = q.x; p[1] = q.y; p[2] = q.z;
-  };
-  refit_store_box(a.blas, a.node_base + i, xb::refit_leaf((uint32_t)first, count, vertex), hi);
-  for (int32_t steps = 0; steps < a.num_nodes; ++steps) {
-    const int32_t p = a.parent[i];
-    if (p < 0) return;
-    __threadfence();                                   // this child's box before its arrival
-    if (atomicAdd(a.arrivals + p, 1u) != 1u) return;   // first arrival (or a malformed third)
-    __threadfence();
-    const float4 ph = a.blas[2 * (a.node_base + p) + 1];
-    const int64_t c = __float_as_uint(ph.z);
-    refit_store_box(a.blas, a.node_base + p,
-                    xb::refit_interior(refit_load_box(a.blas, c), refit_load_box(a.blas, c + 1)), ph);
-    i = p;
-  }
-  atomicExch(a.status, 2);
+__global__ void refit_nodes_kernel(xb::RefitArgs a) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.num_nodes) xb::refit_nodes_at(a, i);
 }
 
 }  // namespace
@@ -2384,9 +2308,9 @@ int xb_refit_mesh(xb_renderer* r, int32_t mesh, const float* positions, const fl
     r->refit_bytes = need;
   }
   char* base = static_cast<char*>(r->refit_mem);
-  RefitArgs a;
-  a.blas = const_cast<float4*>(r->scene.blas);
-  a.tris = const_cast<float4*>(r->scene.tris);
+  xb::RefitArgs a;
+  a.blas = reinterpret_cast<xb::Quad*>(const_cast<float4*>(r->scene.blas));
+  a.tris = reinterpret_cast<xb::Quad*>(const_cast<float4*>(r->scene.tris));
   a.tri_index = r->scene.tri_index;
   float* pos_dev = reinterpret_cast<float*>(base);
   a.pos = pos_dev;
@@ -2422,7 +2346,7 @@ int xb_refit_mesh(xb_renderer* r, int32_t mesh, const float* positions, const fl
   int32_t status = 0;
   float4 root[2];
   CK(cudaMemcpyAsync(&status, a.status, sizeof(status), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(root, a.blas + 2 * ml.node_base, sizeof(root), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(root, r->scene.blas + 2 * ml.node_base, sizeof(root), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   drop_graphs(r);
   if (status != 0)

@@ -11,6 +11,7 @@
 #include "scene_host.h"
 #include "bvh_build.h"
 #include "bvh_refit.h"
+#include "refit_kernels.h"
 
 #include <algorithm>
 #include <atomic>
@@ -18,6 +19,7 @@
 #include <cstring>
 #include <exception>
 #include <future>
+#include <stdexcept>
 #include <thread>
 
 namespace xb {
@@ -450,27 +452,46 @@ void build_tlas(const std::vector<Affine>& l2w, const std::vector<const xb_bvh_n
 }
 
 void refit_blas(const HostMesh& m, std::vector<xb_bvh_node>& nodes) {
-  // a node's children are allocated after it, so children come before parents in reverse order
-  auto vertex = [&](uint32_t slot, int k, float* p) {
-    const int v = m.indices[3 * (size_t)m.prims[slot] + k];
-    p[0] = m.vx[v]; p[1] = m.vy[v]; p[2] = m.vz[v];
-  };
-  for (size_t i = nodes.size(); i-- > 0;) {
+  // the mesh packed as the renderer uploads it (node and slot bases 0), then the device refit's
+  // passes run as loops over their thread indices (refit_kernels.h)
+  const int32_t nn = (int32_t)nodes.size(), nt = m.num_triangles();
+  if (nn == 0) return;
+  auto bits = [](uint32_t u) { float f; std::memcpy(&f, &u, sizeof(f)); return f; };
+  std::vector<Quad> blas(2 * (size_t)nn), tris(3 * (size_t)nt);
+  for (int32_t i = 0; i < nn; ++i) {
+    const xb_bvh_node& n = nodes[i];
+    blas[2 * i] = Quad{n.mn[0], n.mn[1], n.mn[2], n.mx[0]};
+    blas[2 * i + 1] = Quad{n.mx[1], n.mx[2], bits(n.child), bits(n.count)};
+  }
+  for (int32_t s = 0; s < nt; ++s) tris[3 * s].w = bits(m.prims[s]);
+  std::vector<float> pos(3 * (size_t)m.num_vertices());
+  for (int v = 0; v < m.num_vertices(); ++v) { pos[3 * v] = m.vx[v]; pos[3 * v + 1] = m.vy[v]; pos[3 * v + 2] = m.vz[v]; }
+  std::vector<int32_t> parent(nn, -1);
+  std::vector<uint32_t> arrivals(nn, 0);
+  int32_t status = 0;
+  RefitArgs a;
+  a.blas = blas.data();
+  a.tris = tris.data();
+  a.tri_index = m.indices.data();
+  a.pos = pos.data();
+  a.parent = parent.data();
+  a.arrivals = arrivals.data();
+  a.status = &status;
+  a.node_base = 0;
+  a.slot_base = 0;
+  a.num_nodes = nn;
+  a.num_tris = nt;
+  a.num_verts = m.num_vertices();
+  a.tri_offset = 0;
+  a.vtx_offset = 0;
+  for (int32_t s = 0; s < nt; ++s) refit_tris_at(a, s);
+  for (int32_t i = 0; i < nn; ++i) refit_parents_at(a, i);
+  for (int32_t i = 0; i < nn; ++i) refit_nodes_at(a, i);
+  if (status != 0) throw std::invalid_argument("refit: malformed BLAS");
+  for (int32_t i = 0; i < nn; ++i) {
     xb_bvh_node& n = nodes[i];
-    RefitBox b;
-    if (n.count > 0) {
-      b = refit_leaf(n.child, n.count, vertex);
-    } else {
-      const xb_bvh_node& l = nodes[n.child];
-      const xb_bvh_node& r = nodes[n.child + 1];
-      RefitBox lb, rb;
-      for (int k = 0; k < 3; ++k) {
-        lb.mn[k] = l.mn[k]; lb.mx[k] = l.mx[k];
-        rb.mn[k] = r.mn[k]; rb.mx[k] = r.mx[k];
-      }
-      b = refit_interior(lb, rb);
-    }
-    for (int k = 0; k < 3; ++k) { n.mn[k] = b.mn[k]; n.mx[k] = b.mx[k]; }
+    n.mn[0] = blas[2 * i].x; n.mn[1] = blas[2 * i].y; n.mn[2] = blas[2 * i].z;
+    n.mx[0] = blas[2 * i].w; n.mx[1] = blas[2 * i + 1].x; n.mx[2] = blas[2 * i + 1].y;
   }
 }
 
