@@ -2097,7 +2097,8 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   if (!v) return set_err(r, XB_E_INVALID, "xb_upload_scene: null view");
   CK(cudaStreamSynchronize(r->stream));
   free_scene(r);
-  // ── meshes: BLAS nodes (odd-aligned per mesh), slot-ordered triangles ──
+  // ── meshes: BLAS nodes (odd-aligned per mesh), slot-ordered triangles; the refit passes
+  // (refit_kernels.h, which states this layout) and the host refit's packing read it too ──
   std::vector<float4> blas, tris;
   std::vector<int32_t> tri_index, tri_mat, root_of(v->num_meshes, -1);
   std::vector<float> nx, ny, nz;
