@@ -76,6 +76,9 @@ def parse():
     ap.add_argument("--guide-fraction", type=float, default=0.0,
                     help="fixed probability of sampling the network (0: learned per vertex)")
     ap.add_argument("--guide-width", type=int, default=1280)
+    ap.add_argument("--no-incoherent", action="store_true", help="skip the incoherent-ray traversal bench")
+    ap.add_argument("--incoherent-rays", type=int, default=1 << 22)
+    ap.add_argument("--detail-out", default="", help="also write the studies' full results to this JSON file")
     ap.add_argument("--guide-height", type=int, default=720)
     return ap.parse_args()
 
@@ -194,35 +197,64 @@ class quiet_stdout:
         os.close(self.null)
 
 
-def cpu_reference_sample(desc, rays_per_path: float | None, budget_s: float, threads_note: bool = True) -> dict:
-    """The reference CPU backend on a bounded sample of the same view (fewer pixels, same camera)."""
+def shared_config(desc, level: int) -> dict:
+    """The workload, identical in the JSON lines of both arms (this one and --impl reference)."""
+    return {"workload": workload(desc, level), "scene": "config 2 (synthetic, seed 1)",
+            "width": desc.width, "height": desc.height, "min_bounces": desc.min_bounces,
+            "max_bounces": desc.max_bounces, "triangles": desc.num_triangles,
+            "l2": "GPU arm: 256 MiB written between timed steps (L2 flushed); CPU arm: not applicable"}
+
+
+def cpu_reference_run(desc, steps: int, warmup: int, step_seconds: float) -> dict:
+    """The reference's CPU backend (render_frame_tiled from oracle/_ref, Release flags, every
+    host thread) on 1/64 of the view's pixels (the same camera): `warmup` untimed and `steps`
+    timed calls, each of the samples per pixel that fill about `step_seconds` (at most 256), so
+    that thread-pool start-up is a small part of each call. Loads no library of this package."""
     from oracle import ref
-    if not ref.available("fast"):
-        return {"value": None, "unit": "Mrays/s", "cores": None, "kind": "reference",
-                "sample": "oracle/_ref/libxnref_fast.so not built"}
     L = ref.lib("fast")
     cores = int(L.xr_hardware_threads())
     w, h = desc.width // 8, desc.height // 8
     rs = ref.RefScene(desc, flavour="fast")
     rr = ref.RefRenderer(w, h, desc.min_bounces, desc.max_bounces, flavour="fast")
-    _, t1 = rr.render(rs, desc.eye, desc.target, desc.fov, 1, 1)
-    spp = int(max(1, min(256, budget_s / max(t1, 1e-3))))
-    _, secs = rr.render(rs, desc.eye, desc.target, desc.fov, 2, spp)
-    paths = w * h * spp
-    msps = paths / secs / 1e6
-    out = {"unit": "Mrays/s", "cores": cores, "kind": "reference",
-           "msamples_per_s": msps, "seconds": secs,
-           "sample": f"{w}x{h} px (1/64 of the pixels, same camera) x {spp} spp of config 2, "
-                     f"render_frame_tiled with Release flags on {cores} threads; Mrays/s = Msamples/s x "
-                     f"rays per path measured on the GPU for this config (derived: the reference counts no rays)"}
-    out["value"] = msps * rays_per_path if rays_per_path else None
-    return out
+    _, t1 = rr.render(rs, desc.eye, desc.target, desc.fov, 1, 4)
+    spp = int(max(1, min(256, step_seconds / max(t1 / 4, 1e-4))))
+    first = 100
+    for s in range(warmup):
+        rr.render(rs, desc.eye, desc.target, desc.fov, first, spp)
+        first += spp
+    secs = 0.0
+    for s in range(steps):
+        _, t = rr.render(rs, desc.eye, desc.target, desc.fov, first, spp)
+        first += spp
+        secs += t
+    msps = w * h * spp * steps / secs / 1e6
+    return {"cores": cores, "msamples_per_s": msps, "seconds": secs, "spp_per_step": spp,
+            "ms_per_step": secs * 1e3 / steps, "pixels": (w, h), "scene": rs,
+            "sample": f"{w}x{h} px (1/64 of the pixels, same camera) x {spp} spp per call, "
+                      f"render_frame_tiled with Release flags on {cores} threads"}
 
 
-def rays_per_path_port(desc, paths: int = 4096) -> float:
-    """Rays per path of this estimator, counted by the CPU restatement (oracle/) on a sample."""
-    from oracle import port
-    return port.rays_per_path(desc, paths)
+def rays_per_path_oracle(desc, rs) -> float:
+    """Rays per path of this estimator (closest + shadow), counted by the CPU restatement
+    (oracle/port.py) on the reference-built scene `rs` and the reference's camera: the
+    reference counts no rays, so its Mrays/s is derived from this count."""
+    from oracle import port, ref
+    cam = ref.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
+    return port.rays_per_path(rs.view(), cam, desc.width, desc.height, desc.min_bounces, desc.max_bounces)
+
+
+def cpu_reference_sample(desc, rays_per_path: float, budget_s: float) -> dict:
+    """cpu_baseline of this arm: the reference CPU backend for about budget_s seconds; its
+    Mrays/s uses the rays per path this GPU run measured."""
+    from oracle import ref
+    if not ref.available("fast"):
+        return {"value": None, "unit": "Mrays/s", "cores": None, "kind": "reference",
+                "sample": "oracle/_ref/libxnref_fast.so not built"}
+    run = cpu_reference_run(desc, steps=3, warmup=0, step_seconds=budget_s / 3)
+    return {"value": run["msamples_per_s"] * rays_per_path, "unit": "Mrays/s", "cores": run["cores"],
+            "kind": "reference", "msamples_per_s": run["msamples_per_s"], "seconds": run["seconds"],
+            "sample": run["sample"] + "; Mrays/s = Msamples/s x rays per path measured on the GPU "
+                                      "for this config (derived: the reference counts no rays)"}
 
 
 def run_reference(args):
@@ -242,35 +274,25 @@ def reference_line(args) -> dict:
     desc = scenes.icosphere_scene(level=args.level, width=args.width, height=args.height)
     if not ref.available("fast"):
         return {"impl": "reference", "unavailable": "oracle/_ref/libxnref_fast.so was not built"}
-    try:
-        rpp = rays_per_path_port(desc)
-    except Exception as e:  # the restatement is missing: report samples only
-        rpp = None
-    L = ref.lib("fast")
-    cores = int(L.xr_hardware_threads())
-    w, h = desc.width // 8, desc.height // 8
-    rs = ref.RefScene(desc, flavour="fast")
-    rr = ref.RefRenderer(w, h, desc.min_bounces, desc.max_bounces, flavour="fast")
-    spp_per_step = 1
-    for s in range(args.warmup):
-        rr.render(rs, desc.eye, desc.target, desc.fov, 1 + s, spp_per_step)
-    secs = 0.0
-    for s in range(args.steps):
-        _, t = rr.render(rs, desc.eye, desc.target, desc.fov, 1000 + s, spp_per_step)
-        secs += t
-    paths = w * h * spp_per_step * args.steps
-    msps = paths / secs / 1e6
-    value = msps * rpp if rpp else msps
-    unit = "Mrays/s" if rpp else "Msamples/s"
+    # each step about 1 s of CPU work (less when many steps are asked for), whole run within minutes
+    step_s = min(1.0, 150.0 / max(args.steps + args.warmup, 1))
+    run = cpu_reference_run(desc, args.steps, args.warmup, step_s)
+    rpp = rays_per_path_oracle(desc, run["scene"])
+    msps = run["msamples_per_s"]
+    value = msps * rpp
+    unit = "Mrays/s"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": unit, "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": run["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": workload(desc, args.level), "sample_per_step": f"{w}x{h} px x {spp_per_step} spp (1/64 of the pixels)",
-                       "rays_per_path": rpp, "msamples_per_s": msps},
-            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "reference",
-                             "sample": f"{w}x{h} px x {spp_per_step} spp per step, render_frame_tiled, Release flags, {cores} threads"},
-            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic (seeded procedural scene, seed 1)",
+            "config": shared_config(desc, args.level),
+            "cpu_baseline": {"value": value, "unit": unit, "cores": run["cores"], "kind": "reference",
+                             "sample": run["sample"] + " per step"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "detail": {"msamples_per_s": msps, "rays_per_path": rpp,
+                       "rays_per_path_source": "oracle/ restatement on the reference-built scene (derived: "
+                                               "the reference counts no rays)",
+                       "spp_per_step": run["spp_per_step"], "pixels": run["pixels"]}}
     return line
 
 
@@ -283,7 +305,7 @@ def guiding_study(args, device: int) -> dict:
     import xenon_b200 as xb
     from xenon_b200 import scenes
     W, H = args.guide_width, args.guide_height
-    desc = scenes.guiding_room(level=7, width=W, height=H)
+    desc = scenes.guiding_room(width=W, height=H)
     hs = xb.HostScene.from_desc(desc)
     cam = xb.camera(desc.eye, desc.target, desc.fov, W / H)
     eps = 1e-2
@@ -351,8 +373,8 @@ def guiding_study(args, device: int) -> dict:
 
     plain = equal_time(False)
     guided = equal_time(True)
-    return {"workload": "config4: closed room, light above a baffle, smooth glass icosphere L7 "
-                        f"(327,680 tris), {W}x{H}, depth 16",
+    return {"workload": "config4: closed room, light above a baffle, smooth glass geodesic sphere "
+                        f"({desc.meshes[-1].indices.shape[0]:,} tris), {W}x{H}, depth 16",
             "tuning": {"plain": tuned or "defaults", "guided": tuned_g or "defaults"},
             "budget_device_s": args.guide_seconds, "reference": {"spp": done, "device_ms": ref_ms,
                                                                "image_mean": float(ref.mean()),
@@ -490,6 +512,121 @@ def views_study(args, device: int) -> dict:
             "reference": "plain renders of the same views with 4x the samples", "per_view": per_view}
 
 
+def _sig(x, digits: int = 4):
+    """x rounded to `digits` significant digits (keeps the JSON line short)."""
+    if not isinstance(x, float) or x == 0.0 or not np.isfinite(x):
+        return x
+    return float(f"{x:.{digits}g}")
+
+
+def config3_summary(c):
+    if not c or "error" in c:
+        return c
+    return {"workload": "config3", "mrays_per_s": _sig(c["mrays_per_s"]), "msamples_per_s": _sig(c["msamples_per_s"]),
+            "ms_per_spp": _sig(c["ms_per_spp"])}
+
+
+def incoherent_summary(inc):
+    """Mrays/s per scene and batch in the JSON line (the full figures go to --detail-out)."""
+    if not inc or "error" in inc:
+        return inc
+    out = {"rays": inc["rays_per_batch"]}
+    for sc in ("config2", "config3"):
+        out[sc] = {k: _sig(v["mrays_per_s"]) for k, v in inc[sc].items()}
+    return out
+
+
+def views_summary(v):
+    """The config-5 figures kept in the JSON line (the per-view list goes to --detail-out)."""
+    if not v or "error" in v:
+        return v
+    keep = ("guided_msamples_per_s", "plain_batched_msamples_per_s", "plain_one_by_one_msamples_per_s",
+            "relmse_ratio_plain_over_guided_median", "relmse_ratio_plain_over_guided_median_trimmed",
+            "relmse_ratio_equal_time_median_trimmed")
+    return {"workload": "config5: 32 views of config 3", **{k: _sig(v[k]) for k in keep}}
+
+
+def guiding_summary(g):
+    """The config-4 figures kept in the JSON line: equal-time relMSE of plain and guided against
+    the 16k-spp FP64 reference, their ratios, and what each method rendered in the budget."""
+    if not g or "error" in g:
+        return g
+    p, q = g["plain"], g["guided"]
+    return {"workload": g["workload"], "budget_device_s": g["budget_device_s"], "reference_spp": g["reference"]["spp"],
+            "ratio_raw": _sig(g["relmse_ratio_plain_over_guided"]),
+            "ratio_reference_noise_removed": _sig(g["relmse_ratio_reference_noise_removed"]),
+            "ratio_trimmed": _sig(g["relmse_ratio_trimmed"]),
+            "relmse_plain": _sig(p["relmse"]), "relmse_guided": _sig(q["relmse"]),
+            "spp_plain": p["spp"], "spp_guided": q["spp"], "train_ms": _sig(q.get("train_phase_ms", 0.0)),
+            "mean_plain": _sig(p["image_mean"], 6), "mean_guided": _sig(q["image_mean"], 6),
+            "mean_reference": _sig(g["reference"]["image_mean"], 6)}
+
+
+def incoherent_study(args, device: int) -> dict:
+    """Traversal alone on incoherent rays: 2^22 rays with origins uniform in the scene's world
+    bounds and directions uniform on the sphere, and 2^22 secondary rays harvested from bounce 2
+    of the path tracer's own sampling (xenon_b200/raybatch.py), traced through
+    xb_trace_rays_device (closest hit, then any hit) on config 2 and config 3. Device Mrays/s
+    from CUDA events around each launch on the launching stream; inputs and hit records
+    (128 MiB + 256 MiB per batch) exceed the L2."""
+    import torch
+    import xenon_b200 as xb
+    from xenon_b200 import abi, raybatch, scenes
+    out = {}
+    n = args.incoherent_rays
+    for name, make in (("config2", lambda: scenes.icosphere_scene(level=args.level)),
+                       ("config3", lambda: scenes.instanced_grid())):
+        desc = make()
+        hs = xb.HostScene.from_desc(desc)
+        r = xb.Renderer(64, 64, desc.max_bounces, desc.min_bounces, device=device)
+        r.upload_scene(hs)
+        view = hs.view()
+        cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
+        batches = {"uniform": raybatch.incoherent_rays(view, n, seed=5),
+                   "bounce2": raybatch.secondary_rays(r, desc.materials, cam, desc.width, desc.height, n,
+                                                      seed=6, bounce=2)}
+        res = {}
+        stream = torch.cuda.current_stream()
+        for bname, rays in batches.items():
+            d_rays = torch.from_numpy(rays.view(np.uint8).reshape(-1)).to("cuda")
+            d_hits = torch.empty(len(rays) * abi.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+            for mode, mname in ((abi.XB_TRACE_CLOSEST, "closest"), (abi.XB_TRACE_ANY, "any")):
+                def launch():
+                    r.trace_rays_device(d_rays.data_ptr(), len(rays), d_hits.data_ptr(), mode, stream.cuda_stream)
+                for _ in range(2):
+                    launch()
+                r.reset_profile()
+                launch()
+                torch.cuda.synchronize()
+                pr = r.profile()
+                if mode == abi.XB_TRACE_CLOSEST:
+                    nodes, tris, tl, inst = pr.ext_blas_nodes, pr.ext_tris, pr.ext_tlas_nodes, pr.ext_instances
+                else:
+                    nodes, tris, tl, inst = pr.sh_blas_nodes, pr.sh_tris, pr.sh_tlas_nodes, pr.sh_instances
+                bpr = (64 * nodes + 48 * tris + 32 * tl + 48 * inst) / len(rays) + 32 + 64
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                reps = 5
+                ms = 0.0
+                for _ in range(reps):
+                    torch.cuda.synchronize()
+                    ev[0].record(stream)
+                    launch()
+                    ev[1].record(stream)
+                    torch.cuda.synchronize()
+                    ms += ev[0].elapsed_time(ev[1])
+                ms /= reps
+                hits = d_hits.cpu().numpy().view(abi.HIT_DTYPE)
+                res[f"{bname}_{mname}"] = {"mrays_per_s": len(rays) / ms / 1e3, "ms": ms,
+                                           "algorithmic_bytes_per_ray": bpr,
+                                           "achieved_gbs": bpr * len(rays) / ms / 1e6,
+                                           "hit_fraction": float(np.isfinite(hits["t"]).mean()),
+                                           "blas_nodes_per_ray": nodes / len(rays), "tris_per_ray": tris / len(rays)}
+            del d_rays, d_hits
+        r.close()
+        out[name] = res
+    return {"rays_per_batch": n, "entry": "xb_trace_rays_device (64-byte xb_hit records)", **out}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -577,12 +714,14 @@ def main():
                          prof.shadow_launches + prof.accumulate_launches) / n_prof
     launches = launches_per_step * args.steps
 
-    # roofline of the extend kernel: algorithmic bytes per launch / mean launch time
+    # Roofline of the extend kernel: its algorithmic bytes ÷ the time during which at least one
+    # of its launches ran (the union of the launch intervals over all wave lanes, which cannot
+    # exceed the step), from the same steps run again with stage timing.
     peaks = load_peaks()
     ext_bytes = ext_bytes_per_ray * pst.rays_closest
-    ext_launch_ms = prof.extend_ms / max(prof.extend_launches, 1)
-    ext_bytes_per_launch = ext_bytes / max(prof.extend_launches, 1)
-    achieved = ext_bytes_per_launch / (ext_launch_ms * 1e-3) / 1e9
+    ext_busy_ms = prof.extend_busy_ms
+    achieved = ext_bytes / (ext_busy_ms * 1e-3) / 1e9
+    step_avg = ext_bytes / n_prof / (t_max / args.steps * 1e-3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "extend_kernel_config2.json")
     if os.path.exists(tp):
@@ -591,7 +730,7 @@ def main():
         if tj.get("dram_bytes_per_closest_ray"):
             traffic = tj["dram_bytes_per_closest_ray"] * pst.rays_closest / max(prof.extend_launches, 1)
     # the same kernel with one wave in flight (untimed pass): its launches then have the GPU to
-    # themselves, while in the timed region the other lane's kernels run beside them
+    # themselves, while in the timed region the other lanes' kernels run beside them
     lanes = r.tuning()["waves"]
     one_lane = None
     if lanes > 1:
@@ -604,7 +743,7 @@ def main():
             torch.cuda.synchronize()
             r.render_range(cam, base + (args.warmup + args.steps + n_prof + s) * sps, sps)
         p1 = r.profile()
-        a1 = ext_bytes_per_ray * r.stats().rays_closest / max(p1.extend_ms * 1e-3, 1e-12) / 1e9
+        a1 = ext_bytes_per_ray * r.stats().rays_closest / max(p1.extend_busy_ms * 1e-3, 1e-12) / 1e9
         one_lane = {"achieved": a1, "frac": a1 / peaks["hbm_gbs"], "extend_ms_per_launch":
                     p1.extend_ms / max(p1.extend_launches, 1)}
         r.set_tuning(waves=lanes)
@@ -612,14 +751,17 @@ def main():
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                 "peak_source": peaks["source"], "kernel": "extend_kernel (closest-hit traversal)",
                 "algorithmic_bytes_per_ray": ext_bytes_per_ray,
-                "extend_launch_ms_per_step": prof.extend_ms / n_prof, "waves_in_flight": lanes,
-                "timing": f"events around each launch over {n_prof} steps of the timed workload run again "
-                          "with stage timing (the timed steps replay captured graphs); the profiled steps "
-                          f"took {prof_ms / n_prof:.3f} ms each against {dev_ms / args.steps:.3f} in the "
-                          "timed region" + (f"; with {lanes} waves in flight each extend launch shares the "
-                                            "GPU with the other lanes' kernels, so its duration includes "
-                                            "that sharing; one_lane is the same kernel with one wave in "
-                                            "flight" if lanes > 1 else ""),
+                "algorithmic_bytes_per_launch": ext_bytes / max(prof.extend_launches, 1),
+                "extend_busy_ms_per_step": ext_busy_ms / n_prof,
+                "extend_launch_ms_per_step": prof.extend_ms / n_prof,
+                "profiled_ms_per_step": prof_ms / n_prof, "ms_per_step": t_max / args.steps,
+                "step_average_achieved": step_avg, "waves_in_flight": lanes,
+                "timing": "algorithmic bytes / extend busy time: the union of the extend launches' intervals "
+                          f"(CUDA events around each launch) over {n_prof} steps of the timed workload run again "
+                          "with stage timing (the timed steps replay captured graphs, inside which no event "
+                          "times one launch); extend_launch_ms_per_step sums the launches' own durations, "
+                          "which overlap across wave lanes; step_average_achieved divides by the whole "
+                          "timed step instead",
                 "one_lane": one_lane, **work}
 
     # e2e through the public API with host buffers: render + resolve to pinned host memory
@@ -683,6 +825,12 @@ def main():
             views = views_study(args, local)
         except Exception as e:
             views = {"error": f"{type(e).__name__}: {e}"}
+    incoherent = None
+    if rank == 0 and ws == 1 and not args.no_incoherent:
+        try:
+            incoherent = incoherent_study(args, local)
+        except Exception as e:
+            incoherent = {"error": f"{type(e).__name__}: {e}"}
     guiding = None
     if rank == 0 and ws == 1 and not args.no_guiding_study:
         try:
@@ -691,19 +839,26 @@ def main():
             guiding = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
+        detail = {"spp_per_step": sps, "paths_per_step": npix * sps, "rays_per_path": rays_per_path,
+                  "msamples_per_s": msamples, "parallelism": f"sample-sharded x{ws}" if ws > 1 else "1 GPU",
+                  "tuning": r.tuning(), "tuning_source": "xenon_b200/tuning (autotuner)" if tuned else "defaults",
+                  "stage_ms_per_step_profiled": {k: getattr(prof, k) / n_prof for k in
+                                                 ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms",
+                                                  "accumulate_ms", "extend_busy_ms", "shade_busy_ms",
+                                                  "shadow_busy_ms")}}
+        studies = {"config3": config3_summary(config3), "incoherent": incoherent_summary(incoherent),
+                   "views": views_summary(views), "guiding": guiding_summary(guiding)}
+        if args.detail_out:
+            with open(args.detail_out, "w") as f:
+                json.dump({"detail": detail, "config3": config3, "incoherent": incoherent, "views": views,
+                           "guiding": guiding}, f, indent=1)
         line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded procedural scene, seed 1)",
-                "config": {"workload": workload(desc, args.level), "spp_per_step": sps, "paths_per_step": npix * sps,
-                           "rays_per_path": rays_per_path,
-                           "msamples_per_s": msamples, "l2": "flushed between timed steps (256 MiB write)",
-                           "parallelism": f"sample-sharded x{ws}" if ws > 1 else "1 GPU",
-                           "tuning": r.tuning(), "tuning_source": "xenon_b200/tuning (autotuner)" if tuned else "defaults",
-                           "stage_ms_per_step_profiled": {k: getattr(prof, k) / n_prof for k in
-                                                 ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms", "accumulate_ms")}},
+                "config": shared_config(desc, args.level), "detail": detail,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clk.summary(), "config3": config3, "guiding": guiding, "views": views}
+                "clocks": clk.summary(), **studies}
         print(json.dumps(line))
     r.close()
     if ws > 1:

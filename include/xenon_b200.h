@@ -304,8 +304,12 @@ int  xb_upload_scene(xb_renderer *r, const xb_scene_view *view);
  * to keep the uploaded ones. Meshes that carry area lights are refused (XB_E_UNSUPPORTED: their
  * emitter geometry is built on the host at upload; refit the host scene and upload again).
  * Synchronises the render stream; captured bounce graphs are rebuilt on the next render. The
- * accumulated image is kept: call xb_reset for frames of a moving scene. No reference
- * counterpart: the reference rebuilds its BLAS on the host (src/geometry/blas.cpp:183-205). */
+ * arrays are rewritten in place, so ray queries issued on caller streams (xb_trace_rays_device,
+ * xb_trace_rays_noalloc) must have finished before this call. If the uploaded BLAS turns out to
+ * be malformed (XB_E_INVALID), some of it has already been rewritten: the renderer then holds no
+ * scene (later calls fail with XB_E_STATE) until the scene is uploaded again. The accumulated
+ * image is kept: call xb_reset for frames of a moving scene. No reference counterpart: the
+ * reference rebuilds its BLAS on the host (src/geometry/blas.cpp:183-205). */
 int  xb_refit_mesh(xb_renderer *r, int32_t mesh, const float *positions, const float *normals);
 int  xb_set_bounces(xb_renderer *r, int32_t min_bounces, int32_t max_bounces);
 /* Adds spp_to_add samples per pixel; sample k of pixel p is seeded exactly as the CPU backend
@@ -433,6 +437,10 @@ typedef struct xb_profile {
   /* guiding: record finalisation and network training after training waves */
   double train_ms;
   int64_t train_launches;
+  /* the time during which at least one launch of the stage was running: the union of its launch
+   * intervals over all wave lanes and streams (the *_ms sums above count overlapping launches
+   * of several lanes once each, so they can exceed the call's duration; these cannot) */
+  double extend_busy_ms, shade_busy_ms, shadow_busy_ms;
 } xb_profile;
 int  xb_set_profiling(xb_renderer *r, int32_t flags);
 int  xb_get_profile(const xb_renderer *r, xb_profile *out);
@@ -450,12 +458,15 @@ int  xb_trace_rays_device(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit 
 /* Same as xb_trace_rays_device, but the call allocates nothing (no cudaMalloc, cudaFree or
  * allocating library routine): for callers that cannot allocate device memory while they trace,
  * e.g. a plugin whose host application owns all device memory (its own allocator, or a fixed
- * budget set at start-up). Its scratch (ray cursor, count, overflow counter) is a
- * fixed 256-byte device array inside the library, shared by every call: calls that overlap on
- * the GPU race on it, so issue them on one stream or otherwise one at a time. The first call on a
- * device looks up that array's address (cudaGetSymbolAddress, once per device, with the device
- * current); make that first call before any stream capture. Batches above 2^31 - 65 rays are
- * rejected with XB_E_INVALID. It has no counterpart in the reference. */
+ * budget set at start-up). Its scratch (the 64-bit ray cursor and the ray count) is a fixed
+ * 256-byte device array inside the library, shared by every call and cleared at the start of
+ * each: calls that overlap on the GPU race on it, so issue them on one stream or otherwise one at
+ * a time. The first call on a device looks up that array's address (cudaGetSymbolAddress, once
+ * per device, with the device current); make that first call before any stream capture. Batches
+ * above XB_NOALLOC_MAX_RAYS rays are rejected with XB_E_INVALID. Threads whose traversal stack
+ * overflowed (their rays may have lost a hit) are added to the renderer's overflow count
+ * (xb_get_render_stats), as for xb_trace_rays_device. It has no counterpart in the reference. */
+#define XB_NOALLOC_MAX_RAYS ((int64_t)1 << 40)
 int  xb_trace_rays_noalloc(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit *hits,
                            int32_t mode, void *stream);
 

@@ -112,15 +112,16 @@ def seed_pcg(seed: int) -> int:
     return int(lib().xo_seed_pcg(seed))
 
 
-def rays_per_path(desc, paths: int = 4096) -> float:
-    """Closest + shadow rays per path of the estimator on a sample of the scene's view."""
-    from xenon_b200 import HostScene, camera
-    hs = HostScene.from_desc(desc)
-    ps = PortScene(hs.view())
+def rays_per_path(view, cam, width: int, height: int, min_bounces: int, max_bounces: int,
+                  paths: int = 4096) -> float:
+    """Closest + shadow rays per path of the estimator on a coarse grid over a view: `view` is an
+    xb_scene_view (e.g. the reference-built one, oracle/ref.py RefScene.view()) and `cam` the
+    camera's four vectors (eye, lower-left, horizontal, vertical: float[12], e.g. oracle/ref.py
+    camera()) for a width x height image."""
+    from xenon_b200.abi import Camera
+    ps = PortScene(view)
     side = max(8, int(paths ** 0.5))
-    cam = camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
-    # a coarse grid over the same view: scale the camera to side x side pixels
     w = side
-    h = max(1, int(side * desc.height / desc.width))
-    _, rays = ps.render(cam, w, h, desc.min_bounces, desc.max_bounces, 7, 1)
+    h = max(1, int(side * height / width))
+    _, rays = ps.render(Camera.from_array(cam), w, h, min_bounces, max_bounces, 7, 1)
     return float(rays.sum()) / (w * h)

@@ -6,7 +6,9 @@ is computed by the reference itself (oracle/_ref/libxnref_strict.so: its BLAS/TL
 Scene::intersect / intersects, bsdf_eval_for_nee / bsdf_pdf_for_nee / bsdf_sample,
 Camera::look_at, material_prepare, the .xenon / .mat loaders and render_frame_tiled), and for
 the output stage its ImageNoiseEstimator and save_image's 8-bit conversion (output.npz; run
-`python tests/golden/gen_golden.py output` to write that file alone).
+`python tests/golden/gen_golden.py output` to write that file alone). The converged config-1
+image at 256x256 and 16k samples (config1_256.npz) takes minutes: `... gen_golden.py config1`
+writes it alone.
 Inputs are this repo's seeded procedural scenes (xenon_b200/scenes.py), so the files are
 reproducible: `python tests/golden/gen_golden.py`.
 """
@@ -178,7 +180,24 @@ def output_stage():
     print("output-stage vectors written to", HERE)
 
 
+def config1_converged():
+    """Config 1 at its own size, converged: the reference's render of the 256x256 Cornell box
+    over samples 1..16384 (FP64 sums, strict build; about five minutes on eight cores), stored as
+    the float32 mean image (top-down rows)."""
+    desc = scenes.cornell()
+    spp = 16384
+    rr = ref.RefRenderer(desc.width, desc.height, desc.min_bounces, desc.max_bounces)
+    s, secs = rr.render(ref.RefScene(desc), desc.eye, desc.target, desc.fov, 1, spp)
+    np.savez_compressed(os.path.join(HERE, "config1_256.npz"), mean=(s / spp).astype(np.float32),
+                        spp=np.array(spp), seconds=np.array(secs))
+    print(f"config-1 16k-spp reference written ({secs:.0f} s)")
+
+
 if __name__ == "__main__":
+    if sys.argv[1:] == ["config1"]:
+        config1_converged()
+        sys.exit(0)
     if sys.argv[1:] != ["output"]:
         main()
+        config1_converged()
     output_stage()

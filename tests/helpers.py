@@ -70,3 +70,43 @@ def compare_hits(got: np.ndarray, want: np.ndarray, max_ulp: int = 4, prim_ids: 
     for k in ("normal", "geo_normal", "pos"):
         out[k + "_maxabs"] = float(np.abs(got[k][both] - want[k][both]).max()) if both.any() else 0.0
     return out
+
+
+def deep_chain_scene(depth: int = 100, seed: int = 3):
+    """A one-mesh scene whose BLAS is a chain of `depth` interior nodes, every node with the
+    mesh's bounding box: interior node 2k has children 2k+1 (a one-triangle leaf) and 2k+2 (the
+    next interior node; the last one's children are two leaves). Both children of every node are
+    entered at the same t, so the traversal continues into the right child (the reference's
+    order for equal entry distances, blas.cpp:242-262) and pushes the leaf: a ray through the box
+    needs `depth` stack entries, more than the 64 the traversal holds when depth > 64.
+    Returns (host scene, its view with the chain BLAS, rays through the box)."""
+    import ctypes
+
+    from xenon_b200 import HostScene
+    rng = np.random.default_rng(seed)
+    ntri = depth + 1
+    base = rng.random((ntri, 3)).astype(np.float32)
+    pos = np.repeat(base, 3, axis=0) + (rng.random((3 * ntri, 3)) * 0.05).astype(np.float32)
+    desc = scenes.SceneDesc()
+    desc.add_material("m", abi.material())
+    desc.add_mesh(scenes.MeshDesc(positions=pos.astype(np.float32),
+                                  indices=np.arange(3 * ntri, dtype=np.int32).reshape(ntri, 3)))
+    hs = HostScene.from_desc(desc)
+    v = hs.view()
+    mn, mx = pos.min(0), pos.max(0)
+    nodes = np.zeros(2 * depth + 1, abi.NODE_DTYPE)
+    nodes["mn"], nodes["mx"] = mn, mx
+    for k in range(depth):
+        nodes[2 * k]["child"] = 2 * k + 1
+        nodes[2 * k + 1]["child"], nodes[2 * k + 1]["count"] = k, 1
+    nodes[2 * depth]["child"], nodes[2 * depth]["count"] = depth, 1
+    prims = np.arange(ntri, dtype=np.uint32)
+    mv = v.meshes[0]
+    mv.blas_nodes = nodes.ctypes.data
+    mv.num_blas_nodes = len(nodes)
+    mv.blas_prims = prims.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+    v._chain = (nodes, prims)          # the view points into these arrays
+    n = 4096
+    org = np.stack([np.full(n, mn[0] - 1.0), rng.uniform(mn[1], mx[1], n), rng.uniform(mn[2], mx[2], n)], 1)
+    rays = abi.make_rays(org.astype(np.float32), np.tile(np.float32([1, 0, 0]), (n, 1)))
+    return hs, v, rays

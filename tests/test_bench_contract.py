@@ -46,3 +46,24 @@ def test_reference_arm_prints_one_contract_line(ref):
 def test_reference_arm_other_ranks_exit_quietly():
     p = _run(SMALL, {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert p.returncode == 0 and p.stdout.strip() == ""
+
+
+def test_reference_arm_loads_no_library_of_this_package(ref):
+    """The reference arm times the reference alone: no library built from this package's sources
+    (xenon_b200/lib) is loaded into its process, and its `config` is the GPU arm's."""
+    if not ref.available("fast"):
+        pytest.skip("oracle/_ref fast flavour not built")
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference'] + " + repr(SMALL) + "\n"
+            "import bench\n"
+            "from xenon_b200 import scenes\n"
+            "a = bench.parse()\n"
+            "with bench.quiet_stdout():\n"
+            "    line = bench.reference_line(a)\n"
+            "desc = scenes.icosphere_scene(level=a.level, width=a.width, height=a.height)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print(json.dumps({'loaded': 'libxenon_b200' in maps, 'ref': 'libxnref_fast' in maps,\n"
+            "                  'same_config': line['config'] == bench.shared_config(desc, a.level)}))\n")
+    p = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    res = json.loads(p.stdout.strip().splitlines()[-1])
+    assert res == {"loaded": False, "ref": True, "same_config": True}, res

@@ -73,3 +73,23 @@ def test_empty_and_degenerate_batches(ref):
         w = rs.trace(rays, mode)
         assert np.array_equal(np.isfinite(h["t"]), np.isfinite(w["t"])), (mode, h["t"], w["t"])
         assert np.array_equal(h["prim_id"], w["prim_id"]) and np.array_equal(h["instance_id"], w["instance_id"])
+
+
+@pytest.mark.gpu
+def test_stack_overflow_is_reported():
+    """A BLAS deeper than the 64-entry traversal stack: xb_trace_rays reports XB_E_OVERFLOW
+    (the hit may be lost) instead of writing past the stack."""
+    import xenon_b200 as xb
+    from tests.helpers import deep_chain_scene
+    hs, view, rays = deep_chain_scene(depth=100)
+    r = Renderer(16, 16)
+    r.upload_scene(view)
+    with pytest.raises(xb.XenonError) as e:
+        r.trace_rays(rays, abi.XB_TRACE_CLOSEST)
+    assert e.value.code == abi.XB_E_OVERFLOW
+    # a chain the stack holds traces without overflow
+    hs2, view2, rays2 = deep_chain_scene(depth=40)
+    r2 = Renderer(16, 16)
+    r2.upload_scene(view2)
+    h = r2.trace_rays(rays2, abi.XB_TRACE_CLOSEST)
+    assert np.isfinite(h["t"]).any()

@@ -17,12 +17,13 @@ def test_config2_scene_shape():
 
 
 def test_config4_room_shape():
-    d = scenes.guiding_room(level=7)
+    d = scenes.guiding_room()
     assert (d.width, d.height, d.max_bounces) == (1280, 720, 16)
     # the only light: two triangles covering 0.5 % of the 10 x 10 ceiling
     area = sum(l[3] for l in d.lights)
     assert len(d.lights) == 2 and abs(area / (10.0 * 10.0) - 0.005) < 1e-9
-    assert _tris(d) - 18 == 327_680              # the level-7 sphere (20 * 4^7) + 9 quads: walls, baffle, light
+    assert _tris(d) - 18 == 499_280              # the geodesic sphere (20 * 158^2) + 9 quads: walls, baffle, light
+    assert _tris(scenes.guiding_room(level=7)) - 18 == 327_680   # the level-7 icosphere form (20 * 4^7)
     glass = [m for m in d.materials if m[abi.MATERIAL_FIELDS["transmission"]] == 1.0]
     assert len(glass) == 1 and glass[0][abi.MATERIAL_FIELDS["ior"]] == np.float32(1.5)
     assert d.sky[10] == 0.0                      # closed room: the sky's intensity is zero

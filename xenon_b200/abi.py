@@ -170,7 +170,8 @@ class Profile(ctypes.Structure):
                                               "shadow_launches", "accumulate_launches",
                                               "ext_blas_nodes", "ext_tris", "ext_tlas_nodes", "ext_instances",
                                               "sh_blas_nodes", "sh_tris", "sh_tlas_nodes", "sh_instances")] + \
-               [("train_ms", ctypes.c_double), ("train_launches", ctypes.c_int64)]
+               [("train_ms", ctypes.c_double), ("train_launches", ctypes.c_int64)] + \
+               [(k, ctypes.c_double) for k in ("extend_busy_ms", "shade_busy_ms", "shadow_busy_ms")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

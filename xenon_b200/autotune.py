@@ -132,7 +132,7 @@ if __name__ == "__main__":
     elif a.workload == "config1":
         desc = scenes.cornell()
     elif a.workload in ("config4", "config4g"):
-        desc = scenes.guiding_room(level=7)
+        desc = scenes.guiding_room()
     else:
         desc = scenes.instanced_grid()
     hs = xb.HostScene.from_desc(desc)

@@ -173,6 +173,7 @@ struct xb_renderer {
   std::vector<cudaEvent_t> ev_pool;          // event pairs, reused each call
   std::vector<int> ev_stage;                 // stage of each recorded pair
   size_t ev_used = 0;
+  double stage_busy_ms[6] = {0, 0, 0, 0, 0, 0};
   double stage_ms[6] = {0, 0, 0, 0, 0, 0};      // raygen, extend, shade, shadow, accumulate, train
   int64_t stage_launches[6] = {0, 0, 0, 0, 0, 0};
   // learned path guiding
@@ -1239,37 +1240,42 @@ __global__ void bsdf_sample_kernel(DevMaterial m, int64_t n, const float* wo, ui
 // ── trace without allocation (xb_trace_rays_noalloc) ─────────────────────────────
 // Some callers cannot call cudaMalloc while they trace: a plugin whose host application owns
 // every device allocation (its own allocator, or a fixed memory budget set at start-up).
-// For them the work-stealing trace keeps its scratch (the ray cursor, the ray count and an
-// overflow counter) in this fixed file-scope array instead of renderer-allocated memory. It is
-// 256 bytes; every GPU that loads the library holds one copy until the process exits.
-constexpr int kNoAllocScratchWords = 32;
-constexpr int64_t kNoAllocMaxRays = (int64_t)0x7fffffff - 64;   // the cursor is a 32-bit int
-static __device__ __align__(256) int32_t g_noalloc_scratch[2 * kNoAllocScratchWords];
+// For them the work-stealing trace keeps its scratch (the ray cursor and the ray count) in this
+// fixed file-scope array instead of renderer-allocated memory. It is 256 bytes; every GPU that
+// loads the library holds one copy until the process exits.
+//
+// The cursor is 64-bit: every warp's last fetch moves it 32 past the end, so it can run up to
+// n + 32 × (warps in the grid) — under 2^40 + 2^36 for any batch this entry point accepts and
+// any grid it launches (fewer than 2^31 warps), far from wrapping.
+constexpr int kNoAllocScratchWords = 32;                       // 64-bit words: 256 bytes
+constexpr int64_t kNoAllocMaxRays = XB_NOALLOC_MAX_RAYS;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocScratchWords];
 
-__global__ void noalloc_begin_kernel(int32_t* scratch, int32_t n) {
-  // every call starts from a cleared cursor and counters: the array keeps the last call's values
-  if (threadIdx.x < 2 * kNoAllocScratchWords) scratch[threadIdx.x] = 0;
-  if (threadIdx.x == 0) scratch[1] = n;
+__global__ void noalloc_begin_kernel(unsigned long long* scratch, int64_t n) {
+  // every call starts from a cleared cursor: the array keeps the last call's values
+  if (threadIdx.x < kNoAllocScratchWords) scratch[threadIdx.x] = threadIdx.x == 1 ? (unsigned long long)n : 0ull;
 }
 
-// Work-stealing variant of trace_full_kernel: warps take 32 rays at a time from the cursor
-// in scratch[0] (count in scratch[1], stack overflows counted in scratch[2]).
-__global__ void __launch_bounds__(128) trace_stealing_kernel(DevScene sc, const xb_ray* rays,
-                                                             xb_hit* hits, int mode, int32_t* scratch) {
-  __shared__ int s_base[4];
-  const int n = scratch[1];
+// Work-stealing variant of trace_full_kernel: warps take 32 rays at a time from the cursor in
+// scratch[0] (ray count in scratch[1]). Threads that overflowed their traversal stack are counted
+// in the renderer's statistics, as trace_full_kernel counts them.
+__global__ void __launch_bounds__(128) trace_stealing_kernel(DevScene sc, const xb_ray* rays, xb_hit* hits,
+                                                             int mode, unsigned long long* scratch,
+                                                             unsigned long long* stats) {
+  __shared__ unsigned long long s_base[4];
+  const int64_t n = (int64_t)scratch[1];
   uint32_t tstack[kStackSize];
   uint32_t bstack[kStackSize];
   bool overflow = false;
   TraversalCounters tc{0, 0, 0, 0};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (;;) {
-    if (lane == 0) s_base[warp] = atomicAdd(scratch, 32);
+    if (lane == 0) s_base[warp] = atomicAdd(scratch, 32ull);
     __syncwarp();
-    const int base = s_base[warp];
+    const int64_t base = (int64_t)s_base[warp];
     __syncwarp();
     if (base >= n) break;
-    const int i = base + lane;
+    const int64_t i = base + lane;
     if (i >= n) continue;
     const xb_ray rr = rays[i];
     Ray r{v3(rr.org[0], rr.org[1], rr.org[2]), v3(rr.dir[0], rr.dir[1], rr.dir[2]), rr.tmin, rr.tmax};
@@ -1294,7 +1300,7 @@ __global__ void __launch_bounds__(128) trace_stealing_kernel(DevScene sc, const 
     }
     hits[i] = out;
   }
-  if (overflow) atomicAdd(scratch + 2, 1);
+  if (overflow) atomicAdd(stats + STAT_OVERFLOW, 1ull);
 }
 
 DevMaterial to_dev_material(const xb_material& m) {
@@ -1490,14 +1496,36 @@ struct StageTimer {
   }
 };
 
+// Per stage: the summed launch durations, the launch count, and the busy time — the union of
+// the launch intervals, placed on one clock by their start events' times after the call's first
+// event (the first launch of the call; the lanes' waves start after it).
 void collect_stage_times(xb_renderer* r) {
+  std::vector<std::pair<double, double>> spans[6];
   for (size_t i = 0; i + 1 < r->ev_used; i += 2) {
-    float ms = 0.f;
+    float ms = 0.f, start = 0.f;
     if (cudaEventElapsedTime(&ms, r->ev_pool[i], r->ev_pool[i + 1]) == cudaSuccess) {
       const int st = r->ev_stage[i / 2];
       r->stage_ms[st] += ms;
       r->stage_launches[st] += 1;
+      if (cudaEventElapsedTime(&start, r->ev_pool[0], r->ev_pool[i]) == cudaSuccess)
+        spans[st].emplace_back((double)start, (double)start + ms);
     }
+  }
+  for (int st = 0; st < 6; ++st) {
+    std::vector<std::pair<double, double>>& v = spans[st];
+    std::sort(v.begin(), v.end());
+    double busy = 0.0, lo = 0.0, hi = 0.0;
+    for (size_t k = 0; k < v.size(); ++k) {
+      if (k == 0 || v[k].first > hi) {
+        if (k) busy += hi - lo;
+        lo = v[k].first;
+        hi = v[k].second;
+      } else {
+        hi = std::max(hi, v[k].second);
+      }
+    }
+    if (!v.empty()) busy += hi - lo;
+    r->stage_busy_ms[st] += busy;
   }
   r->ev_used = 0;
 }
@@ -2350,9 +2378,12 @@ int xb_refit_mesh(xb_renderer* r, int32_t mesh, const float* positions, const fl
   CK(cudaMemcpyAsync(root, r->scene.blas + 2 * ml.node_base, sizeof(root), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   drop_graphs(r);
-  if (status != 0)
-    return set_err(r, XB_E_INVALID, "xb_refit_mesh: mesh %d's BLAS is malformed (%s)", mesh,
-                   status == 1 ? "an index out of range" : "a cycle");
+  if (status != 0) {
+    // the triangles and some boxes are rewritten already: no render may trace this scene
+    r->has_scene = false;
+    return set_err(r, XB_E_INVALID, "xb_refit_mesh: mesh %d's BLAS is malformed (%s); upload the scene again",
+                   mesh, status == 1 ? "an index out of range" : "a cycle");
+  }
   ml.root.mn[0] = root[0].x; ml.root.mn[1] = root[0].y; ml.root.mn[2] = root[0].z;
   ml.root.mx[0] = root[0].w; ml.root.mx[1] = root[1].x; ml.root.mx[2] = root[1].y;
   // the TLAS over the instances' new world boxes, built on the host as xb_scene_build builds it
@@ -2737,13 +2768,16 @@ int xb_get_profile(const xb_renderer* r_, xb_profile* out) {
   out->sh_tlas_nodes = (int64_t)s[STAT_SH_WORK + 2]; out->sh_instances = (int64_t)s[STAT_SH_WORK + 3];
   out->train_ms = r->stage_ms[STAGE_TRAIN];
   out->train_launches = r->stage_launches[STAGE_TRAIN];
+  out->extend_busy_ms = r->stage_busy_ms[STAGE_EXTEND];
+  out->shade_busy_ms = r->stage_busy_ms[STAGE_SHADE];
+  out->shadow_busy_ms = r->stage_busy_ms[STAGE_SHADOW];
   return XB_OK;
 }
 
 int xb_reset_profile(xb_renderer* r) {
   int rc = check_ready(r);
   if (rc) return rc;
-  for (int i = 0; i < 5; ++i) { r->stage_ms[i] = 0; r->stage_launches[i] = 0; }
+  for (int i = 0; i < 6; ++i) { r->stage_ms[i] = 0; r->stage_launches[i] = 0; r->stage_busy_ms[i] = 0; }
   unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   CK(cudaMemcpyAsync(r->stats + STAT_EXT_WORK, z, sizeof(z), cudaMemcpyHostToDevice, r->stream));
   CK(cudaStreamSynchronize(r->stream));
@@ -2768,7 +2802,7 @@ int xb_trace_rays_device(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit* 
 // Device address of g_noalloc_scratch, looked up once per device (with that device current)
 // by the first call made on it; cudaGetSymbolAddress allocates nothing.
 static std::mutex g_noalloc_mu;
-static int32_t* g_noalloc_ptr[128] = {};
+static unsigned long long* g_noalloc_ptr[128] = {};
 
 int xb_trace_rays_noalloc(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit* hits, int32_t mode,
                           void* stream) {
@@ -2783,7 +2817,7 @@ int xb_trace_rays_noalloc(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit*
   if (n == 0) return XB_OK;
   const int dev = r->cfg.device;
   if (dev < 0 || dev >= 128) return set_err(r, XB_E_UNSUPPORTED, "xb_trace_rays_noalloc: device %d", dev);
-  int32_t* scratch = nullptr;
+  unsigned long long* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
@@ -2791,14 +2825,14 @@ int xb_trace_rays_noalloc(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit*
       cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p)
         return set_err(r, XB_E_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s", cudaGetErrorString(e));
-      g_noalloc_ptr[dev] = static_cast<int32_t*>(p);
+      g_noalloc_ptr[dev] = static_cast<unsigned long long*>(p);
     }
     scratch = g_noalloc_ptr[dev];
   }
   cudaStream_t s = stream ? (cudaStream_t)stream : r->stream;
-  noalloc_begin_kernel<<<1, 2 * kNoAllocScratchWords, 0, s>>>(scratch, (int32_t)n);
+  noalloc_begin_kernel<<<1, kNoAllocScratchWords, 0, s>>>(scratch, n);
   const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)r->num_sms * r->occ_ext);
-  trace_stealing_kernel<<<grid, 128, 0, s>>>(r->scene, rays, hits, mode, scratch);
+  trace_stealing_kernel<<<grid, 128, 0, s>>>(r->scene, rays, hits, mode, scratch, r->stats);
   CK(cudaGetLastError());
   return XB_OK;
 }

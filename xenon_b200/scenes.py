@@ -176,6 +176,66 @@ def icosphere(level: int) -> tuple[np.ndarray, np.ndarray]:
     return v, f.astype(np.int32)
 
 
+def geodesic_sphere(freq: int) -> tuple[np.ndarray, np.ndarray]:
+    """Unit geodesic sphere: every face of the icosahedron split into freq x freq triangles on a
+    barycentric grid, the points projected onto the sphere; 20 * freq**2 triangles (freq 158:
+    499,280), outward winding, closed (vertices on the icosahedron's edges are shared)."""
+    n = int(freq)
+    if n < 1:
+        raise ValueError("geodesic_sphere: freq >= 1")
+    v0, f0 = icosphere(0)
+    edges = {}
+    pts = [v0]
+    count = len(v0)
+    for a, b, c in f0:
+        for p, q in ((a, b), (b, c), (a, c)):
+            key = (min(p, q), max(p, q))
+            if key not in edges and n > 1:
+                k = np.arange(1, n)[:, None] / n
+                pts.append(v0[key[0]] + (v0[key[1]] - v0[key[0]]) * k)
+                edges[key] = count
+                count += n - 1
+
+    def edge_point(p, q, k):
+        """Vertex index of the point k/n of the way from corner p to corner q (0 < k < n)."""
+        if p < q:
+            return edges[(p, q)] + k - 1
+        return edges[(q, p)] + (n - k) - 1
+
+    tris = []
+    for a, b, c in f0:
+        idx = {}
+        for i in range(n + 1):
+            for j in range(n + 1 - i):
+                if i == 0 and j == 0:
+                    idx[i, j] = a
+                elif i == n:
+                    idx[i, j] = b
+                elif j == n:
+                    idx[i, j] = c
+                elif j == 0:
+                    idx[i, j] = edge_point(a, b, i)
+                elif i == 0:
+                    idx[i, j] = edge_point(a, c, j)
+                elif i + j == n:
+                    idx[i, j] = edge_point(b, c, j)
+        inner = [(i, j) for i in range(1, n) for j in range(1, n - i)]
+        if inner:
+            ij = np.array(inner, np.float64)
+            pts.append(v0[a] + (v0[b] - v0[a]) * ij[:, :1] / n + (v0[c] - v0[a]) * ij[:, 1:] / n)
+            for k, key in enumerate(inner):
+                idx[key] = count + k
+            count += len(inner)
+        for i in range(n):
+            for j in range(n - i):
+                tris.append((idx[i, j], idx[i + 1, j], idx[i, j + 1]))
+                if i + j < n - 1:
+                    tris.append((idx[i + 1, j], idx[i + 1, j + 1], idx[i, j + 1]))
+    v = np.concatenate(pts)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v, np.array(tris, np.int32)
+
+
 def value_noise(p: np.ndarray, seed: int, octaves: int = 4, base_freq: float = 1.5) -> np.ndarray:
     """Seeded lattice value noise in [-1, 1]: smoothstep-trilinear, `octaves` octaves with
     doubling frequency and halving amplitude, normalised by the amplitude sum."""
@@ -336,11 +396,13 @@ def instanced_grid(grid: int = 16, levels=(6, 6, 7, 7), width: int = 1920, heigh
 
 
 # ── config 4 ────────────────────────────────────────────────────────────────────
-def guiding_room(level: int = 7, width: int = 1280, height: int = 720, max_bounces: int = 16,
-                 spp: int = 64) -> SceneDesc:
+def guiding_room(level: int | None = None, width: int = 1280, height: int = 720, max_bounces: int = 16,
+                 spp: int = 64, freq: int = 158) -> SceneDesc:
     """Config 4: closed 10x10x10 diffuse room (albedo 0.7), the only light an emissive quad of
     0.5 units^2 (0.5 % of the ceiling) hidden above a diffuse baffle, and a smooth glass sphere
-    mesh (IOR 1.5, roughness 0 → delta). Level 7 = 327,680 tris; level 8 = 1.31 M.
+    mesh (IOR 1.5, roughness 0 → delta). By default the sphere is the geodesic sphere of
+    frequency 158: 499,280 tris, the configuration's 500k; `level` instead takes the icosphere of
+    that level (20 * 4**level tris: level 7 = 327,680), for smaller test scenes.
     The walls have IOR 1 (F0 = 0): a purely Lambertian BSDF whose sampled and evaluated forms
     agree, so the guided and the plain estimator converge to the same image."""
     d = SceneDesc(name="guiding_room", width=width, height=height, spp=spp, max_bounces=max_bounces)
@@ -362,7 +424,11 @@ def guiding_room(level: int = 7, width: int = 1280, height: int = 720, max_bounc
     lm = d.add_mesh(quad_mesh((3.4 - s / 2, L - 0.01, -2.5 - s / 2), (s, 0, 0), (0, 0, s), lightm))
     for tri in (0, 1):
         d.lights.append((lm, tri, (400.0, 380.0, 340.0), s * s / 2))
-    pos, f = displaced_icosphere(level, 1.6, (-1.0, 1.6, -0.5), 7, amplitude=0.0)
+    if level is None:
+        v, f = geodesic_sphere(freq)
+        pos = np.asarray((-1.0, 1.6, -0.5), np.float64) + v * 1.6
+    else:
+        pos, f = displaced_icosphere(level, 1.6, (-1.0, 1.6, -0.5), 7, amplitude=0.0)
     d.add_mesh(MeshDesc(f32(pos), f, None, None, glass))
     d.sky = sky_array(intensity=0.0)
     d.eye, d.target, d.fov = (0.0, 5.0, 4.8), (0.0, 3.5, -5.0), 60.0
