@@ -90,8 +90,15 @@ def test_config1_converged_at_full_size():
     for first in range(1, spp + 1, 1024):
         r.render_range(cam, first, min(1024, spp + 1 - first))
     got = r.resolve()
-    e = relmse(got, want)
-    print("config1 256x256 16k spp relMSE", e, "mean", got.mean(), want.mean())
+    # the reference accumulates non-finite path radiance (it has no guard): the few pixels where
+    # one of its 16k samples was NaN are NaN in its image and are left out, as the parity rules
+    # for NaN say; this library drops such samples and counts them (stats().nonfinite)
+    ok = np.isfinite(want).all(-1)
+    assert (~ok).sum() <= 8, (~ok).sum()
+    e = relmse(got[ok], want[ok])
+    print("config1 256x256 16k spp relMSE", e, "mean", got[ok].mean(), want[ok].mean(),
+          "reference NaN pixels", int((~ok).sum()), "dropped samples", r.stats().nonfinite)
     assert r.stats().overflow == 0
+    assert np.isfinite(got).all()
     assert e < 1e-3, e
-    assert abs(got.mean() / want.mean() - 1) < 1e-3
+    assert abs(got[ok].mean() / want[ok].mean() - 1) < 1e-3
