@@ -420,6 +420,10 @@ typedef struct xb_tuning {
   int32_t shade_occupancy;              /* shading kernels compiled to fit 4, 8 (default) or 12
                                            blocks of 128 threads per SM: fewer registers per
                                            thread, the rest spilled to L1 (other values: 8) */
+  int32_t shared_stack;                 /* traversal kernels: 16 = the first 16 entries of each
+                                           thread's BLAS stack in shared memory (8 KB per block of
+                                           128 threads), the rest in local memory; 1 (default, and
+                                           any other value): all in local memory. Same hits. */
 } xb_tuning;
 int  xb_set_tuning(xb_renderer *r, const xb_tuning *t);
 int  xb_get_tuning(const xb_renderer *r, xb_tuning *out);

@@ -13,6 +13,7 @@ two passes), and keeps the fastest setting:
   graph                          captured CUDA graphs of the bounce loop, or direct launches
   guided_form                    guided bounce as a bounce kernel + network pass, or one fused kernel
   shade_occupancy                blocks per SM the shading kernels are compiled to fit (registers)
+  shared_stack                   BLAS stack entries per thread kept in shared memory (1: none, 16)
   refill                         idle lanes that trigger a warp refill
   extend/shadow/shade_blocks_per_sm   blocks per SM in the grids (persistent kernels: at most
                                       those resident at once)
@@ -41,6 +42,7 @@ SPACE = {
     "graph": [1, 2],
     "guided_form": [1, 2],
     "shade_occupancy": [4, 8, 12],
+    "shared_stack": [1, 16],
     "refill": [2, 4, 8, 16, 24],
     "extend_blocks_per_sm": [2, 4, 8, 16, 64],
     "shadow_blocks_per_sm": [2, 4, 8, 16, 64],

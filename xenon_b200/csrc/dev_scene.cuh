@@ -26,6 +26,27 @@
 namespace xbd {
 
 constexpr int kStackSize = 64;   // BLAS / TLAS / PrimBLAS stacks are 64 deep in the reference
+constexpr int kShStride = 128;   // threads per block of every traversal kernel
+constexpr int kSharedStack = 16; // BLAS stack entries the shared-stack kernels keep in shared memory
+
+// The BLAS / PrimBLAS traversal stack. Its first NSH entries live in shared memory (entry k of
+// thread t at sh[k * kShStride + t]: a warp's 32 accesses fall in 32 distinct banks at any mix of
+// depths), the rest in the thread's local array (entries k >= NSH at loc[k]). NSH = 0 keeps the
+// whole stack in local memory and compiles to plain local-array accesses.
+template <int NSH>
+struct BStack {
+  uint32_t* sh;
+  uint32_t* loc;
+  __device__ __forceinline__ uint32_t get(int k) const {
+    if constexpr (NSH == 0) return loc[k];
+    else return k < NSH ? sh[k * kShStride] : loc[k];
+  }
+  __device__ __forceinline__ void put(int k, uint32_t v) const {
+    if constexpr (NSH == 0) loc[k] = v;
+    else if (k < NSH) sh[k * kShStride] = v;
+    else loc[k] = v;
+  }
+};
 
 struct DevInstance {     // 64 bytes
   float w2l[12];         // world_to_local, columns c0 c1 c2 c3
@@ -322,9 +343,9 @@ __device__ __forceinline__ bool prim_intersect(const float4* pr, const Ray& r, f
 }
 
 // ── BLAS closest hit (blas.cpp:211-265) ──────────────────────────────────────────
-template <bool kCount>
+template <bool kCount, class Stack>
 __device__ __forceinline__ bool blas_closest(const DevScene& sc, int root, const Ray& r,
-                                             HitState& h, int inst_idx, uint32_t* stack,
+                                             HitState& h, int inst_idx, const Stack& stack,
                                              TraversalCounters& cnt, bool& overflow) {
   // The reference pushes (far, near) and pops near at once; here the near child continues in
   // a register and only the far one is pushed: the same visit order, half the stack traffic.
@@ -349,7 +370,7 @@ __device__ __forceinline__ bool blas_closest(const DevScene& sc, int root, const
         }
       }
       if (ptr == 0) break;
-      cur = stack[--ptr];
+      cur = stack.get(--ptr);
       continue;
     }
     if (kCount) cnt.nodes++;
@@ -362,22 +383,22 @@ __device__ __forceinline__ bool blas_closest(const DevScene& sc, int root, const
     const uint32_t er = blas_entry(__float_as_uint(rb.z), __float_as_uint(rb.w), child + 1);
     if (hl && hr) {
       if (ptr + 1 > kStackSize) { overflow = true; break; }
-      if (tl < tr) { stack[ptr++] = er; cur = el; }
-      else { stack[ptr++] = el; cur = er; }
+      if (tl < tr) { stack.put(ptr++, er); cur = el; }
+      else { stack.put(ptr++, el); cur = er; }
     } else if (hl || hr) {
       cur = hl ? el : er;
     } else {
       if (ptr == 0) break;
-      cur = stack[--ptr];
+      cur = stack.get(--ptr);
     }
   }
   return hit;
 }
 
 // ── BLAS any hit (blas.cpp:269-307) ──────────────────────────────────────────────
-template <bool kCount>
+template <bool kCount, class Stack>
 __device__ __forceinline__ bool blas_any(const DevScene& sc, int root, const Ray& r,
-                                         uint32_t* stack, TraversalCounters& cnt, bool& overflow,
+                                         const Stack& stack, TraversalCounters& cnt, bool& overflow,
                                          bool far_first = false) {
   // Whether some triangle lies in [tmin, tmax] does not depend on the visit order, so the order
   // is a tuning choice: nearest child first, or farthest first (shadow rays start on a surface,
@@ -397,7 +418,7 @@ __device__ __forceinline__ bool blas_any(const DevScene& sc, int root, const Ray
         if (ray_triangle(r.o, r.d, r.tmin, ld3(a), ld3(b), ld3(c), r.tmax, t, u, v)) return true;
       }
       if (ptr == 0) return false;
-      cur = stack[--ptr];
+      cur = stack.get(--ptr);
       continue;
     }
     if (kCount) cnt.nodes++;
@@ -410,25 +431,26 @@ __device__ __forceinline__ bool blas_any(const DevScene& sc, int root, const Ray
     const uint32_t er = blas_entry(__float_as_uint(rb.z), __float_as_uint(rb.w), child + 1);
     if (hl && hr) {
       if (ptr + 1 > kStackSize) { overflow = true; return false; }
-      if ((tl < tr) != far_first) { stack[ptr++] = er; cur = el; }
-      else { stack[ptr++] = el; cur = er; }
+      if ((tl < tr) != far_first) { stack.put(ptr++, er); cur = el; }
+      else { stack.put(ptr++, el); cur = er; }
     } else if (hl || hr) {
       cur = hl ? el : er;
     } else {
       if (ptr == 0) return false;
-      cur = stack[--ptr];
+      cur = stack.get(--ptr);
     }
   }
 }
 
 // ── PrimBLAS closest hit (prim_blas.cpp:142-194) ───────────────────────────────
+template <class Stack>
 __device__ __forceinline__ bool pblas_closest(const DevScene& sc, const Ray& r, HitState& h,
-                                              int inst_idx, uint32_t* stack, bool& overflow) {
+                                              int inst_idx, const Stack& stack, bool& overflow) {
   int ptr = 0;
-  stack[ptr++] = 0;
+  stack.put(ptr++, 0);
   bool hit = false;
   while (ptr > 0) {
-    const uint32_t idx = stack[--ptr];
+    const uint32_t idx = stack.get(--ptr);
     const float4 na = ldg4(sc.pnodes + 2 * idx), nb = ldg4(sc.pnodes + 2 * idx + 1);
     float tn;
     if (!aabb_div(na, nb, r, tn) || tn > h.t) continue;
@@ -453,24 +475,25 @@ __device__ __forceinline__ bool pblas_closest(const DevScene& sc, const Ray& r, 
     const bool hr = aabb_div(ra, rb, r, tr) && tr <= h.t;
     if (ptr + 2 > kStackSize) { overflow = true; break; }
     if (hl && hr) {
-      if (tl < tr) { stack[ptr++] = child + 1; stack[ptr++] = child; }
-      else { stack[ptr++] = child; stack[ptr++] = child + 1; }
+      if (tl < tr) { stack.put(ptr++, child + 1); stack.put(ptr++, child); }
+      else { stack.put(ptr++, child); stack.put(ptr++, child + 1); }
     } else if (hl) {
-      stack[ptr++] = child;
+      stack.put(ptr++, child);
     } else if (hr) {
-      stack[ptr++] = child + 1;
+      stack.put(ptr++, child + 1);
     }
   }
   return hit;
 }
 
 // ── PrimBLAS any hit (prim_blas.cpp:197-229) ───────────────────────────────────
-__device__ __forceinline__ bool pblas_any(const DevScene& sc, const Ray& r, uint32_t* stack,
+template <class Stack>
+__device__ __forceinline__ bool pblas_any(const DevScene& sc, const Ray& r, const Stack& stack,
                                           bool& overflow) {
   int ptr = 0;
-  stack[ptr++] = 0;
+  stack.put(ptr++, 0);
   while (ptr > 0) {
-    const uint32_t idx = stack[--ptr];
+    const uint32_t idx = stack.get(--ptr);
     const float4 na = ldg4(sc.pnodes + 2 * idx), nb = ldg4(sc.pnodes + 2 * idx + 1);
     float tn;
     if (!aabb_div(na, nb, r, tn)) continue;
@@ -483,16 +506,16 @@ __device__ __forceinline__ bool pblas_any(const DevScene& sc, const Ray& r, uint
       continue;
     }
     if (ptr + 2 > kStackSize) { overflow = true; return false; }
-    stack[ptr++] = child;
-    stack[ptr++] = child + 1;
+    stack.put(ptr++, child);
+    stack.put(ptr++, child + 1);
   }
   return false;
 }
 
 // ── TLAS closest hit (tlas.cpp:172-245) ──────────────────────────────────────────
-template <bool kCount>
+template <bool kCount, class Stack>
 __device__ __forceinline__ bool scene_closest(const DevScene& sc, const Ray& w, HitState& h,
-                                              uint32_t* tstack, uint32_t* bstack,
+                                              uint32_t* tstack, const Stack& bstack,
                                               TraversalCounters& cnt, bool& overflow) {
   h.t = kInf; h.u = 0.f; h.v = 0.f; h.prim = -1; h.inst = -1;
   if (sc.num_tlas_nodes == 0) return false;
@@ -539,9 +562,9 @@ __device__ __forceinline__ bool scene_closest(const DevScene& sc, const Ray& w, 
 }
 
 // ── TLAS any hit (tlas.cpp:248-290) ──────────────────────────────────────────────
-template <bool kCount>
+template <bool kCount, class Stack>
 __device__ __forceinline__ bool scene_any(const DevScene& sc, const Ray& w, uint32_t* tstack,
-                                          uint32_t* bstack, TraversalCounters& cnt, bool& overflow,
+                                          const Stack& bstack, TraversalCounters& cnt, bool& overflow,
                                           bool far_first = false) {
   if (sc.num_tlas_nodes == 0) return false;
   const V3 inv = v3(1.f / w.d.x, 1.f / w.d.y, 1.f / w.d.z);

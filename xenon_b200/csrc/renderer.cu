@@ -167,6 +167,7 @@ struct xb_renderer {
   int ext_persistent_from = 0;   // bounces >= this trace closest hits with persistent warps
   bool shadow_persistent = true;
   int occ_ext = 1, occ_pext = 1, occ_shadow = 1, occ_pshadow = 1;  // limits
+  int stack_sh = 0;             // BLAS stack entries in shared memory (tuning shared_stack)
   xb_tuning tune{};
   // profiling
   int prof_flags = 0;
@@ -269,7 +270,7 @@ __global__ void raygen_kernel(CamDev cam, int W, int H, int spp_first, int64_t p
 }
 
 // ── extend: closest hit of the bounce's ray queue ─────────────────────────────
-template <bool kCount>
+template <bool kCount, int kSh>
 __global__ void __launch_bounds__(128) extend_kernel(DevScene sc, const float4* __restrict__ ray_o,
                                                      const float4* __restrict__ ray_d,
                                                      float4* hit, int32_t* hit_inst, int32_t* cnt,
@@ -277,7 +278,9 @@ __global__ void __launch_bounds__(128) extend_kernel(DevScene sc, const float4* 
   __shared__ int s_base[4];
   const int n = cnt[CNT_RAYS];
   uint32_t tstack[kStackSize];
-  uint32_t bstack[kStackSize];
+  uint32_t bstack_local[kStackSize];
+  extern __shared__ uint32_t s_stack[];
+  const BStack<kSh> bstack{s_stack + threadIdx.x, bstack_local};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   bool overflow = false;
   TraversalCounters tc{0, 0, 0, 0};
@@ -302,7 +305,7 @@ __global__ void __launch_bounds__(128) extend_kernel(DevScene sc, const float4* 
 }
 
 // ── shadow: any hit; unoccluded items add their contribution ──────────────────
-template <bool kCount>
+template <bool kCount, int kSh>
 __global__ void __launch_bounds__(128) shadow_kernel(DevScene sc, const float4* __restrict__ so,
                                                      const float4* __restrict__ sd,
                                                      const float4* __restrict__ scn, float4* L,
@@ -311,7 +314,9 @@ __global__ void __launch_bounds__(128) shadow_kernel(DevScene sc, const float4* 
   __shared__ int s_base[4];
   const int n = *count;
   uint32_t tstack[kStackSize];
-  uint32_t bstack[kStackSize];
+  uint32_t bstack_local[kStackSize];
+  extern __shared__ uint32_t s_stack[];
+  const BStack<kSh> bstack{s_stack + threadIdx.x, bstack_local};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   bool overflow = false;
   TraversalCounters tc{0, 0, 0, 0};
@@ -339,13 +344,13 @@ __global__ void __launch_bounds__(128) shadow_kernel(DevScene sc, const float4* 
 }
 
 // ── persistent-warp variants (trace_persistent.cuh) ────────────────────────────
-template <bool kCount>
+template <bool kCount, int kSh>
 __global__ void __launch_bounds__(128) extend_persistent_kernel(DevScene sc, TraceQueue q, int refill) {
-  trace_queue_persistent<false, kCount>(sc, q, refill);
+  trace_queue_persistent<false, kCount, kSh>(sc, q, refill);
 }
-template <bool kCount>
+template <bool kCount, int kSh>
 __global__ void __launch_bounds__(128) shadow_persistent_kernel(DevScene sc, TraceQueue q, int refill) {
-  trace_queue_persistent<true, kCount>(sc, q, refill);
+  trace_queue_persistent<true, kCount, kSh>(sc, q, refill);
 }
 
 // ── shade (cpu_tiled.cpp:34-217 for one bounce) ───────────────────────────────
@@ -1167,7 +1172,8 @@ __global__ void __launch_bounds__(128) trace_full_kernel(DevScene sc, const xb_r
                                                          int64_t n, xb_hit* hits, int mode,
                                                          unsigned long long* stats) {
   uint32_t tstack[kStackSize];
-  uint32_t bstack[kStackSize];
+  uint32_t bstack_local[kStackSize];
+  const BStack<0> bstack{nullptr, bstack_local};
   bool overflow = false;
   TraversalCounters tc{0, 0, 0, 0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -1265,7 +1271,8 @@ __global__ void __launch_bounds__(128) trace_stealing_kernel(DevScene sc, const 
   __shared__ unsigned long long s_base[4];
   const int64_t n = (int64_t)scratch[1];
   uint32_t tstack[kStackSize];
-  uint32_t bstack[kStackSize];
+  uint32_t bstack_local[kStackSize];
+  const BStack<0> bstack{nullptr, bstack_local};
   bool overflow = false;
   TraversalCounters tc{0, 0, 0, 0};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1445,6 +1452,9 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.guided_form = std::min(2, pick(t.guided_form, c.guided_form, 1));
   c.shade_occupancy = pick(t.shade_occupancy, c.shade_occupancy, 8);
   if (c.shade_occupancy != 4 && c.shade_occupancy != 8 && c.shade_occupancy != 12) c.shade_occupancy = 8;
+  c.shared_stack = pick(t.shared_stack, c.shared_stack, 1);
+  if (c.shared_stack != 1 && c.shared_stack != kSharedStack) c.shared_stack = 1;
+  r->stack_sh = c.shared_stack > 1 ? c.shared_stack : 0;
   drop_graphs(r);
   r->ext_persistent_from = c.extend_persistent_from_depth;
   r->shadow_persistent = c.shadow_persistent == 1;
@@ -1557,42 +1567,59 @@ LaneRef lane_ref(xb_renderer* r, int k) {
   return LaneRef{&x.wb, x.s, x.s2, x.ev_shade, x.ev_shadow};
 }
 
-void launch_extend(xb_renderer* r, const LaneRef& L, int d, bool count) {
+// The traversal kernels come in two forms: the BLAS stack wholly in local memory (kSh = 0), or
+// its first kSharedStack entries in shared memory (tuning shared_stack).
+
+template <int kSh>
+void launch_extend_k(xb_renderer* r, const LaneRef& L, int d, bool count) {
   WaveBuffers& w = *L.w;
   const int q = d & 1;
   int32_t* cd_ = w.cnt + d * kCntStride;
-  StageTimer t(r, STAGE_EXTEND, L.s);
+  const size_t smem = (size_t)kSh * kShStride * sizeof(uint32_t);
   if (r->thread_per_ray || d < r->ext_persistent_from) {
-    auto kern = count ? extend_kernel<true> : extend_kernel<false>;
-    kern<<<r->grid_ext, 128, 0, L.s>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_, r->stats);
+    auto kern = count ? extend_kernel<true, kSh> : extend_kernel<false, kSh>;
+    kern<<<r->grid_ext, 128, smem, L.s>>>(r->scene, w.ray_o[q], w.ray_d[q], w.hit, w.hit_inst, cd_, r->stats);
   } else {
     TraceQueue tq{w.ray_o[q], w.ray_d[q], cd_ + CNT_RAYS, cd_ + CNT_FETCH_EXT, w.hit, w.hit_inst,
                   nullptr, nullptr, r->stats, 0};
-    auto kern = count ? extend_persistent_kernel<true> : extend_persistent_kernel<false>;
-    kern<<<r->grid_pext, 128, 0, L.s>>>(r->scene, tq, r->refill);
+    auto kern = count ? extend_persistent_kernel<true, kSh> : extend_persistent_kernel<false, kSh>;
+    kern<<<r->grid_pext, 128, smem, L.s>>>(r->scene, tq, r->refill);
+  }
+}
+
+void launch_extend(xb_renderer* r, const LaneRef& L, int d, bool count) {
+  StageTimer t(r, STAGE_EXTEND, L.s);
+  if (r->stack_sh) launch_extend_k<kSharedStack>(r, L, d, count);
+  else launch_extend_k<0>(r, L, d, count);
+}
+
+template <int kSh>
+void launch_shadow_k(xb_renderer* r, const LaneRef& L, int d, int k, bool count, cudaStream_t s) {
+  WaveBuffers& w = *L.w;
+  int32_t* cd_ = w.cnt + d * kCntStride;
+  const size_t smem = (size_t)kSh * kShStride * sizeof(uint32_t);
+  if (r->thread_per_ray || !r->shadow_persistent) {
+    auto kern = count ? shadow_kernel<true, kSh> : shadow_kernel<false, kSh>;
+    kern<<<r->grid_shadow, 128, smem, s>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
+                                           cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
+                                           cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats,
+                                           r->tune.shadow_order == 2);
+  } else {
+    TraceQueue tq{w.sh_o[k], w.sh_d[k], cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
+                  cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), nullptr, nullptr, w.sh_c[k], w.L,
+                  r->stats, r->tune.shadow_order == 2};
+    auto kern = count ? shadow_persistent_kernel<true, kSh> : shadow_persistent_kernel<false, kSh>;
+    kern<<<r->grid_pshadow, 128, smem, s>>>(r->scene, tq, r->refill);
   }
 }
 
 void launch_shadows(xb_renderer* r, const LaneRef& L, int d, bool count, cudaStream_t s) {
-  WaveBuffers& w = *L.w;
-  int32_t* cd_ = w.cnt + d * kCntStride;
   for (int k = 0; k < 2; ++k) {
     if (k == 0 && r->scene.num_lights == 0) continue;
     if (k == 1 && r->scene.num_suns == 0) continue;
     StageTimer t(r, STAGE_SHADOW, s);
-    if (r->thread_per_ray || !r->shadow_persistent) {
-      auto kern = count ? shadow_kernel<true> : shadow_kernel<false>;
-      kern<<<r->grid_shadow, 128, 0, s>>>(r->scene, w.sh_o[k], w.sh_d[k], w.sh_c[k], w.L,
-                                          cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
-                                          cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), r->stats,
-                                          r->tune.shadow_order == 2);
-    } else {
-      TraceQueue tq{w.sh_o[k], w.sh_d[k], cd_ + (k ? CNT_SH_SUN : CNT_SH_AREA),
-                    cd_ + (k ? CNT_FETCH_SH_SUN : CNT_FETCH_SH_AREA), nullptr, nullptr, w.sh_c[k], w.L,
-                    r->stats, r->tune.shadow_order == 2};
-      auto kern = count ? shadow_persistent_kernel<true> : shadow_persistent_kernel<false>;
-      kern<<<r->grid_pshadow, 128, 0, s>>>(r->scene, tq, r->refill);
-    }
+    if (r->stack_sh) launch_shadow_k<kSharedStack>(r, L, d, k, count, s);
+    else launch_shadow_k<0>(r, L, d, k, count, s);
   }
 }
 
@@ -2014,9 +2041,9 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   }
   int rc = XB_OK;
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_kernel<false>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_kernel<false, 0>, 128, 0);
   r->occ_ext = std::max(occ, 1);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_kernel<false>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_kernel<false, 0>, 128, 0);
   r->occ_shadow = std::max(occ, 1);
   // guided shade: dynamic shared memory for the weights, one activation tile and the lobes; at
   // most 4 CTAs per SM so their TMEM (64 columns each) always fits the SM's 512 columns
@@ -2041,9 +2068,9 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
     const int by_smem = smem_sm / std::max<int>(1, (int)(kGuidedShadeSmem + fa.sharedSizeBytes) + smem_rsv);
     r->occ_gshade = std::max(1, std::min(4, std::min(by_regs, by_smem)));
   }
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_persistent_kernel<false>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_persistent_kernel<false, 0>, 128, 0);
   r->occ_pext = std::max(occ, 1);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_persistent_kernel<false>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_persistent_kernel<false, 0>, 128, 0);
   r->occ_pshadow = std::max(occ, 1);
   r->thread_per_ray = (cfg->flags & XB_FLAG_THREAD_PER_RAY) != 0;
   {

@@ -35,14 +35,16 @@ struct TraceQueue {
   int far_first;            // any-hit: descend into the farther child first
 };
 
-template <bool kAny, bool kCount>
+template <bool kAny, bool kCount, int kSh>
 __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const TraceQueue& q,
                                                        int refill) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int n = *q.count;
   uint32_t tstack[kStackSize];
-  uint32_t bstack[kStackSize];
+  uint32_t bstack_local[kStackSize];
+  extern __shared__ uint32_t s_stack[];
+  const BStack<kSh> bstack{s_stack + threadIdx.x, bstack_local};
   TraversalCounters cnt{0, 0, 0, 0};
   bool overflow = false;
 
@@ -118,14 +120,14 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
                 overflow = true;
                 bactive = false; bsp = 0; tsp = 0; tl_count = 0;   // abandon (reported as overflow)
               } else if ((tl < tr) != (kAny && q.far_first)) {
-                bstack[bsp++] = er; bcur = el;
+                bstack.put(bsp++, er); bcur = el;
               } else {
-                bstack[bsp++] = el; bcur = er;
+                bstack.put(bsp++, el); bcur = er;
               }
             } else if (hl || hr) {
               bcur = hl ? el : er;
             } else if (bsp > 0) {
-              bcur = bstack[--bsp];
+              bcur = bstack.get(--bsp);
             } else {
               bactive = false;
             }
@@ -225,7 +227,7 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
       if (kAny && occluded) {
         bsp = 0; tsp = 0; tl_count = 0;
       } else if (bsp > 0) {
-        bcur = bstack[--bsp];
+        bcur = bstack.get(--bsp);
         bactive = true;
       }
     }
