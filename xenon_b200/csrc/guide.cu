@@ -9,9 +9,10 @@
 //                           next through shared memory)
 //   guide_train_kernel      per 128-row tile of training records: forward keeping the activations,
 //                           the mixture's weighted negative log-likelihood gradient at the outputs,
-//                           backward through the layers on the tensor cores (delta * W), weight
-//                           gradients reduced over the tile on the CUDA cores in FP32
-//   adam_kernel             FP32 master weights and Adam moments; then the BF16 copies are rebuilt
+//                           backward through the layers on the tensor cores: per layer one commit
+//                           of the weight gradient delta^T a (summed over the tile's rows) and the
+//                           next error signal delta W
+//   adam_kernel             FP32 master weights and Adam moments, and the BF16 copies of the new weights
 //   finalize_records_kernel training weight of each record once its path has finished
 //   tc_gemm_kernel          one tile of D = A * B^T: the MMA building block, checked on its own
 //
@@ -173,27 +174,25 @@ __device__ __forceinline__ float output_gradient(const float* raw, const float* 
   return loss;
 }
 
-// dW[o][i] += sum_r delta[r][o] a[r][i] and db[o] += sum_r delta[r][o] over this tile.
-// Thread t owns input column i = t % 64 and half of the outputs.
-__device__ __forceinline__ void weight_grad(const float* sDf, int O, const uint8_t* act, float* gW, float* gB) {
-  const int i = threadIdx.x & 63, half = threadIdx.x >> 6;
-  const int on = O / 2, o0 = half * on;
-  float acc[32];
+// This tile's weight gradient of a layer from TMEM columns [64, 128) (run_backward): thread o < O
+// adds its row dW[o][0..64) into gW with 16-byte atomics; and db[o] += sum_r delta[r][o] from the
+// FP32 error signal. Every thread takes part in the TMEM loads.
+__device__ __forceinline__ void add_weight_grad(const Mma& m, const float* sDf, int O, float* gW, float* gB) {
+  const int o = threadIdx.x;
 #pragma unroll
-  for (int j = 0; j < 32; ++j) acc[j] = 0.f;
-  for (int r = 0; r < kTile; ++r) {
-    const float a = load_bf16(act, r, i, kK);
-    if (a == 0.f) continue;
-    const float* d = sDf + r * kHid + o0;
+  for (int c = 0; c < kK; c += 16) {
+    float v[16];
+    m.load16(64 + c, v);
+    if (o < O) {
+      float4* dst = reinterpret_cast<float4*>(gW + (size_t)o * kK + c);
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
-      if (j < on) acc[j] += d[j] * a;
+      for (int q = 0; q < 4; ++q) atomicAdd(dst + q, make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
+    }
   }
-  for (int j = 0; j < on; ++j) atomicAdd(gW + (size_t)(o0 + j) * kK + i, acc[j]);
-  if (threadIdx.x < O) {
+  if (o < O) {
     float s = 0.f;
-    for (int r = 0; r < kTile; ++r) s += sDf[r * kHid + threadIdx.x];
-    atomicAdd(gB + threadIdx.x, s);
+    for (int r = 0; r < kTile; ++r) s += sDf[r * kHid + o];
+    atomicAdd(gB + o, s);
   }
 }
 
@@ -219,7 +218,7 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(TrainArgs A) {
   load_forward_weights(sWf, sBias, A.wf, A.master);
   for (int l = 0; l < 3; ++l) load_matrix(sWb + l * kWBytes, A.wb + l * kHid * kK, kHid, kK);
   load_matrix(sWb + 3 * kWBytes, A.wb + 3 * kHid * kK, kHid, kOut);
-  mma_setup(&tmem_slot, &mbar);
+  mma_setup(&tmem_slot, &mbar, 128);
   Mma m{tmem_slot, &mbar, 0u, A.err, true};
   const bool valid = start + (int)threadIdx.x < n;
   float f[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, om[3] = {0, 0, 1}, c = 0.f, pb = -1.f;
@@ -255,15 +254,16 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(TrainArgs A) {
   if ((threadIdx.x & 31) == 0) sLoss[threadIdx.x >> 5] = loss_part;
   __syncthreads();
   if (threadIdx.x == 0) atomicAdd(A.loss, sLoss[0] + sLoss[1] + sLoss[2] + sLoss[3]);
-  // backward: delta_{l-1} = (delta_l W_l) o [a_l > 0], weight gradients from delta_l and a_l
+  // backward: dW_l = delta_l^T a_l and delta_{l-1} = (delta_l W_l) o [a_l > 0], both on the tensor
+  // cores in one commit (run_backward)
   for (int l = 3; l >= 0 && m.ok; --l) {
     const int O = l == 3 ? kOut : kHid;
-    __syncthreads();
-    weight_grad(sDf, O, sAct + l * kTileBytes, A.grad + off_w(l), A.grad + off_b(l));
-    if (l == 0) break;
     m.sync_before();
-    m.run(smem_u32(sD), smem_u32(sWb + l * kWBytes), O, kHid);
+    m.run_backward(smem_u32(sD), O, smem_u32(sAct + l * kTileBytes), l > 0 ? smem_u32(sWb + l * kWBytes) : 0u);
     if (!m.ok) break;
+    add_weight_grad(m, sDf, O, A.grad + off_w(l), A.grad + off_b(l));
+    if (l == 0) break;
+    __syncthreads();   // every thread's column sums of sDf are done before it is overwritten
     for (int cc = 0; cc < kHid; cc += 16) {
       float dv[16];
       m.load16(cc, dv);
@@ -276,19 +276,30 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(TrainArgs A) {
       store8_bf16(sD, threadIdx.x, cc + 8, kK, dv + 8);
     }
   }
-  mma_teardown(m.tmem);
+  mma_teardown(m.tmem, 128);
 }
 
-__global__ void adam_kernel(float* p, float* g, float* mo, float* ve, int n, float lr, float b1, float b2,
-                            float eps, float c1, float c2) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+// One Adam step on the FP32 master parameters, their moments and the gradient (cleared for the
+// next step), and the new weights' BF16 copies (forward W_l as [out][in], backward W_l^T as
+// [in][out]) written in the same pass.
+__global__ void adam_kernel(float* p, float* g, float* mo, float* ve, __nv_bfloat16* wf, __nv_bfloat16* wb, float lr,
+                            float b1, float b2, float eps, float c1, float c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kParams; i += gridDim.x * blockDim.x) {
     const float gi = g[i];
     const float m = b1 * mo[i] + (1.f - b1) * gi;
     const float v = b2 * ve[i] + (1.f - b2) * gi * gi;
     mo[i] = m;
     ve[i] = v;
-    p[i] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+    const float w = p[i] - lr * (m / c1) / (sqrtf(v / c2) + eps);
+    p[i] = w;
     g[i] = 0.f;
+    const int l = i / off_w(1), j = i - off_w(l);
+    const int outs = l == 3 ? kOut : kHid;
+    if (j < outs * kK) {
+      const int o = j / kK, k = j % kK;
+      wf[l * kHid * kK + o * kK + k] = __float2bfloat16_rn(w);
+      wb[l * kHid * kK + k * outs + o] = __float2bfloat16_rn(w);
+    }
   }
 }
 
@@ -455,8 +466,7 @@ int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_
       const double x = std::min(1.0, (double)(g->t - 1) / (double)total_steps);
       lr_t = (float)(lr * (0.1 + 0.45 * (1.0 + std::cos(3.14159265358979323846 * x))));
     }
-    adam_kernel<<<64, 256, 0, s>>>(g->master, g->grad, g->mom, g->vel, kParams, lr_t, b1, b2, 1e-8f, c1, c2);
-    guide_sync_bf16(g, s);
+    adam_kernel<<<64, 256, 0, s>>>(g->master, g->grad, g->mom, g->vel, g->wf, g->wb, lr_t, b1, b2, 1e-8f, c1, c2);
   }
   return cudaGetLastError() == cudaSuccess ? XB_OK : XB_E_CUDA;
 }

@@ -131,6 +131,37 @@ struct Mma {
       if (threadIdx.x == 0) atomicExch(err, 1);
     }
   }
+  // Training's backward step of one layer, as one commit: the weight gradient
+  // D[128 x 64] = delta^T a over the tile's 128 rows into TMEM columns [64, 128) (row o < O of D
+  // is dW[o][0..64); rows O..127 read other bytes of the tile and are not used), and with
+  // next_addr != 0 the next layer's error signal delta W_l (next_addr: W_l^T [64][O]) into
+  // columns [0, 64). delta: [row][o] bf16 K-major over O columns at d_addr, which the weight
+  // gradient reads as an MN-major operand (o contiguous), as it reads the activations a:
+  // [row][i] over 64 columns at a_addr. MN-major descriptors: SBO = byte stride between 8-element
+  // blocks along M (or N), LBO = byte stride between 8-row blocks along K.
+  __device__ __forceinline__ void run_backward(uint32_t d_addr, int O, uint32_t a_addr, uint32_t next_addr) {
+    if (threadIdx.x == 0) {
+      const uint32_t d_rows = (uint32_t)(O / 8) * 128, a_rows = (uint32_t)(kK / 8) * 128;
+      const uint32_t idesc_w = xbd::idesc_bf16_f32(kTile, kK) | (1u << 15) | (1u << 16);
+      for (int j = 0; j < kTile / 16; ++j)
+        xbd::mma_bf16(tmem + 64, xbd::smem_desc(d_addr + j * 2 * d_rows, d_rows, 128),
+                      xbd::smem_desc(a_addr + j * 2 * a_rows, a_rows, 128), idesc_w, j > 0 ? 1u : 0u);
+      if (next_addr) {
+        const uint32_t sbo = (uint32_t)(O / 8) * 128;
+        for (int j = 0; j < O / 16; ++j)
+          xbd::mma_bf16(tmem, xbd::smem_desc(d_addr + j * 256, 128, sbo), xbd::smem_desc(next_addr + j * 256, 128, sbo),
+                        xbd::idesc_bf16_f32(kTile, kHid), j > 0 ? 1u : 0u);
+      }
+      xbd::mma_commit(mbar);
+    }
+    const bool done = xbd::mbar_wait(mbar, phase);
+    phase ^= 1u;
+    xbd::fence_after_sync();
+    if (__syncthreads_or(done ? 0 : 1)) {
+      ok = false;
+      if (threadIdx.x == 0) atomicExch(err, 1);
+    }
+  }
   // This thread's row (TMEM lane = threadIdx.x), columns [c, c + 16).
   __device__ __forceinline__ void load16(int c, float* v) const {
     const uint32_t warp = threadIdx.x >> 5;
@@ -139,9 +170,10 @@ struct Mma {
   }
 };
 
-__device__ __forceinline__ void mma_setup(uint32_t* tmem_slot, uint64_t* mbar) {
+// ncols: TMEM columns of the CTA (64; training 128: its weight gradients use columns 64..127).
+__device__ __forceinline__ void mma_setup(uint32_t* tmem_slot, uint64_t* mbar, uint32_t ncols = 64) {
   if ((threadIdx.x >> 5) == 0) {
-    xbd::tmem_alloc(tmem_slot, 64);
+    xbd::tmem_alloc(tmem_slot, ncols);
     xbd::tmem_relinquish();
   }
   if (threadIdx.x == 0) {
@@ -153,10 +185,10 @@ __device__ __forceinline__ void mma_setup(uint32_t* tmem_slot, uint64_t* mbar) {
   xbd::fence_after_sync();
 }
 
-__device__ __forceinline__ void mma_teardown(uint32_t tmem) {
+__device__ __forceinline__ void mma_teardown(uint32_t tmem, uint32_t ncols = 64) {
   xbd::fence_before_sync();
   __syncthreads();
-  if ((threadIdx.x >> 5) == 0) xbd::tmem_dealloc(tmem, 64);
+  if ((threadIdx.x >> 5) == 0) xbd::tmem_dealloc(tmem, ncols);
 }
 
 // Hidden-layer epilogue: this thread's row of TMEM + bias, ReLU, to bf16 in `dst`.
