@@ -798,11 +798,12 @@ def main():
                    "unlike `value`); each step's mean image is read back by xb_resolve_async, "
                    "overlapping the next step, and xb_sync ends the timed region"}
 
-    # the single exchange of the multi-GPU path: framebuffer reduce to rank 0 (untimed)
+    # the single exchange of the multi-GPU path: the per-pixel sums reduced to rank 0 on the
+    # device (untimed; xenon_b200.distributed)
     if ws > 1:
         import torch.distributed as dist
-        img = torch.from_numpy(r.resolve()).cuda()
-        dist.reduce(img, dst=0)
+        from xenon_b200 import distributed
+        dist.reduce(distributed._local_moments(r, max(r.spp, 1), "cuda"), dst=0)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

@@ -345,6 +345,10 @@ int  xb_resolve_async(xb_renderer *r, float *out_rgb);
 int  xb_sync(xb_renderer *r);
 /* FP64 per-pixel sums and Welford M2 (needs XB_FLAG_FP64_ACCUM); each double[W*H*3]. */
 int  xb_resolve_fp64(xb_renderer *r, double *sum_rgb, double *m2_rgb);
+/* The same into device memory of the renderer's GPU (top-down rows; either pointer may be NULL),
+ * complete when the call returns: what a multi-GPU caller sums across GPUs (NCCL) without a
+ * round trip through the host. No reference counterpart (the reference renders on one device). */
+int  xb_resolve_fp64_device(xb_renderer *r, double *sum_rgb, double *m2_rgb);
 
 /* Output stage, on the host over an image as xb_resolve returns it (float[W*H*3], first row the
  * bottom of the image as in the reference's framebuffer). The reference does this inside its

@@ -247,3 +247,33 @@ def test_resolve_async_matches_resolve():
     assert np.array_equal(outs[-1], r.resolve())
     assert not np.array_equal(outs[0], outs[-1])
     r.close()
+
+
+@pytest.mark.gpu
+def test_fp64_sums_on_the_device_equal_the_host_copy():
+    """xb_resolve_fp64_device (the multi-GPU exchange's input) gives the bytes xb_resolve_fp64
+    gives, and the per-rank moments of the device path equal those of the host path."""
+    import torch
+
+    from xenon_b200 import distributed
+    desc = scenes.cornell()
+    r = gpu_render(desc, 1, 5, 40, 24, fp64=True)
+    s, m2 = r.resolve_fp64()
+    ds = torch.empty((24, 40, 3), dtype=torch.float64, device="cuda")
+    dm = torch.empty_like(ds)
+    r.resolve_fp64_device(ds.data_ptr(), dm.data_ptr())
+    assert ds.cpu().numpy().tobytes() == s.tobytes()
+    assert dm.cpu().numpy().tobytes() == m2.tobytes()
+    dev = distributed._local_moments(r, 5, "cuda").cpu().numpy()
+    host = distributed._local_moments(_HostOnly(r), 5, "cpu").numpy()
+    assert np.array_equal(dev, host)
+
+
+class _HostOnly:
+    """A renderer seen without its device resolve (the host path of the exchange)."""
+
+    def __init__(self, r):
+        self.r, self.fp64, self.width, self.height = r, True, r.width, r.height
+
+    def resolve_fp64(self):
+        return self.r.resolve_fp64()

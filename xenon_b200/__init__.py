@@ -227,6 +227,12 @@ class Renderer:
         self._check(lib().xb_resolve_fp64(self.h, _p(s), _p(m2)))
         return s, m2
 
+    def resolve_fp64_device(self, sum_ptr: int, m2_ptr: int = 0) -> None:
+        """xb_resolve_fp64_device: FP64 sums and Welford M2 (top-down rows) into device buffers
+        of W*H*3 doubles on the renderer's GPU (e.g. torch tensors' data_ptr(); 0 skips one)."""
+        self._check(lib().xb_resolve_fp64_device(self.h, ctypes.c_void_p(sum_ptr) if sum_ptr else None,
+                                                 ctypes.c_void_p(m2_ptr) if m2_ptr else None))
+
     @property
     def spp(self) -> int:
         return int(lib().xb_get_spp(self.h))

@@ -1958,6 +1958,16 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
   return XB_OK;
 }
 
+// Rows of `rows` x `row` doubles copied with their order reversed (bottom-up accumulation order
+// to the top-down order of the resolved image, cpu_tiled.cpp:224-236).
+__global__ void flip_rows_f64_kernel(const double* __restrict__ src, double* __restrict__ dst, int row, int rows) {
+  const int64_t n = (int64_t)row * rows;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t y = i / row, x = i - y * row;
+    dst[(rows - 1 - y) * (int64_t)row + x] = src[i];
+  }
+}
+
 // ── BLAS refit (xb_refit_mesh): one mesh's triangles and node boxes, topology kept ──────────
 // The passes are refit_kernels.h's, which the host refit (xb_scene_refit_mesh) runs as loops.
 __global__ void refit_tris_kernel(xb::RefitArgs a) {
@@ -2623,6 +2633,28 @@ int xb_resolve_fp64(xb_renderer* r, double* sum, double* m2) {
     CK(cudaStreamSynchronize(r->stream));
     for (int y = 0; y < H; ++y) std::memcpy(outs[k] + (size_t)(H - 1 - y) * row, tmp.data() + (size_t)y * row, row * sizeof(double));
   }
+  return XB_OK;
+}
+
+int xb_resolve_fp64_device(xb_renderer* r, double* sum, double* m2) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  if (!r->sum64) return set_err(r, XB_E_STATE, "renderer was created without XB_FLAG_FP64_ACCUM");
+  const int W = r->cfg.width, H = r->cfg.height;
+  double* outs[2] = {sum, m2};
+  const double* srcs[2] = {r->sum64, r->m2_64};
+  for (int k = 0; k < 2; ++k) {
+    if (!outs[k]) continue;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, outs[k]) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
+        at.device != r->cfg.device)
+      return set_err(r, XB_E_INVALID, "xb_resolve_fp64_device: output %d is not device memory of GPU %d", k,
+                     r->cfg.device);
+    flip_rows_f64_kernel<<<std::min<int64_t>((int64_t)H * W * 3 / 256 + 1, (int64_t)r->num_sms * 8), 256, 0,
+                           r->stream>>>(srcs[k], outs[k], W * 3, H);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(r->stream));
   return XB_OK;
 }
 

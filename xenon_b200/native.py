@@ -49,6 +49,7 @@ SIGNATURES = {
     "xb_render_range": ([_P, _P, _I32, _I32], _I),
     "xb_resolve": ([_P, _P], _I),
     "xb_resolve_fp64": ([_P, _P, _P], _I),
+    "xb_resolve_fp64_device": ([_P, _P, _P], _I),
     "xb_get_spp": ([_P], _I),
     "xb_reset": ([_P], _I),
     "xb_get_render_stats": ([_P, _P], _I),
