@@ -77,6 +77,8 @@ def parse():
                     help="fixed probability of sampling the network (0: learned per vertex)")
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--no-incoherent", action="store_true", help="skip the incoherent-ray traversal bench")
+    ap.add_argument("--no-sky-study", action="store_true", help="skip the sky importance sampling study")
+    ap.add_argument("--sky-seconds", type=float, default=2.0, help="sky study: device time per method")
     ap.add_argument("--incoherent-rays", type=int, default=1 << 22)
     ap.add_argument("--detail-out", default="", help="also write the studies' full results to this JSON file")
     ap.add_argument("--guide-height", type=int, default=720)
@@ -387,6 +389,57 @@ def guiding_study(args, device: int) -> dict:
             "wall_s": time.perf_counter() - t0}
 
 
+def sky_study(args, device: int) -> dict:
+    """Sky importance sampling (XB_FLAG_SKY_IS) against the default estimator on config 2's view
+    at 960x540: equal device time (--sky-seconds per method, CUDA events of each xb_render call),
+    each image's relMSE against a plain FP64 render of 4096 samples at disjoint sample indices."""
+    import xenon_b200 as xb
+    from xenon_b200 import abi, autotune, scenes
+    W, H = args.width // 2, args.height // 2
+    desc = scenes.icosphere_scene(level=args.level, width=W, height=H)
+    hs = xb.HostScene.from_desc(desc)
+    cam = xb.camera(desc.eye, desc.target, desc.fov, W / H)
+    tuned = autotune.load_tuning("config2")
+
+    def renderer(flags=0, fp64=False):
+        r = xb.Renderer(W, H, desc.max_bounces, desc.min_bounces, device=device, fp64=fp64, flags=flags)
+        r.upload_scene(hs)
+        if tuned:
+            r.set_tuning(**tuned)
+        return r
+
+    rr = renderer(fp64=True)
+    ref_spp = 4096
+    for first in range(0, ref_spp, 512):
+        rr.render_range(cam, (1 << 24) + first, 512)
+    s64, _ = rr.resolve_fp64()
+    ref = s64 / ref_spp
+    rr.close()
+    denom = ref ** 2 + 1e-2
+
+    def equal_time(flags):
+        r = renderer(flags)
+        r.render_range(cam, 1 << 23, 8)          # warm-up (graphs, queues), not in the image
+        r.reset()
+        ms, n = 0.0, 0
+        while ms < args.sky_seconds * 1e3:
+            r.render_frame(cam, 8)
+            ms += r.stats().last_ms
+            n += 8
+        img = r.resolve().astype(np.float64)
+        r.close()
+        e = np.sort(((img - ref) ** 2 / denom).mean(2).ravel())
+        return {"spp": n, "device_ms": ms, "relmse": float(e.mean()),
+                "relmse_trimmed": float(e[: int(len(e) * 0.999)].mean()), "image_mean": float(img.mean())}
+
+    plain = equal_time(0)
+    sky = equal_time(abi.XB_FLAG_SKY_IS)
+    return {"workload": f"config2 view {W}x{H}, depth {desc.max_bounces}", "reference_spp": ref_spp,
+            "plain": plain, "sky_is": sky, "ratio_raw": plain["relmse"] / max(sky["relmse"], 1e-30),
+            "ratio_trimmed": plain["relmse_trimmed"] / max(sky["relmse_trimmed"], 1e-30),
+            "mean_reference": float(ref.mean())}
+
+
 def config3_study(args, device: int) -> dict:
     """Config 3: TLAS over 16x16 instances of 4 seeded meshes (random materials), sky + 4 quad
     lights, 1920x1080, depth 12, with its autotuned launch settings; device Mrays/s and
@@ -534,6 +587,13 @@ def incoherent_summary(inc):
     for sc in ("config2", "config3"):
         out[sc] = {k: _sig(v["mrays_per_s"]) for k, v in inc[sc].items()}
     return out
+
+
+def sky_summary(k):
+    if not k or "error" in k:
+        return k
+    return {"ratio_raw": _sig(k["ratio_raw"]), "ratio_trimmed": _sig(k["ratio_trimmed"]),
+            "spp_plain": k["plain"]["spp"], "spp_sky": k["sky_is"]["spp"]}
 
 
 def views_summary(v):
@@ -832,6 +892,12 @@ def main():
             incoherent = incoherent_study(args, local)
         except Exception as e:
             incoherent = {"error": f"{type(e).__name__}: {e}"}
+    sky = None
+    if rank == 0 and ws == 1 and not args.no_sky_study:
+        try:
+            sky = sky_study(args, local)
+        except Exception as e:
+            sky = {"error": f"{type(e).__name__}: {e}"}
     guiding = None
     if rank == 0 and ws == 1 and not args.no_guiding_study:
         try:
@@ -848,11 +914,11 @@ def main():
                                                   "accumulate_ms", "extend_busy_ms", "shade_busy_ms",
                                                   "shadow_busy_ms")}}
         studies = {"config3": config3_summary(config3), "incoherent": incoherent_summary(incoherent),
-                   "views": views_summary(views), "guiding": guiding_summary(guiding)}
+                   "views": views_summary(views), "sky_is": sky_summary(sky), "guiding": guiding_summary(guiding)}
         if args.detail_out:
             with open(args.detail_out, "w") as f:
                 json.dump({"detail": detail, "config3": config3, "incoherent": incoherent, "views": views,
-                           "guiding": guiding}, f, indent=1)
+                           "sky_is": sky, "guiding": guiding}, f, indent=1)
         line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",

@@ -281,6 +281,14 @@ typedef struct xb_renderer xb_renderer;
                                        contribution f cos E / P(pick), MIS weight 1. Off (parity):
                                        the reference's 1e8 divisor (src/render/cpu_tiled.cpp:166-183),
                                        with which a sun adds about 1e-8 of its light */
+#define XB_FLAG_SKY_IS          8   /* sky importance sampling: at non-delta, non-transmissive
+                                       vertices seen from the front, the next direction comes from
+                                       the one-sample MIS mixture of the sky's luminance
+                                       distribution (probability 1/2) and the BSDF sampler; the path
+                                       carries the importance ratio, so the image converges to the
+                                       default one (the sky is weighted by 1 in
+                                       src/render/cpu_tiled.cpp:40-54). Ignored while guiding is on.
+                                       Changes the random-number draws (not in parity mode). */
 
 typedef struct xb_config {
   int32_t width, height;

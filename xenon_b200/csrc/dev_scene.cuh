@@ -114,7 +114,35 @@ struct DevScene {
   float sky_inv_sharpness;
   float sky_intensity;
   int32_t sun_nee;   // XB_FLAG_SUN_NEE: directional lights weighted as delta lights (else the reference's 1e8)
+  const float* sky_cdf;   // XB_FLAG_SKY_IS: kSkyBins + 1 cumulative bin masses over y in [-1, 1] (or nullptr)
 };
+
+// The sky's luminance distribution over directions. The gradient sky (Environment::evaluate)
+// depends on the direction's y alone, so its distribution is a piecewise-constant density of y
+// over kSkyBins equal bins of [-1, 1] times a uniform azimuth: pdf(w) = mass(bin(w.y)) / (dy 2 pi).
+constexpr int kSkyBins = 256;
+
+__device__ __forceinline__ float sky_pdf(const float* cdf, V3 d) {
+  int b = (int)((d.y + 1.f) * (0.5f * kSkyBins));
+  b = b < 0 ? 0 : (b > kSkyBins - 1 ? kSkyBins - 1 : b);
+  return (__ldg(cdf + b + 1) - __ldg(cdf + b)) * ((float)kSkyBins / (4.f * 3.14159265358979f));
+}
+
+__device__ __forceinline__ V3 sky_sample(const float* cdf, float u0, float u1) {
+  int lo = 0, hi = kSkyBins;                 // the bin b with cdf[b] <= u0 < cdf[b + 1]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(cdf + mid) <= u0) lo = mid;
+    else hi = mid;
+  }
+  const float c0 = __ldg(cdf + lo), c1 = __ldg(cdf + lo + 1);
+  const float t = c1 > c0 ? fminf(fmaxf((u0 - c0) / (c1 - c0), 0.f), 1.f) : 0.5f;
+  const float y = fminf(fmaxf(-1.f + ((float)lo + t) * (2.f / kSkyBins), -1.f), 1.f);
+  const float rr = sqrtf(fmaxf(0.f, 1.f - y * y));
+  float sp, cp;
+  sincospif(2.f * u1, &sp, &cp);
+  return v3(rr * cp, y, rr * sp);
+}
 
 struct Ray {
   V3 o, d;

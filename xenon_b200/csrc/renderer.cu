@@ -581,6 +581,7 @@ struct GuideShadeArgs {
   int* err;
   float4* gq[5];             // two-kernel form: the deferred vertices (nullptr: fused form)
   uint64_t* gq_rng;
+  float sky_alpha;           // network-free form with XB_FLAG_SKY_IS: probability of the sky proposal
 };
 
 constexpr float kNaN = __builtin_nanf("");
@@ -682,8 +683,8 @@ __global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(Shad
           // its sampler refracts about (and its pdf can be NaN there), so neither its pdf nor a
           // corrected form of it is the density of what its sampler returns.
           const uint32_t mf = sc.mats[fh.mat_id].flags;
-          guided = (kNet || g.gq[0] != nullptr) && (mf & (kMatDelta | kMatTransmissive)) == 0 &&
-                   dot(fh.normal, -ray.d) > 0.f;
+          guided = (kNet || g.gq[0] != nullptr || g.sky_alpha > 0.f) &&
+                   (mf & (kMatDelta | kMatTransmissive)) == 0 && dot(fh.normal, -ray.d) > 0.f;
           for (int k = 0; k < 3; ++k) {
             const float pk = (k == 0 ? fh.pos.x : k == 1 ? fh.pos.y : fh.pos.z);
             feat[k] = fminf(fmaxf((pk - g.bmin[k]) * g.binv[k], 0.f), 1.f);
@@ -786,7 +787,7 @@ __global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(Shad
         tp = tp / p;
         ratio = ratio * (surv / surv_g);
       }
-      if (!kNet && guided) {
+      if (!kNet && guided && g.gq[0] != nullptr) {
         // two-kernel form: the network pass samples this vertex's direction
         dq[0] = make_float4(fh.pos.x, fh.pos.y, fh.pos.z, __int_as_float(fh.mat_id));
         dq[1] = make_float4(fh.normal.x, fh.normal.y, fh.normal.z, __int_as_float(pid));
@@ -806,12 +807,19 @@ __global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(Shad
         if (!bsdf_sample(wo_l, mat, rng, s)) break;
         wiw = onb.to_world(s.wi);
       } else {
+        // the proposal: the network's mixture (kNet) or the sky's luminance distribution
         float pb;
-        if (rng.next_float() < alpha) {
-          const float u0 = rng.next_float(), u1 = rng.next_float(), u2 = rng.next_float();
-          float d[3];
-          xbg::mix_sample(lob, u0, u1, u2, d);
-          wiw = v3(d[0], d[1], d[2]);
+        const float ap = kNet ? alpha : g.sky_alpha;
+        if (rng.next_float() < ap) {
+          if constexpr (kNet) {
+            const float u0 = rng.next_float(), u1 = rng.next_float(), u2 = rng.next_float();
+            float d[3];
+            xbg::mix_sample(lob, u0, u1, u2, d);
+            wiw = v3(d[0], d[1], d[2]);
+          } else {
+            const float u0 = rng.next_float(), u1 = rng.next_float();
+            wiw = sky_sample(sc.sky_cdf, u0, u1);
+          }
           s.wi = onb.to_local(wiw);
           s.delta = false;
           if (!bsdf_lobe_for_direction(wo_l, s.wi, mat, rng.next_float(), s.f, s.pdf, pb)) break;
@@ -820,7 +828,8 @@ __global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(Shad
           wiw = onb.to_world(s.wi);
           pb = bsdf_density(wo_l, s.wi, mat);
         }
-        const float pm = alpha * xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) + (1.f - alpha) * pb;
+        const float q = kNet ? xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) : sky_pdf(sc.sky_cdf, wiw);
+        const float pm = ap * q + (1.f - ap) * pb;
         if (!(pm > 0.f)) break;
         n_ratio = ratio * (pb / pm);
         if (training && (pid % g.rec_stride) == 0) {
@@ -1310,6 +1319,34 @@ __global__ void __launch_bounds__(128) trace_stealing_kernel(DevScene sc, const 
   if (overflow) atomicAdd(stats + STAT_OVERFLOW, 1ull);
 }
 
+// XB_FLAG_SKY_IS: the sky's luminance (Rec. 709 weights) at the centre of each of kSkyBins bins
+// of y = cos(theta) in [-1, 1], by Environment::evaluate's formula (src/scene/environment.h:34-46),
+// floored at 1e-3 of the largest so that every direction can be proposed, as normalised
+// cumulative masses. False when the sky is black.
+bool sky_table(const DevScene& sc, std::vector<float>& cdf) {
+  std::vector<double> f(kSkyBins);
+  double fmax = 0.0;
+  for (int b = 0; b < kSkyBins; ++b) {
+    const double y = -1.0 + (b + 0.5) * (2.0 / kSkyBins);
+    double c[3];
+    for (int k = 0; k < 3; ++k) {
+      const double hz = sc.sky_horizon[k];
+      c[k] = y < 0.0 ? hz + (sc.sky_ground[k] - hz) * std::min(-y, 1.0)
+                     : hz + (sc.sky_zenith[k] - hz) * std::pow(y, (double)sc.sky_inv_sharpness);
+      c[k] *= sc.sky_intensity;
+    }
+    f[b] = std::max(0.0, 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2]);
+    fmax = std::max(fmax, f[b]);
+  }
+  if (!(fmax > 0.0)) return false;
+  cdf.assign(kSkyBins + 1, 0.f);
+  std::vector<double> acc(kSkyBins + 1, 0.0);
+  for (int b = 0; b < kSkyBins; ++b) acc[b + 1] = acc[b] + std::max(f[b], 1e-3 * fmax);
+  for (int b = 0; b <= kSkyBins; ++b) cdf[b] = (float)(acc[b] / acc[kSkyBins]);
+  cdf[kSkyBins] = 1.f;
+  return true;
+}
+
 DevMaterial to_dev_material(const xb_material& m) {
   xb_material_derived d = xb::prepare_material(m);
   DevMaterial o{};
@@ -1688,6 +1725,17 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
         else
           guided_shade_kernel<false, 8><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
       }
+    } else if (r->scene.sky_cdf) {
+      // sky importance sampling: the network-free guided bounce with the sky as its proposal
+      ga.ratio_in = d > 0 ? w.ratio[q] : nullptr;
+      ga.ratio_out = w.ratio[nq];
+      ga.rec_stride = 1;
+      ga.sky_alpha = 0.5f;
+      StageTimer t(r, STAGE_SHADE, L.s);
+      if (r->tune.shade_occupancy == 4)
+        guided_shade_kernel<false, 4><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
+      else
+        guided_shade_kernel<false, 8><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
     } else {
       StageTimer t(r, STAGE_SHADE, L.s);
       if (r->tune.shade_occupancy == 4) shade_kernel<4><<<r->grid_shade, 128, 0, L.s>>>(sa);
@@ -2339,6 +2387,10 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   sc.sky_inv_sharpness = 1.0f / v->sky.sharpness;
   sc.sky_intensity = v->sky.intensity;
   sc.sun_nee = (r->cfg.flags & XB_FLAG_SUN_NEE) != 0;
+  if ((r->cfg.flags & XB_FLAG_SKY_IS) && sc.sky_intensity > 0.f) {
+    std::vector<float> cdf;
+    if (sky_table(sc, cdf) && (rc = dev_upload(r, cdf, &sc.sky_cdf))) return rc;
+  }
   r->has_scene = true;
   return XB_OK;
 }
