@@ -533,6 +533,23 @@ def views_study(args, device: int) -> dict:
     g.reset_stats()
     guided_imgs = g.render_views(views)
     guided_ms = g.stats().last_ms
+    # aggregate throughput at the configuration's own spp draws ({16, 64, 256, 1024}, no cap):
+    # the same 32 views, plain and guided (the trained network), each in one xb_render_views call
+    full = None
+    if args.views_max_spp:
+        fspecs = scenes.config5_views(desc, 32, seed=1, max_spp=0)
+        fviews = [(c, w, h, spp, mb) for c, (_, _, _, w, h, spp, mb) in zip(cams, fspecs)]
+        fpaths = sum(w * h * spp for (_, w, h, spp, _) in fviews)
+        g.reset_stats()
+        g.render_views(fviews)
+        fg_ms = g.stats().last_ms
+        rp = renderer()
+        rp.reset_stats()
+        rp.render_views(fviews)
+        fp_ms = rp.stats().last_ms
+        rp.close()
+        full = {"paths": fpaths, "spp": [v[3] for v in fviews], "plain_batched_msamples_per_s": fpaths / fp_ms / 1e3,
+                "guided_msamples_per_s": fpaths / fg_ms / 1e3, "plain_ms": fp_ms, "guided_ms": fg_ms}
     g.close()
 
     def relmse(img, ref):
@@ -561,6 +578,7 @@ def views_study(args, device: int) -> dict:
             "relmse_ratio_plain_over_guided_median": float(np.median(raw)),
             "relmse_ratio_plain_over_guided_median_trimmed": float(np.median(trim)),
             "relmse_ratio_equal_time_median_trimmed": float(np.median(trim)) * speed,
+            "full_spp": full,
             "relmse": "mean over pixels of (x - ref)^2 / (ref^2 + 0.01); trimmed: without the 0.1% largest pixels",
             "reference": "plain renders of the same views with 4x the samples", "per_view": per_view}
 
@@ -603,7 +621,11 @@ def views_summary(v):
     keep = ("guided_msamples_per_s", "plain_batched_msamples_per_s", "plain_one_by_one_msamples_per_s",
             "relmse_ratio_plain_over_guided_median", "relmse_ratio_plain_over_guided_median_trimmed",
             "relmse_ratio_equal_time_median_trimmed")
-    return {"workload": "config5: 32 views of config 3", **{k: _sig(v[k]) for k in keep}}
+    out = {"workload": "config5: 32 views of config 3", **{k: _sig(v[k]) for k in keep}}
+    if v.get("full_spp"):
+        out["full_spp_plain_msamples_per_s"] = _sig(v["full_spp"]["plain_batched_msamples_per_s"])
+        out["full_spp_guided_msamples_per_s"] = _sig(v["full_spp"]["guided_msamples_per_s"])
+    return out
 
 
 def guiding_summary(g):

@@ -10,6 +10,14 @@
     python -m xenon_b200.profile_cases config2 [W H SPP]    config-2 scene, its tuning, SPP samples
                                                             (default 640x360, 2): prints the rays
     python -m xenon_b200.profile_cases config3 [SPP]        config-3 scene at full size, its tuning
+    python -m xenon_b200.profile_cases config2_wave [SS]    config-2 scene at 1920x1080, one sample as
+                                                            one wave (2,073,600 paths, one lane, direct
+                                                            launches; under 1 GB of queues): every
+                                                            kernel of a bounce at its full size; SS = 16
+                                                            keeps 16 BLAS stack entries in shared memory
+    python -m xenon_b200.profile_cases trace_uniform [N]    2^N (default 22) incoherent rays on the config-2
+                                                            scene through xb_trace_rays_device, closest
+                                                            then any hit
 
 Each case prints one line and exits 0; it renders a handful of samples so a capture of one
 launch ends quickly.
@@ -89,7 +97,37 @@ def config3(spp: int = 8) -> None:
     print("config3 spp", spp, "rays_closest", st.rays_closest, "rays_shadow", st.rays_shadow, "ms", st.last_ms)
 
 
-CASES = {"shadow_d0": shadow_d0, "guide_small": guide_small, "guided_room": guided_room,
+def config2_wave(shared_stack: int = 1) -> None:
+    xb, autotune, scenes = _lib()
+    desc = scenes.icosphere_scene(level=8)
+    w, h = desc.width, desc.height
+    r = xb.Renderer(w, h, desc.max_bounces, desc.min_bounces)
+    r.upload_scene(xb.HostScene.from_desc(desc))
+    r.set_tuning(**autotune.load_tuning("config2"))
+    r.set_tuning(waves=1, wave_paths=w * h, graph=2, shared_stack=shared_stack)
+    r.render_frame(xb.camera(desc.eye, desc.target, desc.fov, w / h), 1)
+    st = r.stats()
+    print("config2_wave rays_closest", st.rays_closest, "rays_shadow", st.rays_shadow, "ms", st.last_ms)
+
+
+def trace_uniform(log2n: int = 22) -> None:
+    xb, _, scenes = _lib()
+    import torch
+    from xenon_b200 import abi, raybatch
+    desc = scenes.icosphere_scene(level=8)
+    hs = xb.HostScene.from_desc(desc)
+    r = xb.Renderer(64, 64)
+    r.upload_scene(hs)
+    rays = raybatch.incoherent_rays(hs.view(), 1 << log2n, seed=5)
+    d_rays = torch.from_numpy(rays.view("u1").reshape(-1)).cuda()
+    d_hits = torch.empty(len(rays) * abi.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    for mode in (abi.XB_TRACE_CLOSEST, abi.XB_TRACE_ANY):
+        r.trace_rays_device(d_rays.data_ptr(), len(rays), d_hits.data_ptr(), mode)
+    torch.cuda.synchronize()
+    print("trace_uniform rays", len(rays))
+
+
+CASES = {"config2_wave": config2_wave, "trace_uniform": trace_uniform, "shadow_d0": shadow_d0, "guide_small": guide_small, "guided_room": guided_room,
          "plain_room": plain_room, "config2": config2, "config3": config3}
 
 if __name__ == "__main__":
