@@ -18,11 +18,19 @@ sample of every pixel (2,073,600 paths: camera rays, bounce rays and NEE shadow 
                threads) on a bounded sample of the same view; its Mrays/s uses the rays per path
                this GPU run measured (the reference counts no rays)
 
+Studies at the end of the line (their full results with --detail-out): config3 (throughput of
+config 3), incoherent (traversal alone on 2^22 incoherent and 2^22 bounce-2 rays, config 2 and 3),
+views (config 5), sky_is (sky importance sampling at equal time) and guiding (config 4, equal-time
+relMSE of guided vs plain: the second half of the metric).
+
 Multi-GPU (torchrun): each rank renders its own sample indices (rank r renders samples
 r*K+1 ...), so per-GPU work is fixed (weak scaling); the only exchange is one NCCL reduce of
 the framebuffer after the timed region.
 
---impl reference times the reference's CPU implementation of this path on the host cores.
+--impl reference times the reference's CPU implementation of this path on the host cores
+(oracle/_ref: render_frame_tiled with its Release flags, every host thread, about one second of
+samples per step on 1/64 of the view's pixels); its process loads no library of this package,
+and its `config` is this arm's.
 """
 from __future__ import annotations
 
