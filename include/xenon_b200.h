@@ -384,6 +384,15 @@ typedef struct xb_noise_stats {
 int  xb_image_to_rgb8(const float *rgb, int32_t width, int32_t height, uint8_t *out_rgb8);
 int  xb_write_png(const char *path, const float *rgb, int32_t width, int32_t height);
 int  xb_image_noise_stats(const float *rgb, int32_t width, int32_t height, xb_noise_stats *out);
+/* The same output stage on the device, over the renderer's current mean image (what xb_resolve
+ * would return) right after accumulation, without the image leaving the GPU: rgb8 (host
+ * uint8[W*H*3], or NULL) receives xb_image_to_rgb8's pixels, stats (or NULL) the noise
+ * statistics. Per-pixel values follow the same float operations as the host forms; the FP64
+ * sums are reduced per block, so the mean scores can differ from the host's in the last bit of
+ * the float, and the 8-bit values where CUDA's powf and the host's round the gamma differently. */
+int  xb_output_stage(xb_renderer *r, uint8_t *rgb8, xb_noise_stats *stats);
+/* 8-bit pixels as xb_image_to_rgb8 (or xb_output_stage) returns them, written as xb_write_png writes. */
+int  xb_write_png_rgb8(const char *path, const uint8_t *rgb8, int32_t width, int32_t height);
 int  xb_get_spp(const xb_renderer *r);
 int  xb_reset(xb_renderer *r);
 /* Renders samples [spp_first, spp_first + spp_count) of the sequence (1-based), e.g. one shard

@@ -109,3 +109,14 @@ int main() {{
     assert out[2:] == ["error", str(-5)]                    # XB_E_IO
     xb.write_png(str(tmp_path / "py.png"), img)
     assert (tmp_path / "cpp.png").read_bytes() == (tmp_path / "py.png").read_bytes()
+
+
+def test_png_from_8bit_pixels_equals_png_from_the_image(tmp_path):
+    """xb_write_png_rgb8 over xb_image_to_rgb8's pixels writes the same file as xb_write_png."""
+    import xenon_b200 as xb
+    rng = np.random.default_rng(4)
+    img = (rng.random((37, 53, 3)) * 1.3 - 0.1).astype(np.float32)
+    a, b = tmp_path / "a.png", tmp_path / "b.png"
+    xb.write_png(str(a), img)
+    xb.write_png_rgb8(str(b), xb.image_to_rgb8(img))
+    assert a.read_bytes() == b.read_bytes()

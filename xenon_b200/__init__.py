@@ -227,6 +227,15 @@ class Renderer:
         self._check(lib().xb_resolve_fp64(self.h, _p(s), _p(m2)))
         return s, m2
 
+    def output_stage(self, rgb8: bool = True, stats: bool = True):
+        """xb_output_stage: the PNG's 8-bit pixels (H, W, 3) and the noise statistics of the current
+        mean image, computed on the device; returns (rgb8 or None, stats dict or None)."""
+        pix = np.empty((self.height, self.width, 3), np.uint8) if rgb8 else None
+        st = abi.NoiseStats() if stats else None
+        self._check(lib().xb_output_stage(self.h, _p(pix) if pix is not None else None,
+                                          ctypes.byref(st) if st is not None else None))
+        return pix, (st.as_dict() if st is not None else None)
+
     def resolve_fp64_device(self, sum_ptr: int, m2_ptr: int = 0) -> None:
         """xb_resolve_fp64_device: FP64 sums and Welford M2 (top-down rows) into device buffers
         of W*H*3 doubles on the renderer's GPU (e.g. torch tensors' data_ptr(); 0 skips one)."""
@@ -327,6 +336,13 @@ def write_png(path: str, rgb: np.ndarray) -> None:
     img = np.ascontiguousarray(rgb, np.float32)
     h, w = img.shape[:2]
     check(lib().xb_write_png(str(path).encode(), _p(img), w, h))
+
+
+def write_png_rgb8(path: str, rgb8: np.ndarray) -> None:
+    """xb_write_png_rgb8: 8-bit pixels (H, W, 3), top row first, as a PNG file."""
+    pix = np.ascontiguousarray(rgb8, np.uint8)
+    h, w = pix.shape[:2]
+    check(lib().xb_write_png_rgb8(str(path).encode(), _p(pix), w, h))
 
 
 def noise_stats(rgb: np.ndarray) -> dict:

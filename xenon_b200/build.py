@@ -20,7 +20,7 @@ LIB = os.path.join(LIBDIR, "libxenon_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 CXX_SRCS = ["scene_host.cpp", "bvh_levels.cpp", "loaders.cpp", "capi_scene.cpp", "image_out.cpp"]
-CU_STRICT = ["renderer.cu", "bvh_device.cu"]
+CU_STRICT = ["renderer.cu", "bvh_device.cu", "output_dev.cu"]
 CU_FAST = ["guide.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"

@@ -89,15 +89,21 @@ int xb_image_to_rgb8(const float* rgb, int32_t width, int32_t height, uint8_t* o
 int xb_write_png(const char* path, const float* rgb, int32_t width, int32_t height) {
   if (!path || !rgb || width <= 0 || height <= 0 || (int64_t)width * 3 + 1 > 65535 * 16)
     return xb::fail(XB_E_INVALID, "xb_write_png: bad arguments");
-  const int64_t row = (int64_t)width * 3;
-  std::vector<uint8_t> pix((size_t)(row * height));
+  std::vector<uint8_t> pix((size_t)((int64_t)width * 3 * height));
   xb_image_to_rgb8(rgb, width, height, pix.data());
+  return xb_write_png_rgb8(path, pix.data(), width, height);
+}
+
+int xb_write_png_rgb8(const char* path, const uint8_t* pix, int32_t width, int32_t height) {
+  if (!path || !pix || width <= 0 || height <= 0 || (int64_t)width * 3 + 1 > 65535 * 16)
+    return xb::fail(XB_E_INVALID, "xb_write_png_rgb8: bad arguments");
+  const int64_t row = (int64_t)width * 3;
   // scanlines with filter type 0, in a zlib stream of stored (uncompressed) deflate blocks
   std::vector<uint8_t> raw;
   raw.reserve((size_t)((row + 1) * height));
   for (int64_t r = 0; r < height; ++r) {
     raw.push_back(0);
-    raw.insert(raw.end(), pix.begin() + r * row, pix.begin() + (r + 1) * row);
+    raw.insert(raw.end(), pix + r * row, pix + (r + 1) * row);
   }
   std::vector<uint8_t> z = {0x78, 0x01};
   size_t pos = 0;

@@ -36,6 +36,7 @@
 #include "bvh_refit.h"
 #include "refit_kernels.h"
 #include "capi_common.h"
+#include "output_dev.h"
 #include "dev_bsdf.cuh"
 #include "dev_math.cuh"
 #include "dev_scene.cuh"
@@ -2666,6 +2667,18 @@ int xb_resolve(xb_renderer* r, float* out) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, r->resolve_buf, (size_t)W * H * 3 * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
   CK(cudaStreamSynchronize(r->stream));
+  return XB_OK;
+}
+
+int xb_output_stage(xb_renderer* r, uint8_t* rgb8, xb_noise_stats* stats) {
+  int rc = check_ready(r);
+  if (rc) return rc;
+  const int W = r->cfg.width, H = r->cfg.height;
+  const float inv = r->spp > 0 ? 1.0f / (float)r->spp : 0.f;
+  resolve_kernel<<<r->num_sms * 8, 256, 0, r->stream>>>(r->accum, W, H, inv, r->resolve_buf);
+  CK(cudaGetLastError());
+  rc = xb::device_output_stage(r->resolve_buf, W, H, r->num_sms, r->stream, rgb8, stats);
+  if (rc) return set_err(r, rc, "%s", xb::g_last_error.c_str());
   return XB_OK;
 }
 

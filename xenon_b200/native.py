@@ -72,6 +72,8 @@ SIGNATURES = {
     "xb_image_to_rgb8": ([_P, _I, _I, _P], _I),
     "xb_write_png": ([ctypes.c_char_p, _P, _I, _I], _I),
     "xb_image_noise_stats": ([_P, _I, _I, _P], _I),
+    "xb_output_stage": ([_P, _P, _P], _I),
+    "xb_write_png_rgb8": ([ctypes.c_char_p, _P, _I, _I], _I),
     "xb_set_guiding": ([_P, _P], _I),
     "xb_get_guiding": ([_P, _P], _I),
     "xb_get_guiding_stats": ([_P, _P], _I),
