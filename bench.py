@@ -676,7 +676,8 @@ def incoherent_study(args, device: int) -> dict:
                    "bounce2": raybatch.secondary_rays(r, desc.materials, cam, desc.width, desc.height, n,
                                                       seed=6, bounce=2)}
         res = {}
-        stream = torch.cuda.current_stream()
+        # the launches and the events on one explicit stream (handle 0 would mean the renderer's own)
+        stream = torch.cuda.Stream()
         for bname, rays in batches.items():
             d_rays = torch.from_numpy(rays.view(np.uint8).reshape(-1)).to("cuda")
             d_hits = torch.empty(len(rays) * abi.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
@@ -702,7 +703,7 @@ def incoherent_study(args, device: int) -> dict:
                     ev[0].record(stream)
                     launch()
                     ev[1].record(stream)
-                    torch.cuda.synchronize()
+                    ev[1].synchronize()
                     ms += ev[0].elapsed_time(ev[1])
                 ms /= reps
                 hits = d_hits.cpu().numpy().view(abi.HIT_DTYPE)

@@ -40,7 +40,9 @@ def test_noalloc_trace_matches_trace_device(mode):
     d_ref = torch.zeros(n * abi.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     d_a = torch.zeros_like(d_ref)
     d_b = torch.zeros_like(d_ref)
-    stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()                 # the buffers' fills (torch's stream) before the traces
+    ts = torch.cuda.Stream()                 # an explicit stream (kept alive): handle 0 means the renderer's own
+    stream = ts.cuda_stream
     L = xb.lib()
     xb.native.check(L.xb_trace_rays_device(r.h, ctypes.c_void_p(d_rays.data_ptr()), n,
                                            ctypes.c_void_p(d_ref.data_ptr()), mode, ctypes.c_void_p(stream)), r.h)
@@ -98,7 +100,9 @@ def test_noalloc_reports_stack_overflow():
     d_rays = _device_bytes(torch, rays)
     d_hits = torch.zeros(n * abi.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     L = xb.lib()
-    stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    ts = torch.cuda.Stream()
+    stream = ts.cuda_stream
     counts = []
     for fn in (L.xb_trace_rays_device, L.xb_trace_rays_noalloc):
         before = r.stats().overflow

@@ -317,6 +317,8 @@ class Renderer:
         return hits
 
     def trace_rays_device(self, rays_ptr: int, n: int, hits_ptr: int, mode: int = 0, stream: int = 0) -> None:
+        """xb_trace_rays_device on `stream` (a cudaStream_t handle; 0: the renderer's own stream,
+        which does not wait for the legacy default stream — pass torch's stream explicitly)."""
         self._check(lib().xb_trace_rays_device(self.h, ctypes.c_void_p(rays_ptr), int(n),
                                                ctypes.c_void_p(hits_ptr), int(mode),
                                                ctypes.c_void_p(stream) if stream else None))

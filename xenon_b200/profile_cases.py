@@ -123,7 +123,7 @@ def trace_uniform(log2n: int = 22) -> None:
     d_hits = torch.empty(len(rays) * abi.HIT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     for mode in (abi.XB_TRACE_CLOSEST, abi.XB_TRACE_ANY):
         r.trace_rays_device(d_rays.data_ptr(), len(rays), d_hits.data_ptr(), mode)
-    torch.cuda.synchronize()
+    r.sync()
     print("trace_uniform rays", len(rays))
 
 
