@@ -377,6 +377,10 @@ def guiding_study(args, device: int) -> dict:
         e = (img - ref) ** 2 / denom
         pix = e.mean(2).ravel()
         trimmed = np.sort(pix)[: int(len(pix) * 0.999)]
+        worst = np.argsort(pix)[-5:][::-1]
+        info["worst_pixels"] = [{"pixel": int(i), "relmse": float(pix[i]), "value": float(img.reshape(-1, 3)[i].mean()),
+                                 "reference": float(ref.reshape(-1, 3)[i].mean())} for i in worst]
+        info["pixels_relmse_over_1"] = int((pix > 1.0).sum())
         return {"spp": spp, "samples_rendered": rendered, "device_ms": ms, "relmse": float(pix.mean()),
                 "relmse_minus_reference_noise": float(pix.mean()) - ref_err,
                 "relmse_trimmed_0.1pct": float(trimmed.mean()), "image_mean": float(img.mean()), **info}
