@@ -18,8 +18,8 @@ sample of every pixel (2,073,600 paths: camera rays, bounce rays and NEE shadow 
                threads) on a bounded sample of the same view; its Mrays/s uses the rays per path
                this GPU run measured (the reference counts no rays)
 
-Studies at the end of the line (their full results with --detail-out): config3 (throughput of
-config 3), incoherent (traversal alone on 2^22 incoherent and 2^22 bounce-2 rays, config 2 and 3),
+Studies at the end of the line (their full results with --detail-out): bvh_build (config 2's
+BVH built on the host and on the device), config3 (throughput of config 3), incoherent (traversal alone on 2^22 incoherent and 2^22 bounce-2 rays, config 2 and 3),
 views (config 5), sky_is (sky importance sampling at equal time) and guiding (config 4, equal-time
 relMSE of guided vs plain: the second half of the metric).
 
@@ -86,6 +86,7 @@ def parse():
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--no-incoherent", action="store_true", help="skip the incoherent-ray traversal bench")
     ap.add_argument("--no-sky-study", action="store_true", help="skip the sky importance sampling study")
+    ap.add_argument("--no-build-study", action="store_true", help="skip the BVH build timing")
     ap.add_argument("--sky-seconds", type=float, default=2.0, help="sky study: device time per method")
     ap.add_argument("--incoherent-rays", type=int, default=1 << 22)
     ap.add_argument("--detail-out", default="", help="also write the studies' full results to this JSON file")
@@ -450,6 +451,30 @@ def sky_study(args, device: int) -> dict:
             "plain": plain, "sky_is": sky, "ratio_raw": plain["relmse"] / max(sky["relmse"], 1e-30),
             "ratio_trimmed": plain["relmse_trimmed"] / max(sky["relmse_trimmed"], 1e-30),
             "mean_reference": float(ref.mean())}
+
+
+def build_study(args) -> dict:
+    """BVH build of config 2's scene (1,310,722 triangles, binned SAH as the reference builds it):
+    wall time of the recursive host build on one thread and on every host thread, and of the
+    level-synchronous build on the device (XB_BUILD_DEVICE); all three give the same node arrays
+    (GPU tests). Median of three builds each, after one untimed device build."""
+    import xenon_b200 as xb
+    from xenon_b200 import abi, scenes
+    desc = scenes.icosphere_scene(level=args.level)
+
+    def timed(**kw):
+        t = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            xb.HostScene.from_desc(desc, **kw)
+            t.append(time.perf_counter() - t0)
+        return float(np.median(t))
+
+    xb.HostScene.from_desc(desc, build_mode=abi.XB_BUILD_DEVICE)
+    out = {"triangles": desc.num_triangles, "host_1_thread_s": timed(build_threads=1),
+           "host_all_threads_s": timed(build_threads=0), "device_s": timed(build_mode=abi.XB_BUILD_DEVICE),
+           "host_threads": os.cpu_count()}
+    return out
 
 
 def config3_study(args, device: int) -> dict:
@@ -927,6 +952,12 @@ def main():
             incoherent = incoherent_study(args, local)
         except Exception as e:
             incoherent = {"error": f"{type(e).__name__}: {e}"}
+    build = None
+    if rank == 0 and ws == 1 and not args.no_build_study:
+        try:
+            build = build_study(args)
+        except Exception as e:
+            build = {"error": f"{type(e).__name__}: {e}"}
     sky = None
     if rank == 0 and ws == 1 and not args.no_sky_study:
         try:
@@ -948,11 +979,12 @@ def main():
                                                  ("raygen_ms", "extend_ms", "shade_ms", "shadow_ms",
                                                   "accumulate_ms", "extend_busy_ms", "shade_busy_ms",
                                                   "shadow_busy_ms")}}
-        studies = {"config3": config3_summary(config3), "incoherent": incoherent_summary(incoherent),
+        studies = {"bvh_build": {k: _sig(v) for k, v in build.items()} if build and "error" not in build else build,
+                   "config3": config3_summary(config3), "incoherent": incoherent_summary(incoherent),
                    "views": views_summary(views), "sky_is": sky_summary(sky), "guiding": guiding_summary(guiding)}
         if args.detail_out:
             with open(args.detail_out, "w") as f:
-                json.dump({"detail": detail, "config3": config3, "incoherent": incoherent, "views": views,
+                json.dump({"detail": detail, "bvh_build": build, "config3": config3, "incoherent": incoherent, "views": views,
                            "sky_is": sky, "guiding": guiding}, f, indent=1)
         line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
