@@ -282,7 +282,8 @@ typedef struct xb_renderer xb_renderer;
                                        the reference's 1e8 divisor (src/render/cpu_tiled.cpp:166-183),
                                        with which a sun adds about 1e-8 of its light */
 #define XB_FLAG_SKY_IS          8   /* sky importance sampling: at non-delta, non-transmissive
-                                       vertices seen from the front, the next direction comes from
+                                       vertices seen from the front with a broad lobe (not a
+                                       conductor of GGX alpha < 0.25), the next direction comes from
                                        the one-sample MIS mixture of the sky's luminance
                                        distribution (probability 1/2) and the BSDF sampler; the path
                                        carries the importance ratio, so the image converges to the

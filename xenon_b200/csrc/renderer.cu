@@ -684,9 +684,14 @@ __global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(Shad
           // evaluates their transmission with a half vector (wo + wi / ior) other than the one
           // its sampler refracts about (and its pdf can be NaN there), so neither its pdf nor a
           // corrected form of it is the density of what its sampler returns.
-          const uint32_t mf = sc.mats[fh.mat_id].flags;
-          guided = (kNet || g.gq[0] != nullptr || g.sky_alpha > 0.f) &&
-                   (mf & (kMatDelta | kMatTransmissive)) == 0 && dot(fh.normal, -ray.d) > 0.f;
+          // The sky proposal (network-free form with XB_FLAG_SKY_IS) serves broad lobes only:
+          // a glossy conductor's lobe is rarely reached by a sky direction, so half of its
+          // samples would be lost and the other half carry twice the weight.
+          const DevMaterial& gm = sc.mats[fh.mat_id];
+          const uint32_t mf = gm.flags;
+          const bool proposal = kNet || g.gq[0] != nullptr ||
+                                (g.sky_alpha > 0.f && (!(mf & kMatConductor) || gm.alpha >= 0.25f));
+          guided = proposal && (mf & (kMatDelta | kMatTransmissive)) == 0 && dot(fh.normal, -ray.d) > 0.f;
           for (int k = 0; k < 3; ++k) {
             const float pk = (k == 0 ? fh.pos.x : k == 1 ? fh.pos.y : fh.pos.z);
             feat[k] = fminf(fmaxf((pk - g.bmin[k]) * g.binv[k], 0.f), 1.f);
