@@ -83,8 +83,6 @@ def parse():
     ap.add_argument("--guide-steps-per-spp", type=int, default=32)
     ap.add_argument("--guide-fraction", type=float, default=0.0,
                     help="fixed probability of sampling the network (0: learned per vertex)")
-    ap.add_argument("--guide-max-fraction", type=float, default=0.0,
-                    help="cap on the learned probability of sampling the network (0: the default, 0.95)")
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--no-incoherent", action="store_true", help="skip the incoherent-ray traversal bench")
     ap.add_argument("--no-sky-study", action="store_true", help="skip the sky importance sampling study")
@@ -361,8 +359,7 @@ def guiding_study(args, device: int) -> dict:
             fixed = args.guide_fraction > 0
             r.set_guiding(True, train_spp=args.guide_train_spp, steps_per_spp=args.guide_steps_per_spp,
                           batch=16384, guide_fraction=args.guide_fraction if fixed else 0.7,
-                          fixed_fraction=1 if fixed else 0, keep_training_samples=2,
-                          max_fraction=args.guide_max_fraction)
+                          fixed_fraction=1 if fixed else 0, keep_training_samples=2)
         ms, rendered, chunk = 0.0, 0, 8
         while ms < args.guide_seconds * 1e3:
             r.render_frame(cam, chunk)
@@ -376,7 +373,7 @@ def guiding_study(args, device: int) -> dict:
             info.update(r.guiding_stats())
             info["config"] = {k: v for k, v in r.guiding().items() if k in
                               ("train_spp", "steps_per_spp", "batch", "learning_rate", "guide_fraction",
-                               "fixed_fraction", "keep_training_samples", "max_fraction")}
+                               "fixed_fraction", "keep_training_samples")}
         r.close()
         e = (img - ref) ** 2 / denom
         pix = e.mean(2).ravel()

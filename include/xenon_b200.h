@@ -550,9 +550,6 @@ typedef struct xb_guiding {
   int32_t guided_bounces;   /* the network proposes at bounces 0 .. guided_bounces - 1; later
                              * vertices sample their BSDF (the path's importance ratio carries
                              * on); default: every bounce */
-  float max_fraction;       /* cap on the learned probability of sampling the network (training
-                             * and rendering use min(network's, cap)); a vertex's importance ratio
-                             * stays below 1 / (1 - cap). Default (0): 0.95, the network's range */
 } xb_guiding;
 
 /* Enables, disables or reconfigures guiding (0 fields take defaults). The first enabling, or a

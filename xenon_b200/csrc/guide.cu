@@ -114,7 +114,6 @@ struct TrainArgs {
   int cap, batch;
   uint64_t seed, t;       // tile placement of this step
   float alpha_fixed;      // selection probability the renderer uses (< 0: the network's own)
-  float alpha_max;        // cap on the network's own
   const float* csum;      // sum of the batch's weights
   const __nv_bfloat16* wf;
   const __nv_bfloat16* wb;
@@ -128,7 +127,7 @@ struct TrainArgs {
 // the mixture the renderer samples (a: the learned selection probability; pb < 0: p = q alone)
 // (oracle: loss_grad_raw).
 __device__ __forceinline__ float output_gradient(const float* raw, const float* om, float cb, float pb,
-                                                 float alpha_fixed, float alpha_max, float* g) {
+                                                 float alpha_fixed, float* g) {
   float lob[kLobeFloats];
   raw_to_lobes(raw, lob);
   float v[kLobes], cosv[kLobes], q = 0.f;
@@ -142,15 +141,13 @@ __device__ __forceinline__ float output_gradient(const float* raw, const float* 
   q = fmaxf(q, 1e-30f);
   const bool mix = pb >= 0.f;
   const bool learned = mix && alpha_fixed < 0.f;
-  const float a_net = learned ? selection(raw) : 0.f;
-  const bool capped = learned && a_net > alpha_max;   // the cap's constant: no gradient to the logit
-  const float a = mix ? (learned ? fminf(a_net, alpha_max) : alpha_fixed) : 1.f;
+  const float a = mix ? (learned ? selection(raw) : alpha_fixed) : 1.f;
   const float pm = fmaxf(mix ? a * q + (1.f - a) * pb : q, 1e-30f);
   const float loss = cb > 0.f ? -cb * logf(pm) : 0.f;
   const float cq = cb * (a * q / pm);   // d(-log pm) = (a q / pm) d(-log q) for q's parameters
 #pragma unroll
   for (int i = 40; i < kOut; ++i) g[i] = 0.f;
-  if (learned && !capped) {
+  if (learned) {
     const float sg = (a - kAMin) / (kAMax - kAMin);
     g[kSelect] = cb * (-(q - pb) / pm) * (kAMax - kAMin) * sg * (1.f - sg);
   }
@@ -249,7 +246,7 @@ __global__ void __launch_bounds__(128, 1) guide_train_kernel(TrainArgs A) {
     for (int i = 0; i < kOut; ++i) raw[i] += sBias[3 * kHid + i];
     const float cb = (valid && csum > 0.f) ? c / csum : 0.f;
     float g[kOut];
-    loss_part = output_gradient(raw, om, cb, pb, A.alpha_fixed, A.alpha_max, g);
+    loss_part = output_gradient(raw, om, cb, pb, A.alpha_fixed, g);
     for (int i = 0; i < kOut; ++i) sDf[threadIdx.x * kHid + i] = g[i];
     for (int k0 = 0; k0 < kOut; k0 += 8) store8_bf16(sD, threadIdx.x, k0, kOut, g + k0);
   }
@@ -447,7 +444,7 @@ void guide_finalize_records(Guide* g, cudaStream_t s, const float4* L, int grid,
 }
 
 int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_count, int cap, int steps,
-                int batch, float lr, uint64_t seed, float alpha_fixed, int64_t total_steps, float alpha_max) {
+                int batch, float lr, uint64_t seed, float alpha_fixed, int64_t total_steps) {
   steps = std::min(steps, g->max_steps);
   batch = std::max(kTile, (batch + kTile - 1) / kTile * kTile);
   const int tiles = batch / kTile;
@@ -457,7 +454,7 @@ int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_
   for (int k = 0; k < steps; ++k) {
     const uint64_t t = (uint64_t)g->t;
     weight_sum_kernel<<<tiles, kTile, 0, s>>>(recs, rec_count, cap, batch, seed, t, g->csum + k);
-    TrainArgs a{recs, rec_count, cap, batch, seed, t, alpha_fixed, alpha_max, g->csum + k, g->wf, g->wb, g->master, g->grad,
+    TrainArgs a{recs, rec_count, cap, batch, seed, t, alpha_fixed, g->csum + k, g->wf, g->wb, g->master, g->grad,
                 g->loss + k, g->err};
     guide_train_kernel<<<tiles, kTile, kTrainSmem, s>>>(a);
     g->t += 1;
@@ -481,7 +478,7 @@ int guide_gradient(Guide* g, cudaStream_t s, const float* recs, const int32_t* c
   weight_sum_kernel<<<batch / kTile, kTile, 0, s>>>(recs, count, n, batch, 0, 0, g->csum);
   cudaMemsetAsync(grad_dev, 0, kParams * 4, s);
   cudaMemsetAsync(loss_dev, 0, 4, s);
-  TrainArgs a{recs, count, n, batch, 0, 0, -1.f, kAMax, g->csum, g->wf, g->wb, g->master, grad_dev, loss_dev, g->err};
+  TrainArgs a{recs, count, n, batch, 0, 0, -1.f, g->csum, g->wf, g->wb, g->master, grad_dev, loss_dev, g->err};
   guide_train_kernel<<<batch / kTile, kTile, kTrainSmem, s>>>(a);
   return cudaGetLastError() == cudaSuccess ? XB_OK : XB_E_CUDA;
 }

@@ -40,13 +40,11 @@ void guide_infer(Guide* g, cudaStream_t s, const float* feats, int feat_stride, 
 // `steps` Adam steps on records [0, min(*rec_count, cap)): each step takes batch / 128 tiles of 128
 // consecutive records at random starts (the whole set, in order, when there are no more records
 // than the batch).
-// alpha_max caps the network's own selection probability (the renderer samples with the capped one).
 // alpha_fixed: the selection probability the renderer samples with (< 0: the network's own output,
 // which is then trained too). total_steps > 0: the learning rate follows a cosine from lr down
 // to lr / 10 over that many Adam steps (counted from the network's first step); 0: constant lr.
 int guide_train(Guide* g, cudaStream_t s, const float* recs, const int32_t* rec_count, int cap, int steps,
-                int batch, float lr, uint64_t seed, float alpha_fixed, int64_t total_steps,
-                float alpha_max = kAMax);
+                int batch, float lr, uint64_t seed, float alpha_fixed, int64_t total_steps);
 // Loss and gradient (no update) over records [0, min(*count, n)) into grad_dev[kParams], loss_dev[1].
 int guide_gradient(Guide* g, cudaStream_t s, const float* recs, const int32_t* count, int n, float* grad_dev,
                    float* loss_dev);

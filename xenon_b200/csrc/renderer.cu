@@ -571,7 +571,6 @@ struct GuideShadeArgs {
   const __nv_bfloat16* wf;   // forward weights (bf16)
   const float* master;       // FP32 parameters (biases)
   float alpha;               // probability of sampling the network (< 0: learned per vertex)
-  float alpha_max;           // cap on the learned probability
   float bmin[3], binv[3];    // position -> [0,1]^3
   const float* ratio_in;     // importance ratio of each incoming path (nullptr: 1)
   float* ratio_out;
@@ -711,7 +710,7 @@ __global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(Shad
       if (!m.ok) break;   // uniform: every thread saw the same failed wait
       // every thread is past the last layer's completion: the activation tile is free
       xbg::raw_to_lobes<true>(raw, lob);
-      alpha = g.alpha >= 0.f ? g.alpha : fminf(xbg::selection<true>(raw), g.alpha_max);
+      alpha = g.alpha >= 0.f ? g.alpha : xbg::selection<true>(raw);
     }
     // ── phase 2: NEE, roulette, the next direction (cpu_tiled.cpp:89-216) ──
     if (alive) do {
@@ -945,7 +944,7 @@ __global__ void __launch_bounds__(128, 4) guide_sample_kernel(ShadeArgs a, Guide
       xbg::forward_tile(m, sA, sW, sBias, raw);
       if (!m.ok) break;   // uniform: every thread saw the same failed wait
       xbg::raw_to_lobes<true>(raw, lob);
-      alpha = g.alpha >= 0.f ? g.alpha : fminf(xbg::selection<true>(raw), g.alpha_max);
+      alpha = g.alpha >= 0.f ? g.alpha : xbg::selection<true>(raw);
     }
     bool emit_next = false, emit_rec = false;
     float4 n_o, n_d, n_tp;
@@ -1707,7 +1706,6 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
       ga.wf = xbg::guide_weights_bf16(gd);
       ga.master = xbg::guide_master(gd);
       ga.alpha = r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f;
-      ga.alpha_max = r->gcfg.max_fraction;
       ga.ratio_in = d > 0 ? w.ratio[q] : nullptr;
       ga.ratio_out = w.ratio[nq];
       for (int k = 0; k < 3; ++k) { ga.bmin[k] = r->gbmin[k]; ga.binv[k] = r->gbinv[k]; }
@@ -1933,7 +1931,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
         if (xbg::guide_train(gd, L.s, xbg::guide_records(gd), xbg::guide_record_count(gd),
                              xbg::guide_record_capacity(gd), steps, r->gcfg.batch, r->gcfg.learning_rate,
                              r->gcfg.seed, r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f,
-                             (int64_t)r->gcfg.train_spp * r->gcfg.steps_per_spp, r->gcfg.max_fraction) != XB_OK)
+                             (int64_t)r->gcfg.train_spp * r->gcfg.steps_per_spp) != XB_OK)
           return set_err(r, XB_E_CUDA, "guide training launch failed");
         r->last_loss_index = steps - 1;
       }
@@ -2788,12 +2786,10 @@ int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
   if (c.max_records == 0) c.max_records = 1 << 21;
   if (c.seed == 0) c.seed = 1;
   if (c.guided_bounces == 0) c.guided_bounces = kMaxDepth;
-  if (c.max_fraction == 0.f) c.max_fraction = xbg::kAMax;
   if (c.train_spp < -1 || c.steps_per_spp < 0 || c.steps_per_spp > xbg::kMaxTrainSteps || c.batch < 0 ||
       c.batch % 128 != 0 || c.batch > (1 << 20) || !(c.learning_rate > 0.f) || !(c.guide_fraction > 0.f) ||
       c.guide_fraction > 1.f || c.max_records < 128 || c.max_records > (1 << 24) || c.record_stride < 0 || c.guided_bounces < 0 ||
-      (c.fixed_fraction != 0 && c.fixed_fraction != 1) || c.keep_training_samples < 0 || c.keep_training_samples > 2 ||
-      !(c.max_fraction >= xbg::kAMin && c.max_fraction <= xbg::kAMax))
+      (c.fixed_fraction != 0 && c.fixed_fraction != 1) || c.keep_training_samples < 0 || c.keep_training_samples > 2)
     return set_err(r, XB_E_INVALID, "xb_set_guiding: bad configuration");
   if (!c.enabled) {
     r->guiding = false;
