@@ -303,7 +303,16 @@ __device__ __forceinline__ bool cosine_sample(V3 wo, V3 color, const DevMaterial
 }
 
 // ── combined eval / pdf for NEE (bsdf.h:601-657) ───────────────────────────────
-__device__ __forceinline__ V3 bsdf_eval(V3 wo, V3 wi, const DevMaterial& m) {
+// The three entry points the bounce kernels call: inlined (the default build) or, built with
+// XB_BSDF_CALLS, kept as calls so that a bounce kernel holds one copy of each body (its two NEE
+// sites evaluate the BSDF) — less code for the instruction cache, more register traffic at the calls.
+#ifdef XB_BSDF_CALLS
+#define XB_BSDF_ENTRY __device__ __noinline__
+#else
+#define XB_BSDF_ENTRY __device__ __forceinline__
+#endif
+
+XB_BSDF_ENTRY V3 bsdf_eval(V3 wo, V3 wi, const DevMaterial& m) {
   if (m.flags & kMatDelta) return v3s(0.f);
   if (m.flags & kMatConductor) return mfr_eval(wo, wi, m);
   if (m.flags & kMatTransmissive) return (wi.z > 0.f) ? mfr_eval(wo, wi, m) : mft_eval(wo, wi, m);
@@ -317,7 +326,7 @@ __device__ __forceinline__ V3 bsdf_eval(V3 wo, V3 wi, const DevMaterial& m) {
   return v3s(0.f);
 }
 
-__device__ __forceinline__ float bsdf_pdf(V3 wo, V3 wi, const DevMaterial& m) {
+XB_BSDF_ENTRY float bsdf_pdf(V3 wo, V3 wi, const DevMaterial& m) {
   if (m.flags & kMatDelta) return 0.f;
   if (m.flags & kMatConductor) return mfr_pdf(wo, wi, m);
   if (m.flags & kMatTransmissive) {
@@ -333,7 +342,7 @@ __device__ __forceinline__ float bsdf_pdf(V3 wo, V3 wi, const DevMaterial& m) {
 }
 
 // ── lobe selection and sampling (bsdf.h:666-708) ───────────────────────────────
-__device__ __forceinline__ bool bsdf_sample(V3 wo, const DevMaterial& m, Pcg& rng, BsdfSample& s) {
+XB_BSDF_ENTRY bool bsdf_sample(V3 wo, const DevMaterial& m, Pcg& rng, BsdfSample& s) {
   s.delta = false;
   s.pdf = 0.f;
   s.f = v3s(0.f);
