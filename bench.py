@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--guide-steps-per-spp", type=int, default=32)
     ap.add_argument("--guide-fraction", type=float, default=0.0,
                     help="fixed probability of sampling the network (0: learned per vertex)")
+    ap.add_argument("--guide-first", type=int, default=0,
+                    help="config 4: first sample index after the first train_spp samples (0: continuous)")
+    ap.add_argument("--guide-ref-cache", default="", help="config 4: load (or save) the FP64 reference here")
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--no-incoherent", action="store_true", help="skip the incoherent-ray traversal bench")
     ap.add_argument("--no-sky-study", action="store_true", help="skip the sky importance sampling study")
@@ -336,19 +339,25 @@ def guiding_study(args, device: int) -> dict:
         return r
 
     t0 = time.perf_counter()
-    rr = renderer(fp64=True)
-    ref_ms = 0.0
-    done = 0
     ref_first = 1 << 24            # sample indices disjoint from the compared renders (1, 2, ...)
-    while done < args.guide_ref_spp:
-        n = min(256, args.guide_ref_spp - done)
-        rr.render_range(cam, ref_first + done, n)
-        ref_ms += rr.stats().last_ms
-        done += n
-    s64, m2 = rr.resolve_fp64()
-    ref = s64 / done
-    ref_var = m2 / max(done - 1, 1)
-    rr.close()
+    if args.guide_ref_cache and os.path.exists(args.guide_ref_cache):
+        z = np.load(args.guide_ref_cache)
+        ref, ref_var, done, ref_ms = z["ref"], z["var"], int(z["spp"]), float(z["ms"])
+    else:
+        rr = renderer(fp64=True)
+        ref_ms = 0.0
+        done = 0
+        while done < args.guide_ref_spp:
+            n = min(256, args.guide_ref_spp - done)
+            rr.render_range(cam, ref_first + done, n)
+            ref_ms += rr.stats().last_ms
+            done += n
+        s64, m2 = rr.resolve_fp64()
+        ref = s64 / done
+        ref_var = m2 / max(done - 1, 1)
+        rr.close()
+        if args.guide_ref_cache:
+            np.savez(args.guide_ref_cache, ref=ref, var=ref_var, spp=done, ms=ref_ms)
     denom = ref ** 2 + eps
     ref_err = float(np.mean(ref_var / done / denom))   # the reference's own expected relMSE
 
@@ -361,8 +370,14 @@ def guiding_study(args, device: int) -> dict:
                           batch=16384, guide_fraction=args.guide_fraction if fixed else 0.7,
                           fixed_fraction=1 if fixed else 0, keep_training_samples=2)
         ms, rendered, chunk = 0.0, 0, 8
+        ntrain = args.guide_train_spp
         while ms < args.guide_seconds * 1e3:
-            r.render_frame(cam, chunk)
+            # samples 1..train_spp (the guided render's training samples), then samples from
+            # --guide-first on (default: train_spp + 1, one continuous sequence)
+            if args.guide_first and rendered >= ntrain:
+                r.render_range(cam, args.guide_first + rendered - ntrain, chunk)
+            else:
+                r.render_range(cam, 1 + rendered, chunk)
             ms += r.stats().last_ms
             rendered += chunk
             if guided and rendered == args.guide_train_spp:

@@ -16,7 +16,11 @@ constexpr int kIn = 64, kHid = 64, kOut = 48, kLobes = 8;
 constexpr int kLobeFloats = 40;  // 8 x (mu xyz, kappa, weight)
 constexpr int kSelect = 40;      // raw output holding the selection logit
 constexpr int kOutRow = 41;      // forward output per row: the lobes, then the selection probability
-constexpr float kAMin = 0.05f, kAMax = 0.95f;   // range of the learned selection probability
+// Range of the learned selection probability; a vertex's importance ratio stays below 1 / (1 - kAMax).
+#ifndef XB_GUIDE_AMAX
+#define XB_GUIDE_AMAX 0.95f
+#endif
+constexpr float kAMin = 0.05f, kAMax = XB_GUIDE_AMAX;
 // Training record (floats): 0-8 features (position in [0,1]^3, normal, outgoing direction),
 // 9-11 sampled direction omega, 12 weight c (set once the path has finished), 13 path index
 // (int bits), 14-16 throughput before the vertex, 17-19 path radiance before the continuation,
