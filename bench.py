@@ -85,6 +85,9 @@ def parse():
                     help="fixed probability of sampling the network (0: learned per vertex)")
     ap.add_argument("--guide-first", type=int, default=0,
                     help="config 4: first sample index after the first train_spp samples (0: continuous)")
+    ap.add_argument("--guide-blocks", default="0,1048576,2097152",
+                    help="config 4: renders per method, each from its own block of sample indices "
+                         "(--guide-first values, comma-separated; empty: --guide-first alone)")
     ap.add_argument("--guide-ref-cache", default="", help="config 4: load (or save) the FP64 reference here")
     ap.add_argument("--guide-width", type=int, default=1280)
     ap.add_argument("--no-incoherent", action="store_true", help="skip the incoherent-ray traversal bench")
@@ -312,10 +315,12 @@ def reference_line(args) -> dict:
 
 def guiding_study(args, device: int) -> dict:
     """Config 4: equal device-time relMSE of the guided and the plain wavefront against a plain
-    FP64 reference. Both methods render in chunks of samples until their summed device time
-    (CUDA events of each xb_render call) reaches the budget; the guided budget includes its
-    online training on the first train_spp samples, of which the second half (rendered once
-    half of the Adam steps are taken) is part of its image."""
+    FP64 reference of 16k samples. Both methods render in chunks of samples until their summed
+    device time (CUDA events of each xb_render call) reaches the budget; the guided budget
+    includes its online training on the first train_spp samples, of which the second half
+    (rendered once half of the Adam steps are taken) is part of its image. Each method renders
+    --guide-blocks times, the samples after training drawn from disjoint blocks of sample
+    indices; the ratios are of the relMSE pooled over those renders (and per render)."""
     import xenon_b200 as xb
     from xenon_b200 import scenes
     W, H = args.guide_width, args.guide_height
@@ -361,7 +366,7 @@ def guiding_study(args, device: int) -> dict:
     denom = ref ** 2 + eps
     ref_err = float(np.mean(ref_var / done / denom))   # the reference's own expected relMSE
 
-    def equal_time(guided: bool) -> dict:
+    def equal_time(guided: bool, first: int) -> dict:
         r = renderer(guided=guided)
         info = {}
         if guided:
@@ -374,8 +379,8 @@ def guiding_study(args, device: int) -> dict:
         while ms < args.guide_seconds * 1e3:
             # samples 1..train_spp (the guided render's training samples), then samples from
             # --guide-first on (default: train_spp + 1, one continuous sequence)
-            if args.guide_first and rendered >= ntrain:
-                r.render_range(cam, args.guide_first + rendered - ntrain, chunk)
+            if first and rendered >= ntrain:
+                r.render_range(cam, first + rendered - ntrain, chunk)
             else:
                 r.render_range(cam, 1 + rendered, chunk)
             ms += r.stats().last_ms
@@ -401,19 +406,36 @@ def guiding_study(args, device: int) -> dict:
                 "relmse_minus_reference_noise": float(pix.mean()) - ref_err,
                 "relmse_trimmed_0.1pct": float(trimmed.mean()), "image_mean": float(img.mean()), **info}
 
-    plain = equal_time(False)
-    guided = equal_time(True)
+    # Several independent renders per method (disjoint blocks of sample indices after the
+    # training samples): the room's caustics make single renders' relMSE a lottery of a few
+    # bright samples, so the ratios are reported per block and pooled over the blocks.
+    blocks = [int(b) for b in args.guide_blocks.split(",")] if args.guide_blocks else [args.guide_first]
+    per_block = []
+    for first in blocks:
+        plain = equal_time(False, first)
+        guided = equal_time(True, first)
+        per_block.append({"first": first, "plain": plain, "guided": guided,
+                          "ratio_raw": plain["relmse"] / max(guided["relmse"], 1e-30),
+                          "ratio_trimmed": plain["relmse_trimmed_0.1pct"] / max(guided["relmse_trimmed_0.1pct"], 1e-30)})
+
+    def pooled(key, method):
+        return float(np.mean([b[method][key] for b in per_block]))
+    pool = {k: {m: pooled(k, m) for m in ("plain", "guided")}
+            for k in ("relmse", "relmse_minus_reference_noise", "relmse_trimmed_0.1pct")}
     return {"workload": "config4: closed room, light above a baffle, smooth glass geodesic sphere "
                         f"({desc.meshes[-1].indices.shape[0]:,} tris), {W}x{H}, depth 16",
             "tuning": {"plain": tuned or "defaults", "guided": tuned_g or "defaults"},
             "budget_device_s": args.guide_seconds, "reference": {"spp": done, "device_ms": ref_ms,
                                                                "image_mean": float(ref.mean()),
                                                                "expected_relmse": ref_err},
-            "plain": plain, "guided": guided,
-            "relmse_ratio_plain_over_guided": plain["relmse"] / max(guided["relmse"], 1e-30),
-            "relmse_ratio_reference_noise_removed": plain["relmse_minus_reference_noise"] /
-                max(guided["relmse_minus_reference_noise"], 1e-30),
-            "relmse_ratio_trimmed": plain["relmse_trimmed_0.1pct"] / max(guided["relmse_trimmed_0.1pct"], 1e-30),
+            "blocks": per_block,
+            # the first block's renders (samples 1, 2, ...: the continuous sequence) as before
+            "plain": per_block[0]["plain"], "guided": per_block[0]["guided"],
+            "pooled": pool,
+            "relmse_ratio_plain_over_guided": pool["relmse"]["plain"] / max(pool["relmse"]["guided"], 1e-30),
+            "relmse_ratio_reference_noise_removed": pool["relmse_minus_reference_noise"]["plain"] /
+                max(pool["relmse_minus_reference_noise"]["guided"], 1e-30),
+            "relmse_ratio_trimmed": pool["relmse_trimmed_0.1pct"]["plain"] / max(pool["relmse_trimmed_0.1pct"]["guided"], 1e-30),
             "wall_s": time.perf_counter() - t0}
 
 
@@ -686,14 +708,20 @@ def guiding_summary(g):
     if not g or "error" in g:
         return g
     p, q = g["plain"], g["guided"]
-    return {"workload": g["workload"], "budget_device_s": g["budget_device_s"], "reference_spp": g["reference"]["spp"],
-            "ratio_raw": _sig(g["relmse_ratio_plain_over_guided"]),
-            "ratio_reference_noise_removed": _sig(g["relmse_ratio_reference_noise_removed"]),
-            "ratio_trimmed": _sig(g["relmse_ratio_trimmed"]),
-            "relmse_plain": _sig(p["relmse"]), "relmse_guided": _sig(q["relmse"]),
-            "spp_plain": p["spp"], "spp_guided": q["spp"], "train_ms": _sig(q.get("train_phase_ms", 0.0)),
-            "mean_plain": _sig(p["image_mean"], 6), "mean_guided": _sig(q["image_mean"], 6),
-            "mean_reference": _sig(g["reference"]["image_mean"], 6)}
+    out = {"workload": g["workload"], "budget_device_s": g["budget_device_s"], "reference_spp": g["reference"]["spp"],
+           "ratio_raw": _sig(g["relmse_ratio_plain_over_guided"]),
+           "ratio_reference_noise_removed": _sig(g["relmse_ratio_reference_noise_removed"]),
+           "ratio_trimmed": _sig(g["relmse_ratio_trimmed"])}
+    if "blocks" in g:
+        out["renders_per_method"] = len(g["blocks"])
+        out["ratio_raw_per_render"] = [_sig(b["ratio_raw"], 3) for b in g["blocks"]]
+        out["ratio_trimmed_per_render"] = [_sig(b["ratio_trimmed"], 3) for b in g["blocks"]]
+        out["relmse_plain"] = _sig(g["pooled"]["relmse"]["plain"])
+        out["relmse_guided"] = _sig(g["pooled"]["relmse"]["guided"])
+    out.update({"spp_plain": p["spp"], "spp_guided": q["spp"], "train_ms": _sig(q.get("train_phase_ms", 0.0)),
+                "mean_plain": _sig(p["image_mean"], 6), "mean_guided": _sig(q["image_mean"], 6),
+                "mean_reference": _sig(g["reference"]["image_mean"], 6)})
+    return out
 
 
 def incoherent_study(args, device: int) -> dict:

@@ -545,7 +545,7 @@ typedef struct xb_guiding {
                                    * kept; 2: those after train_spp / 2 (rendered once half of
                                    * the Adam steps are taken) are kept */
   int32_t fixed_fraction;   /* 0: the network also outputs the probability of sampling it at each
-                             * vertex (in [0.05, 0.95], trained with the mixture);
+                             * vertex (in [0.05, 0.6], trained with the mixture);
                              * 1: guide_fraction everywhere */
   int32_t guided_bounces;   /* the network proposes at bounces 0 .. guided_bounces - 1; later
                              * vertices sample their BSDF (the path's importance ratio carries

@@ -33,7 +33,7 @@ N_HID = 64
 N_OUT = 48
 N_LOBES = 8
 KAPPA_MIN, KAPPA_MAX = -4.0, 6.0
-A_MIN, A_MAX = 0.05, 0.95
+A_MIN, A_MAX = 0.05, 0.6   # the network's selection range (xenon_b200/csrc/guide.h kAMin, kAMax)
 SELECT = 40                     # raw output holding the selection logit
 LAYERS = [(N_HID, N_IN), (N_HID, N_HID), (N_HID, N_HID), (N_OUT, N_HID)]  # (out, in)
 
