@@ -708,7 +708,8 @@ def guiding_summary(g):
     if not g or "error" in g:
         return g
     p, q = g["plain"], g["guided"]
-    out = {"workload": g["workload"], "budget_device_s": g["budget_device_s"], "reference_spp": g["reference"]["spp"],
+    out = {"workload": "config4 (" + g["workload"].split("(")[1].split(")")[0] + " sphere)",
+           "budget_device_s": g["budget_device_s"], "reference_spp": g["reference"]["spp"],
            "ratio_raw": _sig(g["relmse_ratio_plain_over_guided"]),
            "ratio_reference_noise_removed": _sig(g["relmse_ratio_reference_noise_removed"]),
            "ratio_trimmed": _sig(g["relmse_ratio_trimmed"])}
