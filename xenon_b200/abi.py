@@ -158,7 +158,7 @@ class Tuning(ctypes.Structure):
                                               "extend_blocks_per_sm", "shadow_blocks_per_sm",
                                               "shade_blocks_per_sm", "wave_paths", "shadow_order", "overlap",
                                               "waves", "lane_stagger", "graph", "guided_form",
-                                              "shade_occupancy", "shared_stack")]
+                                              "shade_occupancy", "shared_stack", "pixel_order")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

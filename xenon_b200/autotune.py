@@ -14,6 +14,7 @@ two passes), and keeps the fastest setting:
   guided_form                    guided bounce as a bounce kernel + network pass, or one fused kernel
   shade_occupancy                blocks per SM the shading kernels are compiled to fit (registers)
   shared_stack                   BLAS stack entries per thread kept in shared memory (1: none, 16)
+  pixel_order                    camera rays in scanline order or in 8x4 pixel tiles per warp
   refill                         idle lanes that trigger a warp refill
   extend/shadow/shade_blocks_per_sm   blocks per SM in the grids (persistent kernels: at most
                                       those resident at once)
@@ -43,6 +44,7 @@ SPACE = {
     "guided_form": [1, 2],
     "shade_occupancy": [4, 8, 12],
     "shared_stack": [1, 16],
+    "pixel_order": [1, 2],
     "refill": [2, 4, 8, 16, 24],
     "extend_blocks_per_sm": [2, 4, 8, 16, 64],
     "shadow_blocks_per_sm": [2, 4, 8, 16, 64],

@@ -246,13 +246,39 @@ struct CamDev {
   V3 eye, ll, hor, ver;
 };
 
+// Pixel of queue slot j (of npix) when slots go to 8x4 pixel tiles: the 32 slots of a warp cover
+// one tile, tiles in row-major order over the part of the image they fill; the pixels of the
+// right and bottom remainders (width or height not a multiple of 8 or 4) follow in scanline
+// order. A bijection on [0, npix).
+__device__ __forceinline__ int64_t tile_pixel(int64_t j, int W, int H) {
+  const int W8 = W & ~7, H4 = H & ~3;
+  const int64_t nfull = (int64_t)W8 * H4;
+  if (j < nfull) {
+    const int64_t t = j >> 5;
+    const int r = (int)(j & 31);
+    const int tpr = W8 >> 3;
+    const int64_t ty = t / tpr, tx = t - ty * tpr;
+    return (ty * 4 + (r >> 3)) * W + tx * 8 + (r & 7);
+  }
+  int64_t q = j - nfull;
+  const int rw = W - W8;
+  if (q < (int64_t)rw * H4) return (q / rw) * W + W8 + q % rw;
+  q -= (int64_t)rw * H4;
+  return (H4 + q / W) * (int64_t)W + q % W;
+}
+
+// Queue slot p holds path p's camera ray (path p: sample p / npix of pixel p % npix), or with
+// tiles, path (p / npix) * npix + tile_pixel(p % npix): the same paths, the same seeds, the same
+// per-pixel sums (accumulation reads the radiance by path), but each warp's rays start in one 8x4
+// tile, so its camera rays and their bounce-0 shadow rays traverse more of the same nodes.
 __global__ void raygen_kernel(CamDev cam, int W, int H, int spp_first, int64_t paths,
                               float4* ray_o, float4* ray_d, float4* tp, uint64_t* rng,
-                              int32_t* path, float4* L, int32_t* cnt) {
+                              int32_t* path, float4* L, int32_t* cnt, int tiles) {
   const int64_t npix = (int64_t)W * H;
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < paths;
        p += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t pixel = p % npix;
+    const int64_t pixel = tiles ? tile_pixel(p % npix, W, H) : p % npix;
+    const int64_t pid = p - p % npix + pixel;
     const int64_t s = spp_first + p / npix;
     const int x = (int)(pixel % W), y = (int)(pixel / W);
     Pcg g{pcg_seed_state((uint64_t)pixel + (uint64_t)s * 0xdeadbeefULL)};
@@ -264,8 +290,8 @@ __global__ void raygen_kernel(CamDev cam, int W, int H, int spp_first, int64_t p
     ray_d[p] = make_float4(d.x, d.y, d.z, kInf);
     tp[p] = make_float4(1.f, 1.f, 1.f, -1.f);
     rng[p] = g.state;
-    path[p] = (int32_t)p;
-    L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    path[p] = (int32_t)pid;
+    L[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt[CNT_RAYS] = (int32_t)paths;
 }
@@ -1495,6 +1521,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.guided_form = std::min(2, pick(t.guided_form, c.guided_form, 1));
   c.shade_occupancy = pick(t.shade_occupancy, c.shade_occupancy, 8);
   if (c.shade_occupancy != 4 && c.shade_occupancy != 8 && c.shade_occupancy != 12) c.shade_occupancy = 8;
+  c.pixel_order = std::min(2, pick(t.pixel_order, c.pixel_order, 1));
   c.shared_stack = pick(t.shared_stack, c.shared_stack, 1);
   if (c.shared_stack != 1 && c.shared_stack != kSharedStack) c.shared_stack = 1;
   r->stack_sh = c.shared_stack > 1 ? c.shared_stack : 0;
@@ -1912,7 +1939,7 @@ int run_waves(xb_renderer* r, const xb_camera* cam, int spp_first, int spp_count
       {
         StageTimer t(r, STAGE_RAYGEN, L.s);
         raygen_kernel<<<g_rg, 256, 0, L.s>>>(cd, W, H, sample0, paths, w.ray_o[0], w.ray_d[0], w.tp[0],
-                                             w.rng[0], w.path[0], w.L, w.cnt);
+                                             w.rng[0], w.path[0], w.L, w.cnt, r->tune.pixel_order == 2);
       }
       int rc = run_bounces(r, L, k, train, rec_stride, depth_max, nullptr);
       if (rc) return rc;
