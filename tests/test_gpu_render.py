@@ -89,7 +89,7 @@ def test_traversal_variants_render_identically(builder):
                         (0, {"extend_persistent_from_depth": 1, "shadow_order": 2, "refill": 4}),
                         (0, {"shared_stack": 16}),
                         (0, {"shared_stack": 16, "extend_persistent_from_depth": 1, "shadow_persistent": 2}),
-                        (0, {"pixel_order": 2}), (0, {"pixel_order": 2, "waves": 3})):
+                        (0, {"pixel_order": 1}), (0, {"pixel_order": 1, "waves": 3})):
         r = Renderer(64, 48, desc.max_bounces, desc.min_bounces, flags=flags)
         r.upload_scene(HostScene.from_desc(desc))
         if tune:

@@ -1062,7 +1062,7 @@ struct ViewPieces {
 };
 
 __global__ void raygen_views_kernel(ViewPieces pk, int64_t paths, float4* ray_o, float4* ray_d, float4* tp,
-                                    uint64_t* rng, int32_t* path, float4* L, int8_t* maxd, int32_t* cnt) {
+                                    uint64_t* rng, int32_t* path, float4* L, int8_t* maxd, int32_t* cnt, int tiles) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < paths;
        p += (int64_t)gridDim.x * blockDim.x) {
     int i = 0;
@@ -1070,7 +1070,9 @@ __global__ void raygen_views_kernel(ViewPieces pk, int64_t paths, float4* ray_o,
     const ViewPiece& v = pk.p[i];
     const int64_t npix = (int64_t)v.W * v.H;
     const int64_t local = p - v.path_off;
-    const int64_t pixel = local % npix;
+    // a piece holds whole samples of its view: slots map to pixels as in raygen_kernel
+    const int64_t pixel = tiles ? tile_pixel(local % npix, v.W, v.H) : local % npix;
+    const int64_t pid = p - local % npix + pixel;
     const int64_t s = v.s_first + local / npix;
     const int x = (int)(pixel % v.W), y = (int)(pixel / v.W);
     // cpu_tiled.cpp:20-32, as raygen_kernel
@@ -1083,9 +1085,9 @@ __global__ void raygen_views_kernel(ViewPieces pk, int64_t paths, float4* ray_o,
     ray_d[p] = make_float4(d.x, d.y, d.z, kInf);
     tp[p] = make_float4(1.f, 1.f, 1.f, -1.f);
     rng[p] = g.state;
-    path[p] = (int32_t)p;
-    L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-    maxd[p] = (int8_t)v.max_bounces;
+    path[p] = (int32_t)pid;
+    L[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+    maxd[pid] = (int8_t)v.max_bounces;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt[CNT_RAYS] = (int32_t)paths;
 }
@@ -1521,7 +1523,7 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.guided_form = std::min(2, pick(t.guided_form, c.guided_form, 1));
   c.shade_occupancy = pick(t.shade_occupancy, c.shade_occupancy, 8);
   if (c.shade_occupancy != 4 && c.shade_occupancy != 8 && c.shade_occupancy != 12) c.shade_occupancy = 8;
-  c.pixel_order = std::min(2, pick(t.pixel_order, c.pixel_order, 1));
+  c.pixel_order = std::min(2, pick(t.pixel_order, c.pixel_order, 2));
   c.shared_stack = pick(t.shared_stack, c.shared_stack, 1);
   if (c.shared_stack != 1 && c.shared_stack != kSharedStack) c.shared_stack = 1;
   r->stack_sh = c.shared_stack > 1 ? c.shared_stack : 0;
@@ -2021,7 +2023,7 @@ int run_view_waves(xb_renderer* r, const xb_view* views, int count, float4* accu
     {
       StageTimer t(r, STAGE_RAYGEN, L.s);
       raygen_views_kernel<<<g_rg, 256, 0, L.s>>>(pk, paths, w.ray_o[0], w.ray_d[0], w.tp[0], w.rng[0],
-                                                 w.path[0], w.L, w.maxd, w.cnt);
+                                                 w.path[0], w.L, w.maxd, w.cnt, r->tune.pixel_order == 2);
     }
     int rc = run_bounces(r, L, k, false, 1, wave_depth, w.maxd);
     if (rc) return rc;
