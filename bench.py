@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--guide-steps-per-spp", type=int, default=32)
     ap.add_argument("--guide-fraction", type=float, default=0.0,
                     help="fixed probability of sampling the network (0: learned per vertex)")
+    ap.add_argument("--guide-ratio-cap", type=float, default=0.0,
+                    help="bound on a path's importance ratio (xb_guiding.ratio_cap; 0: the library's default)")
     ap.add_argument("--guide-first", type=int, default=0,
                     help="config 4: first sample index after the first train_spp samples (0: continuous)")
     ap.add_argument("--guide-blocks", default="0,1048576,2097152",
@@ -373,7 +375,8 @@ def guiding_study(args, device: int) -> dict:
             fixed = args.guide_fraction > 0
             r.set_guiding(True, train_spp=args.guide_train_spp, steps_per_spp=args.guide_steps_per_spp,
                           batch=16384, guide_fraction=args.guide_fraction if fixed else 0.7,
-                          fixed_fraction=1 if fixed else 0, keep_training_samples=2)
+                          fixed_fraction=1 if fixed else 0, keep_training_samples=2,
+                          ratio_cap=args.guide_ratio_cap)
         ms, rendered, chunk = 0.0, 0, 8
         ntrain = args.guide_train_spp
         while ms < args.guide_seconds * 1e3:
@@ -393,7 +396,7 @@ def guiding_study(args, device: int) -> dict:
             info.update(r.guiding_stats())
             info["config"] = {k: v for k, v in r.guiding().items() if k in
                               ("train_spp", "steps_per_spp", "batch", "learning_rate", "guide_fraction",
-                               "fixed_fraction", "keep_training_samples")}
+                               "fixed_fraction", "keep_training_samples", "ratio_cap")}
         r.close()
         e = (img - ref) ** 2 / denom
         pix = e.mean(2).ravel()

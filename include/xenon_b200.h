@@ -553,6 +553,13 @@ typedef struct xb_guiding {
   int32_t guided_bounces;   /* the network proposes at bounces 0 .. guided_bounces - 1; later
                              * vertices sample their BSDF (the path's importance ratio carries
                              * on); default: every bounce */
+  float ratio_cap;          /* bound on a path's importance ratio prod p_bsdf / p: at a guided
+                             * vertex the probability of sampling the network is lowered to
+                             * 1 - ratio / ratio_cap (0 once the ratio reaches the cap), so a
+                             * path whose guided vertices missed its light cannot carry more than
+                             * ratio_cap times the plain estimator's weight; the estimator stays
+                             * unbiased. 0: default 2.5; < 0: no bound beyond each vertex's
+                             * 1 / (1 - a) */
 } xb_guiding;
 
 /* Enables, disables or reconfigures guiding (0 fields take defaults). The first enabling, or a

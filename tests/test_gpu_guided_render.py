@@ -67,6 +67,10 @@ def test_guided_converges_to_the_plain_image(sphere, bounces):
     kws = [dict(train_spp=-1), dict(train_spp=64, steps_per_spp=8, batch=4096)]
     if bounces > 2:   # the network at the first bounce only; later vertices carry its ratio
         kws.append(dict(train_spp=64, steps_per_spp=8, batch=4096, guided_bounces=1))
+        # no bound on the path's importance ratio (each vertex still within 1 / (1 - a)), and
+        # a tight one under which most vertices past the first sample their BSDF alone
+        kws.append(dict(train_spp=64, steps_per_spp=8, batch=4096, ratio_cap=-1.0))
+        kws.append(dict(train_spp=64, steps_per_spp=8, batch=4096, ratio_cap=1.25))
     for kw in kws:
         mg, vg, stg, gst = _render(sc, cam, spp, True, bounces, **kw)
         # non-finite samples are dropped from the image and counted; they must stay rare
@@ -175,6 +179,13 @@ def test_keep_training_samples_modes():
     r.upload_scene(sc)
     with pytest.raises(xb.XenonError):
         r.set_guiding(True, keep_training_samples=3)
+    # a bound below 1 would hold no path; 0 selects the default, < 0 no bound
+    with pytest.raises(xb.XenonError):
+        r.set_guiding(True, ratio_cap=0.5)
+    r.set_guiding(True)
+    assert r.guiding()["ratio_cap"] == 2.5
+    r.set_guiding(True, ratio_cap=-1.0)
+    assert r.guiding()["ratio_cap"] == -1.0
     r.close()
 
 

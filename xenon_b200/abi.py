@@ -191,7 +191,7 @@ class Guiding(ctypes.Structure):
                 ("max_records", ctypes.c_int32), ("record_stride", ctypes.c_int32), ("seed", ctypes.c_uint64),
                 ("bounds_min", ctypes.c_float * 3), ("bounds_max", ctypes.c_float * 3),
                 ("keep_training_samples", ctypes.c_int32), ("fixed_fraction", ctypes.c_int32),
-                ("guided_bounces", ctypes.c_int32)]
+                ("guided_bounces", ctypes.c_int32), ("ratio_cap", ctypes.c_float)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_}

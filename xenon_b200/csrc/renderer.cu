@@ -609,7 +609,16 @@ struct GuideShadeArgs {
   float4* gq[5];             // two-kernel form: the deferred vertices (nullptr: fused form)
   uint64_t* gq_rng;
   float sky_alpha;           // network-free form with XB_FLAG_SKY_IS: probability of the sky proposal
+  float ratio_cap;           // bound on the path's importance ratio (<= 0: none)
 };
+
+// The probability of sampling the proposal at a vertex whose path carries `ratio`: at most
+// 1 - ratio / cap, so that the worst case of the vertex's factor p_bsdf / p = 1 / (1 - a) keeps
+// the path's ratio within the cap. It depends on the path's prefix only, so the estimator stays
+// unbiased; a path at or above the cap samples its BSDF alone.
+__device__ __forceinline__ float capped_selection(float a, float ratio, float cap) {
+  return cap > 0.f ? fminf(a, fmaxf(0.f, 1.f - ratio / cap)) : a;
+}
 
 constexpr float kNaN = __builtin_nanf("");
 constexpr int kLobStride = xbg::kLobeFloats + 1;   // conflict-free per-thread rows
@@ -841,7 +850,7 @@ __global__ void __launch_bounds__(128, kNet ? 4 : kOcc) guided_shade_kernel(Shad
       } else {
         // the proposal: the network's mixture (kNet) or the sky's luminance distribution
         float pb;
-        const float ap = kNet ? alpha : g.sky_alpha;
+        const float ap = capped_selection(kNet ? alpha : g.sky_alpha, ratio, g.ratio_cap);
         if (rng.next_float() < ap) {
           if constexpr (kNet) {
             const float u0 = rng.next_float(), u1 = rng.next_float(), u2 = rng.next_float();
@@ -988,7 +997,8 @@ __global__ void __launch_bounds__(128, 4) guide_sample_kernel(ShadeArgs a, Guide
       BsdfSample s;
       V3 wiw;
       float pb;
-      if (rng.next_float() < alpha) {
+      const float ap = capped_selection(alpha, ratio, g.ratio_cap);
+      if (rng.next_float() < ap) {
         const float u0 = rng.next_float(), u1 = rng.next_float(), u2 = rng.next_float();
         float d[3];
         xbg::mix_sample(lob, u0, u1, u2, d);
@@ -1001,7 +1011,7 @@ __global__ void __launch_bounds__(128, 4) guide_sample_kernel(ShadeArgs a, Guide
         wiw = onb.to_world(s.wi);
         pb = bsdf_density(wo_l, s.wi, mat);
       }
-      const float pm = alpha * xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) + (1.f - alpha) * pb;
+      const float pm = ap * xbg::mix_pdf(lob, wiw.x, wiw.y, wiw.z) + (1.f - ap) * pb;
       if (!(pm > 0.f)) break;
       n_ratio = ratio * (pb / pm);
       if (training && (pid % g.rec_stride) == 0) {
@@ -1735,6 +1745,7 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
       ga.wf = xbg::guide_weights_bf16(gd);
       ga.master = xbg::guide_master(gd);
       ga.alpha = r->gcfg.fixed_fraction ? r->gcfg.guide_fraction : -1.f;
+      ga.ratio_cap = r->gcfg.ratio_cap;
       ga.ratio_in = d > 0 ? w.ratio[q] : nullptr;
       ga.ratio_out = w.ratio[nq];
       for (int k = 0; k < 3; ++k) { ga.bmin[k] = r->gbmin[k]; ga.binv[k] = r->gbinv[k]; }
@@ -2815,10 +2826,12 @@ int xb_set_guiding(xb_renderer* r, const xb_guiding* g) {
   if (c.max_records == 0) c.max_records = 1 << 21;
   if (c.seed == 0) c.seed = 1;
   if (c.guided_bounces == 0) c.guided_bounces = kMaxDepth;
+  if (c.ratio_cap == 0.f) c.ratio_cap = 2.5f;
   if (c.train_spp < -1 || c.steps_per_spp < 0 || c.steps_per_spp > xbg::kMaxTrainSteps || c.batch < 0 ||
       c.batch % 128 != 0 || c.batch > (1 << 20) || !(c.learning_rate > 0.f) || !(c.guide_fraction > 0.f) ||
       c.guide_fraction > 1.f || c.max_records < 128 || c.max_records > (1 << 24) || c.record_stride < 0 || c.guided_bounces < 0 ||
-      (c.fixed_fraction != 0 && c.fixed_fraction != 1) || c.keep_training_samples < 0 || c.keep_training_samples > 2)
+      (c.fixed_fraction != 0 && c.fixed_fraction != 1) || c.keep_training_samples < 0 || c.keep_training_samples > 2 ||
+      !(c.ratio_cap < 0.f || c.ratio_cap >= 1.f))
     return set_err(r, XB_E_INVALID, "xb_set_guiding: bad configuration");
   if (!c.enabled) {
     r->guiding = false;
