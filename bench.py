@@ -495,9 +495,11 @@ def sky_study(args, device: int) -> dict:
 
 def build_study(args) -> dict:
     """BVH build of config 2's scene (1,310,722 triangles, binned SAH as the reference builds it):
-    wall time of the recursive host build on one thread and on every host thread, and of the
-    level-synchronous build on the device (XB_BUILD_DEVICE); all three give the same node arrays
-    (GPU tests). Median of three builds each, after one untimed device build."""
+    wall time of xb_scene_build (the BLAS, the TLAS and the flattened arrays; the mesh already
+    added) with the recursive host build on one thread and on every host thread, and with the
+    level-synchronous build on the device (XB_BUILD_DEVICE, host-to-device copy of the build items
+    and the read-back of the nodes included); all three give the same node arrays (GPU tests).
+    Median of three builds each, after one untimed device build."""
     import xenon_b200 as xb
     from xenon_b200 import abi, scenes
     desc = scenes.icosphere_scene(level=args.level)
@@ -505,8 +507,9 @@ def build_study(args) -> dict:
     def timed(**kw):
         t = []
         for _ in range(3):
+            s = xb.HostScene.from_desc(desc, build=False)
             t0 = time.perf_counter()
-            xb.HostScene.from_desc(desc, **kw)
+            s.build(**kw)
             t.append(time.perf_counter() - t0)
         return float(np.median(t))
 

@@ -64,10 +64,11 @@ class HostScene:
             pass
 
     @classmethod
-    def from_desc(cls, desc, build_threads: int = 0, build_mode: int = abi.XB_BUILD_RECURSIVE) -> "HostScene":
+    def from_desc(cls, desc, build_threads: int = 0, build_mode: int = abi.XB_BUILD_RECURSIVE,
+                  build: bool = True) -> "HostScene":
         """Builds the scene's BVHs with `build_threads` threads (0: all hardware threads), in the
         recursive or the level-synchronous form (build_mode); the arrays are the same for any
-        count and either form."""
+        count and either form. build=False: the scene is filled but not built (build() does it)."""
         s = cls()
         L = lib()
         for name, m in zip(desc.material_names, desc.materials):
@@ -97,10 +98,16 @@ class HostScene:
         for (geom, t, sc, r, iid) in desc.instances:
             check(L.xb_scene_add_instance(s.h, int(geom), _p(np.asarray(t, np.float32)), float(sc),
                                           _p(np.asarray(r, np.float32)), int(iid)))
-        check(L.xb_scene_set_build_threads(s.h, int(build_threads)))
-        check(L.xb_scene_set_build_mode(s.h, int(build_mode)))
-        check(L.xb_scene_build(s.h))
+        if build:
+            s.build(build_threads, build_mode)
         return s
+
+    def build(self, build_threads: int = 0, build_mode: int = abi.XB_BUILD_RECURSIVE) -> None:
+        """xb_scene_build: the BVHs (BLAS per mesh, PrimBLAS, TLAS) and the flattened arrays."""
+        L = lib()
+        check(L.xb_scene_set_build_threads(self.h, int(build_threads)))
+        check(L.xb_scene_set_build_mode(self.h, int(build_mode)))
+        check(L.xb_scene_build(self.h))
 
     @classmethod
     def load(cls, path: str) -> "HostScene":

@@ -48,9 +48,10 @@ void place_level_nodes(const std::vector<LevelNodeRecord>& all, std::vector<xb_b
 
 void build_bvh_levels(std::vector<BuildItem>& items, int bins, uint32_t max_leaf, bool leaf_cost,
                       std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
-// The same build run by the device (bvh_device.cu) on the current CUDA device: the same
-// arrays. Throws std::runtime_error on a CUDA error, std::invalid_argument on bad arguments.
-void build_bvh_device(std::vector<BuildItem>& items, int bins, uint32_t max_leaf, bool leaf_cost,
+// The same build run by the device (bvh_device.cu) on the current CUDA device: the same node
+// and order arrays; the host items are left in their input order (the reordered items stay on
+// the device). Throws std::runtime_error on a CUDA error, std::invalid_argument on bad arguments.
+void build_bvh_device(const std::vector<BuildItem>& items, int bins, uint32_t max_leaf, bool leaf_cost,
                       std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
 
 }  // namespace xb

@@ -8,7 +8,8 @@
 // host form run the device's pass code. The loop (run_level_build) is the same for both; an
 // executor supplies the memory and runs the passes.
 //
-// One depth:
+// One depth (nodes of more than kLevelChunk items; lvl_small_at splits each smaller node whole,
+// in one thread, with the same steps):
 //   1. lvl_bounds_at:   per chunk, the items' box and centroid bounds;
 //   2. lvl_plane_at:    per node, the chunk bounds folded in chunk order; a leaf, or the axis;
 //   3. lvl_bins_at:     per chunk of a splitting node, its bin counts and boxes;
@@ -74,20 +75,20 @@ XB_HD void level_error(int32_t* error, int32_t code) {
 #endif
 }
 
+// Chunks of a node of `size` items: none for a node that one thread splits whole (lvl_small_at).
+XB_HD uint32_t level_node_chunks(uint32_t size) {
+  return size > kLevelChunk ? (size + kLevelChunk - 1) / kLevelChunk : 0u;
+}
+
 XB_HD void lvl_bounds_at(const LevelArgs& a, uint32_t c) {
   const ChunkRef r = a.chunks[c];
   level_chunk_bounds(a.items, r.b, r.e, a.chunk_box[c], a.chunk_cbox[c]);
 }
 
-XB_HD void lvl_plane_at(const LevelArgs& a, uint32_t x) {
+// A node's box and split plane from its folded chunk bounds (box: the items', cb: their
+// centroids').
+XB_HD void lvl_plane_finish(const LevelArgs& a, uint32_t x, const RefitBox& box, const RefitBox& cb) {
   const LevelTask t = a.tasks[x];
-  RefitBox box, cb;
-  refit_empty(box);
-  refit_empty(cb);
-  for (uint32_t c = t.chunk0; c < t.chunk0 + t.nchunks; ++c) {
-    refit_grow(box, a.chunk_box[c]);
-    refit_grow(cb, a.chunk_cbox[c]);
-  }
   NodeOut o;
   o.box = box;
   o.state = 0;
@@ -98,6 +99,19 @@ XB_HD void lvl_plane_at(const LevelArgs& a, uint32_t x) {
   o.scale = 0.f;
   if (t.hi - t.lo > a.max_leaf && level_plane(cb, a.bins, &o.axis, &o.cmin, &o.scale)) o.state = 1;
   a.out[x] = o;
+}
+
+XB_HD void lvl_plane_at(const LevelArgs& a, uint32_t x) {
+  const LevelTask t = a.tasks[x];
+  if (t.nchunks == 0) return;
+  RefitBox box, cb;
+  refit_empty(box);
+  refit_empty(cb);
+  for (uint32_t c = t.chunk0; c < t.chunk0 + t.nchunks; ++c) {
+    refit_grow(box, a.chunk_box[c]);
+    refit_grow(cb, a.chunk_cbox[c]);
+  }
+  lvl_plane_finish(a, x, box, cb);
 }
 
 XB_HD void lvl_bins_at(const LevelArgs& a, uint32_t c) {
@@ -113,10 +127,19 @@ XB_HD void lvl_bins_at(const LevelArgs& a, uint32_t c) {
   }
 }
 
-XB_HD void lvl_sah_at(const LevelArgs& a, uint32_t x) {
+// A splitting node's SAH sweep over its folded bins: the plane, or a leaf.
+XB_HD void lvl_sah_finish(const LevelArgs& a, uint32_t x, const RefitBox* bin_box, const int* bin_cnt) {
   NodeOut& o = a.out[x];
-  if (o.state != 1) return;
   const LevelTask t = a.tasks[x];
+  float best;
+  const int best_bin = level_sah(bin_box, bin_cnt, a.bins, o.box, &best);
+  if ((a.leaf_cost && best >= (float)(t.hi - t.lo)) || best_bin < 0) o.state = 0;
+  else o.best_bin = best_bin;
+}
+
+XB_HD void lvl_sah_at(const LevelArgs& a, uint32_t x) {
+  const LevelTask t = a.tasks[x];
+  if (t.nchunks == 0 || a.out[x].state != 1) return;
   RefitBox bin_box[kLevelMaxBins];
   int bin_cnt[kLevelMaxBins];
   for (int k = 0; k < a.bins; ++k) { refit_empty(bin_box[k]); bin_cnt[k] = 0; }
@@ -125,10 +148,7 @@ XB_HD void lvl_sah_at(const LevelArgs& a, uint32_t x) {
       bin_cnt[k] += a.chunk_cnt[(size_t)c * a.bins + k];
       refit_grow(bin_box[k], a.chunk_bins[(size_t)c * a.bins + k]);
     }
-  float best;
-  const int best_bin = level_sah(bin_box, bin_cnt, a.bins, o.box, &best);
-  if ((a.leaf_cost && best >= (float)(t.hi - t.lo)) || best_bin < 0) o.state = 0;
-  else o.best_bin = best_bin;
+  lvl_sah_finish(a, x, bin_box, bin_cnt);
 }
 
 XB_HD void lvl_pass_at(const LevelArgs& a, uint32_t c) {
@@ -140,17 +160,23 @@ XB_HD void lvl_pass_at(const LevelArgs& a, uint32_t c) {
   a.chunk_pass[c] = n;
 }
 
-XB_HD void lvl_prefix_at(const LevelArgs& a, uint32_t x) {
+// m items of a splitting node go left; a partition leaving a side empty goes to the median.
+XB_HD void lvl_prefix_finish(const LevelArgs& a, uint32_t x, uint32_t m) {
   NodeOut& o = a.out[x];
-  if (o.state != 1) return;
   const LevelTask t = a.tasks[x];
+  o.m = m;
+  if (m == 0 || m == t.hi - t.lo) o.state = 2;
+}
+
+XB_HD void lvl_prefix_at(const LevelArgs& a, uint32_t x) {
+  const LevelTask t = a.tasks[x];
+  if (t.nchunks == 0 || a.out[x].state != 1) return;
   uint32_t m = 0;
   for (uint32_t c = t.chunk0; c < t.chunk0 + t.nchunks; ++c) {
     a.chunk_before[c] = m;
     m += a.chunk_pass[c];
   }
-  o.m = m;
-  if (m == 0 || m == t.hi - t.lo) o.state = 2;
+  lvl_prefix_finish(a, x, m);
 }
 
 XB_HD void lvl_rank_at(const LevelArgs& a, uint32_t c) {
@@ -170,6 +196,51 @@ XB_HD void lvl_rank_at(const LevelArgs& a, uint32_t c) {
   }
 }
 
+// The bidirectional std::partition of libstdc++ over items [first, last) by level_pass: from the
+// left, stop at an item that fails; from the right, at one that passes; swap; until they meet.
+XB_HD void level_partition(LevelItem* it, uint32_t first, uint32_t last, const NodeOut& o, int bins) {
+  for (;;) {
+    for (;;) {
+      if (first == last) return;
+      if (level_pass(it[first], o.axis, o.cmin, o.scale, bins, o.best_bin)) ++first;
+      else break;
+    }
+    --last;
+    for (;;) {
+      if (first == last) return;
+      if (!level_pass(it[last], o.axis, o.cmin, o.scale, bins, o.best_bin)) --last;
+      else break;
+    }
+    const LevelItem t = it[first];
+    it[first] = it[last];
+    it[last] = t;
+    ++first;
+  }
+}
+
+// A node of at most kLevelChunk items, split whole: its bounds, plane, bins, SAH sweep and
+// partition are the chunked passes' for a node of one chunk (a fold over one chunk is that
+// chunk's own result), and the partition is the one the exchange ranks reproduce.
+XB_HD void lvl_small_at(const LevelArgs& a, uint32_t x) {
+  const LevelTask t = a.tasks[x];
+  if (t.nchunks != 0) return;
+  RefitBox box, cb;
+  level_chunk_bounds(a.items, t.lo, t.hi, box, cb);
+  lvl_plane_finish(a, x, box, cb);
+  NodeOut& o = a.out[x];
+  if (o.state != 1) return;
+  RefitBox bin_box[kLevelMaxBins];
+  int bin_cnt[kLevelMaxBins];
+  level_chunk_bins(a.items, t.lo, t.hi, o.axis, o.cmin, o.scale, a.bins, bin_box, bin_cnt);
+  lvl_sah_finish(a, x, bin_box, bin_cnt);
+  if (o.state != 1) return;
+  uint32_t m = 0;
+  for (uint32_t i = t.lo; i < t.hi; ++i) m += level_pass(a.items[i], o.axis, o.cmin, o.scale, a.bins, o.best_bin);
+  lvl_prefix_finish(a, x, m);
+  if (o.state != 1) return;
+  level_partition(a.items, t.lo, t.hi, o, a.bins);
+}
+
 // Swaps the pair slot s names and clears the slot, so the tables are all -1 again for the next
 // depth (they start so).
 XB_HD void lvl_exchange_at(const LevelArgs& a, uint32_t s) {
@@ -187,7 +258,8 @@ XB_HD void lvl_exchange_at(const LevelArgs& a, uint32_t s) {
 // The level loop over n items (already in the executor's memory). Exec provides
 //   void run_depth(LevelArgs& a, const std::vector<LevelTask>&, const std::vector<ChunkRef>&,
 //                  std::vector<NodeOut>& out, int32_t* error)
-//       sets a's memory, runs the eight passes and reads back every node's outcome and the error;
+//       sets a's memory, runs lvl_small_at and the eight passes and reads back every node's
+//       outcome and the error;
 //   void median_split(uint32_t lo, uint32_t mid, uint32_t hi, int axis)
 //       std::nth_element of items [lo, hi) at mid by centroid[axis].
 template <class Exec>
@@ -205,10 +277,10 @@ void run_level_build(Exec& ex, uint32_t n, int bins, uint32_t max_leaf, bool lea
     chunks.clear();
     for (size_t x = begin; x < end; ++x) {
       const uint32_t lo = all[x].lo, hi = all[x].hi;
-      LevelTask t{lo, hi, (uint32_t)chunks.size(), 0};
-      for (uint32_t c = lo; c < hi; c += kLevelChunk) {
+      LevelTask t{lo, hi, (uint32_t)chunks.size(), level_node_chunks(hi - lo)};
+      for (uint32_t k = 0; k < t.nchunks; ++k) {
+        const uint32_t c = lo + k * kLevelChunk;
         chunks.push_back(ChunkRef{(uint32_t)(x - begin), c, std::min(hi, c + kLevelChunk)});
-        ++t.nchunks;
       }
       tasks.push_back(t);
     }

@@ -69,6 +69,7 @@ struct HostLevelExec {
     a.left_of = left_of.data();
     a.right_of = right_of.data();
     a.error = error;
+    for (uint32_t i = 0; i < a.ntasks; ++i) lvl_small_at(a, i);
     for (uint32_t i = 0; i < a.nchunks; ++i) lvl_bounds_at(a, i);
     for (uint32_t i = 0; i < a.ntasks; ++i) lvl_plane_at(a, i);
     for (uint32_t i = 0; i < a.nchunks; ++i) lvl_bins_at(a, i);
