@@ -101,6 +101,27 @@ def test_traversal_variants_render_identically(builder):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("flags", [0, 1])
+def test_opaque_scene_bounce_renders_like_the_general_one(flags):
+    """A scene without delta, transmissive or subsurface materials shades with the bounce kernel
+    compiled without those lobes; adding an unused glass material selects the general kernel, and
+    the images are equal."""
+    from xenon_b200 import abi
+    imgs = []
+    for extra in (False, True):
+        desc = scenes.icosphere_scene(level=5)
+        if extra:   # listed, never referenced by a triangle
+            desc.add_material("unused_glass", abi.material(base_color=(1.0, 1.0, 1.0), transmission=1.0,
+                                                           roughness=0.0, ior=1.5))
+        r = Renderer(64, 48, desc.max_bounces, desc.min_bounces,
+                     flags=abi.XB_FLAG_THREAD_PER_RAY if flags else 0)
+        r.upload_scene(HostScene.from_desc(desc))
+        r.render_frame(camera(desc.eye, desc.target, desc.fov, 64 / 48), 3)
+        imgs.append(r.resolve())
+    assert np.array_equal(imgs[0], imgs[1])
+
+
+@pytest.mark.gpu
 def test_two_waves_in_flight_render_identically():
     """Consecutive waves on two to four stream lanes accumulate in sample order: the images (FP32
     and FP64 sums, plain and guided, one view and many) equal the one-lane images bit for bit."""

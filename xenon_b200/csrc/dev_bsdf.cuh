@@ -312,11 +312,21 @@ __device__ __forceinline__ bool cosine_sample(V3 wo, V3 color, const DevMaterial
 #define XB_BSDF_ENTRY __device__ __forceinline__
 #endif
 
+// kOpaque: the scene has no delta, transmissive or subsurface material (the renderer checks at
+// upload), so those branches are left out of the bounce kernel's code; the same arithmetic runs
+// for every material it does have.
+template <bool kOpaque>
+__device__ __forceinline__ uint32_t lobe_flags(const DevMaterial& m) {
+  return kOpaque ? (m.flags & kMatConductor) : m.flags;
+}
+
+template <bool kOpaque = false>
 XB_BSDF_ENTRY V3 bsdf_eval(V3 wo, V3 wi, const DevMaterial& m) {
-  if (m.flags & kMatDelta) return v3s(0.f);
-  if (m.flags & kMatConductor) return mfr_eval(wo, wi, m);
-  if (m.flags & kMatTransmissive) return (wi.z > 0.f) ? mfr_eval(wo, wi, m) : mft_eval(wo, wi, m);
-  if (m.flags & kMatSubsurface) {
+  const uint32_t fl = lobe_flags<kOpaque>(m);
+  if (fl & kMatDelta) return v3s(0.f);
+  if (fl & kMatConductor) return mfr_eval(wo, wi, m);
+  if (fl & kMatTransmissive) return (wi.z > 0.f) ? mfr_eval(wo, wi, m) : mft_eval(wo, wi, m);
+  if (fl & kMatSubsurface) {
     if (wi.z <= 0.f) return v3s(0.f);
     return ss_color(m) * (1.f - m.metallic) * kInvPi;
   }
@@ -326,15 +336,17 @@ XB_BSDF_ENTRY V3 bsdf_eval(V3 wo, V3 wi, const DevMaterial& m) {
   return v3s(0.f);
 }
 
+template <bool kOpaque = false>
 XB_BSDF_ENTRY float bsdf_pdf(V3 wo, V3 wi, const DevMaterial& m) {
-  if (m.flags & kMatDelta) return 0.f;
-  if (m.flags & kMatConductor) return mfr_pdf(wo, wi, m);
-  if (m.flags & kMatTransmissive) {
+  const uint32_t fl = lobe_flags<kOpaque>(m);
+  if (fl & kMatDelta) return 0.f;
+  if (fl & kMatConductor) return mfr_pdf(wo, wi, m);
+  if (fl & kMatTransmissive) {
     float f = fresnel_dielectric(fabsf(wo.z), m.ior);
     if (wi.z > 0.f) return f * mfr_pdf(wo, wi, m);
     return (1.f - f) * mft_pdf(wo, wi, m);
   }
-  if (m.flags & kMatSubsurface) return diffuse_pdf(wi);
+  if (fl & kMatSubsurface) return diffuse_pdf(wi);
   float spec = m.f0[0];
   float diff = 1.f - spec;
   if (wi.z > 0.f) return diffuse_pdf(wi) * diff + mfr_pdf(wo, wi, m) * spec;
@@ -342,22 +354,24 @@ XB_BSDF_ENTRY float bsdf_pdf(V3 wo, V3 wi, const DevMaterial& m) {
 }
 
 // ── lobe selection and sampling (bsdf.h:666-708) ───────────────────────────────
+template <bool kOpaque = false>
 XB_BSDF_ENTRY bool bsdf_sample(V3 wo, const DevMaterial& m, Pcg& rng, BsdfSample& s) {
   s.delta = false;
   s.pdf = 0.f;
   s.f = v3s(0.f);
   s.wi = v3s(0.f);
-  if (m.flags & kMatDelta) {
-    if (m.flags & kMatTransmissive) {
+  const uint32_t fl = lobe_flags<kOpaque>(m);
+  if (fl & kMatDelta) {
+    if (fl & kMatTransmissive) {
       float f = fresnel_dielectric(wo.z, m.ior);
       if (rng.next_float() < f) return delta_refl_sample(wo, m, s);
       return delta_trans_sample(wo, m, s);
     }
     return delta_refl_sample(wo, m, s);
   }
-  if (m.flags & kMatConductor) return mfr_sample(wo, m, rng, s);
-  if (m.flags & kMatSubsurface) return cosine_sample(wo, ss_color(m), m, rng, s);
-  if (m.flags & kMatTransmissive) {
+  if (fl & kMatConductor) return mfr_sample(wo, m, rng, s);
+  if (fl & kMatSubsurface) return cosine_sample(wo, ss_color(m), m, rng, s);
+  if (fl & kMatTransmissive) {
     float f = fresnel_dielectric(fabsf(wo.z), m.ior);
     if (rng.next_float() < f) {
       if (!mfr_sample(wo, m, rng, s)) return false;

@@ -141,6 +141,7 @@ struct xb_renderer {
   std::vector<void*> scene_mem;
   DevScene scene{};
   bool has_scene = false;
+  bool scene_opaque = false;   // no delta, transmissive or subsurface material: shade_kernel<*, true>
   // framebuffer
   float4* accum = nullptr;                // FP32 per-pixel sum
   double* sum64 = nullptr;                // FP64 sum (flag)
@@ -417,7 +418,9 @@ __device__ __forceinline__ void add_L(float4* L, int p, V3 c) {
 // kOcc: the blocks of 128 threads the kernel is compiled to fit on one SM (xb_tuning
 // shade_occupancy): 4 keeps every value in registers (108), 8 and 12 cap them at 64 and 40 and
 // spill the rest to L1; the bounce is latency-bound, so more resident warps usually win.
-template <int kOcc>
+// kOpaque: the form for scenes without delta, transmissive or subsurface materials (smaller
+// code: the bounce's largest stall is the instruction cache), the same results.
+template <int kOcc, bool kOpaque>
 __global__ void __launch_bounds__(128, kOcc) shade_kernel(ShadeArgs a) {
   const int n = a.cnt[CNT_RAYS];
   const DevScene& sc = a.sc;
@@ -495,8 +498,8 @@ __global__ void __launch_bounds__(128, kOcc) shade_kernel(ShadeArgs a) {
             const V3 wo_l = onb.to_local(-ray.d);
             const V3 wi_l = onb.to_local(wi);
             if (cos_l > 1e-6f && wi_l.z > 1e-6f) {
-              const V3 f = bsdf_eval(wo_l, wi_l, mat);
-              const float bp = bsdf_pdf(wo_l, wi_l, mat);
+              const V3 f = bsdf_eval<kOpaque>(wo_l, wi_l, mat);
+              const float bp = bsdf_pdf<kOpaque>(wo_l, wi_l, mat);
               const float lpdf = ((1.0f / lt.p0.w) * pick_pdf) * (dsq / cos_l);
               const float mis = mis_power2(lpdf, bp);
               const float cs = wi_l.z;
@@ -524,8 +527,8 @@ __global__ void __launch_bounds__(128, kOcc) shade_kernel(ShadeArgs a) {
             const V3 wo_l = onb.to_local(-ray.d);
             const V3 wi_l = onb.to_local(sdir);
             if (wi_l.z > 1e-6f) {
-              const V3 f = bsdf_eval(wo_l, wi_l, mat);
-              const float bp = bsdf_pdf(wo_l, wi_l, mat);
+              const V3 f = bsdf_eval<kOpaque>(wo_l, wi_l, mat);
+              const float bp = bsdf_pdf<kOpaque>(wo_l, wi_l, mat);
               const float cs = wi_l.z;
               // cpu_tiled.cpp:166-183 divides by a 1e8 "pdf" (the sun then adds ~1e-8 of its
               // light); XB_FLAG_SUN_NEE weighs the delta light by its pick probability alone,
@@ -553,7 +556,7 @@ __global__ void __launch_bounds__(128, kOcc) shade_kernel(ShadeArgs a) {
         const Onb onb(fh.normal);
         const V3 wo_l = onb.to_local(-ray.d);
         BsdfSample s;
-        if (!bsdf_sample(wo_l, mat, rng, s)) break;
+        if (!bsdf_sample<kOpaque>(wo_l, mat, rng, s)) break;
         if (s.delta) {
           tp = tp * s.f;
         } else {
@@ -1784,9 +1787,15 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
         guided_shade_kernel<false, 8><<<r->grid_shade, 128, 0, L.s>>>(sa, ga);
     } else {
       StageTimer t(r, STAGE_SHADE, L.s);
-      if (r->tune.shade_occupancy == 4) shade_kernel<4><<<r->grid_shade, 128, 0, L.s>>>(sa);
-      else if (r->tune.shade_occupancy == 12) shade_kernel<12><<<r->grid_shade, 128, 0, L.s>>>(sa);
-      else shade_kernel<8><<<r->grid_shade, 128, 0, L.s>>>(sa);
+      if (r->scene_opaque) {
+        if (r->tune.shade_occupancy == 4) shade_kernel<4, true><<<r->grid_shade, 128, 0, L.s>>>(sa);
+        else if (r->tune.shade_occupancy == 12) shade_kernel<12, true><<<r->grid_shade, 128, 0, L.s>>>(sa);
+        else shade_kernel<8, true><<<r->grid_shade, 128, 0, L.s>>>(sa);
+      } else {
+        if (r->tune.shade_occupancy == 4) shade_kernel<4, false><<<r->grid_shade, 128, 0, L.s>>>(sa);
+        else if (r->tune.shade_occupancy == 12) shade_kernel<12, false><<<r->grid_shade, 128, 0, L.s>>>(sa);
+        else shade_kernel<8, false><<<r->grid_shade, 128, 0, L.s>>>(sa);
+      }
     }
     CK(cudaEventRecord(L.ev_shade[d], L.s));
     if (network_pass) {   // beside the shadow rays of this bounce, before the next closest hits
@@ -2374,7 +2383,11 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   }
   // ── materials, emitters, sky ──
   std::vector<DevMaterial> mats;
-  for (int i = 0; i < v->num_materials; ++i) mats.push_back(to_dev_material(v->materials[i]));
+  bool opaque = true;
+  for (int i = 0; i < v->num_materials; ++i) {
+    mats.push_back(to_dev_material(v->materials[i]));
+    opaque = opaque && (mats.back().flags & (kMatDelta | kMatTransmissive | kMatSubsurface)) == 0;
+  }
   std::vector<DevLight> lights;
   for (int i = 0; i < v->num_lights; ++i) {
     const xb_light& l = v->lights[i];
@@ -2437,6 +2450,7 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
     std::vector<float> cdf;
     if (sky_table(sc, cdf) && (rc = dev_upload(r, cdf, &sc.sky_cdf))) return rc;
   }
+  r->scene_opaque = opaque;
   r->has_scene = true;
   return XB_OK;
 }
