@@ -735,12 +735,13 @@ def incoherent_study(args, device: int) -> dict:
     """Traversal alone on incoherent rays: 2^22 rays with origins uniform in the scene's world
     bounds and directions uniform on the sphere, and 2^22 secondary rays harvested from bounce 2
     of the path tracer's own sampling (xenon_b200/raybatch.py), traced through
-    xb_trace_rays_device (closest hit, then any hit) on config 2 and config 3. Device Mrays/s
-    from CUDA events around each launch on the launching stream; inputs and hit records
-    (128 MiB + 256 MiB per batch) exceed the L2."""
+    xb_trace_rays_device (closest hit, then any hit) on config 2 and config 3, with each
+    workload's tuning (which picks persistent warps or one ray per thread for each kind of query).
+    Device Mrays/s from CUDA events around each launch on the launching stream; inputs and hit
+    records (128 MiB + 256 MiB per batch) exceed the L2."""
     import torch
     import xenon_b200 as xb
-    from xenon_b200 import abi, raybatch, scenes
+    from xenon_b200 import abi, autotune, raybatch, scenes
     out = {}
     n = args.incoherent_rays
     for name, make in (("config2", lambda: scenes.icosphere_scene(level=args.level)),
@@ -749,6 +750,9 @@ def incoherent_study(args, device: int) -> dict:
         hs = xb.HostScene.from_desc(desc)
         r = xb.Renderer(64, 64, desc.max_bounces, desc.min_bounces, device=device)
         r.upload_scene(hs)
+        tuned = autotune.load_tuning(name)
+        if tuned:   # persistent or one-ray-per-thread queries, as the workload's tuning picks
+            r.set_tuning(**tuned)
         view = hs.view()
         cam = xb.camera(desc.eye, desc.target, desc.fov, desc.width / desc.height)
         batches = {"uniform": raybatch.incoherent_rays(view, n, seed=5),

@@ -480,7 +480,11 @@ int  xb_reset_profile(xb_renderer *r);
 #define XB_TRACE_CLOSEST 0
 #define XB_TRACE_ANY     1
 int  xb_trace_rays(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit *hits, int32_t mode);
-/* Same on device memory and a caller stream (cudaStream_t, NULL = default). */
+/* Same on device memory and a caller stream (cudaStream_t, NULL = default). Closest-hit queries
+ * run on persistent warps when xb_tuning.extend_persistent_from_depth <= 1, any-hit queries when
+ * shadow_persistent = 1 (the renderer's own choice for its bounce and shadow rays; both are the
+ * defaults), else one ray per thread (also with XB_FLAG_THREAD_PER_RAY); the records are the same
+ * either way. Calls on different streams may overlap: they share no device state. */
 int  xb_trace_rays_device(xb_renderer *r, const xb_ray *rays, int64_t n, xb_hit *hits,
                           int32_t mode, void *stream);
 

@@ -40,6 +40,29 @@ def test_closest_and_any_hit_match_reference(name, ref):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", list(SCENES))
+def test_query_forms_return_the_same_records(name):
+    """xb_trace_rays runs its queries on persistent warps (the default tuning) or one ray per
+    thread (XB_FLAG_THREAD_PER_RAY, or a tuning without persistent bounce/shadow rays): the hit
+    records are equal byte for byte."""
+    desc = SCENES[name]()
+    rays = mixed_rays(desc, 1 << 15, seed=12)
+    hs = HostScene.from_desc(desc)
+    out = []
+    for flags, tune in ((0, {}), (abi.XB_FLAG_THREAD_PER_RAY, {}),
+                        (0, {"extend_persistent_from_depth": 64, "shadow_persistent": 2}),
+                        (0, {"refill": 1}), (0, {"refill": 32})):
+        r = Renderer(64, 64, flags=flags)
+        r.upload_scene(hs)
+        if tune:
+            r.set_tuning(**tune)
+        out.append((r.trace_rays(rays, abi.XB_TRACE_CLOSEST).tobytes(), r.trace_rays(rays, abi.XB_TRACE_ANY).tobytes()))
+        r.close()
+    for o in out[1:]:
+        assert o == out[0]
+
+
+@pytest.mark.gpu
 def test_reference_built_view_uploads_as_is(ref):
     """The drop-in path: the reference's own BLAS/TLAS arrays go through xb_upload_scene."""
     desc = scenes.instanced_grid(grid=3, levels=(3, 3, 3, 3), with_prims=True)

@@ -169,6 +169,7 @@ struct xb_renderer {
   int ext_persistent_from = 0;   // bounces >= this trace closest hits with persistent warps
   bool shadow_persistent = true;
   int occ_ext = 1, occ_pext = 1, occ_shadow = 1, occ_pshadow = 1;  // limits
+  int occ_api[2] = {1, 1};   // trace_api_persistent_kernel<closest / any>
   int stack_sh = 0;             // BLAS stack entries in shared memory (tuning shared_stack)
   xb_tuning tune{};
   // profiling
@@ -374,11 +375,13 @@ __global__ void __launch_bounds__(128) shadow_kernel(DevScene sc, const float4* 
 // ── persistent-warp variants (trace_persistent.cuh) ────────────────────────────
 template <bool kCount, int kSh>
 __global__ void __launch_bounds__(128) extend_persistent_kernel(DevScene sc, TraceQueue q, int refill) {
-  trace_queue_persistent<false, kCount, kSh>(sc, q, refill);
+  QueueIO io{q, *q.count};
+  trace_persistent<false, kCount, kSh>(sc, io, refill, false);
 }
 template <bool kCount, int kSh>
 __global__ void __launch_bounds__(128) shadow_persistent_kernel(DevScene sc, TraceQueue q, int refill) {
-  trace_queue_persistent<true, kCount, kSh>(sc, q, refill);
+  QueueIO io{q, *q.count};
+  trace_persistent<true, kCount, kSh>(sc, io, refill, q.far_first != 0);
 }
 
 // ── shade (cpu_tiled.cpp:34-217 for one bounce) ───────────────────────────────
@@ -1259,6 +1262,73 @@ __global__ void __launch_bounds__(128) trace_full_kernel(DevScene sc, const xb_r
   }
   if (overflow) atomicAdd(stats + STAT_OVERFLOW, 1ull);
   flush_counters(stats + (mode == XB_TRACE_CLOSEST ? STAT_EXT_WORK : STAT_SH_WORK), tc);
+}
+
+// xb_trace_rays_device on persistent warps (trace_persistent.cuh): each warp owns a contiguous
+// range of the caller's rays and refills its idle lanes from it, so a long ray no longer holds
+// its warp's finished lanes, and no cursor is shared between calls (calls on different streams
+// may overlap, as with trace_full_kernel). The hit records are trace_full_kernel's.
+struct ApiIO {
+  const xb_ray* rays;
+  xb_hit* hits;
+  unsigned long long* st;
+  int next, stop;
+  __device__ __forceinline__ int end() const { return stop; }
+  __device__ __forceinline__ int grab(int, int, int k) {
+    const int b = next;
+    next += k;
+    return b;
+  }
+  template <bool kAny>
+  __device__ __forceinline__ void load(int ray, V3& o, V3& d, float& tmin, float& tmax) const {
+    const xb_ray rr = rays[ray];
+    o = v3(rr.org[0], rr.org[1], rr.org[2]);
+    d = v3(rr.dir[0], rr.dir[1], rr.dir[2]);
+    tmin = rr.tmin;
+    tmax = rr.tmax;
+  }
+  __device__ __forceinline__ static xb_hit miss() {
+    xb_hit out;
+    memset(&out, 0, sizeof(out));
+    out.t = kInf; out.prim_id = -1; out.instance_id = -1; out.mat_id = -1;
+    return out;
+  }
+  __device__ __forceinline__ void finish_any(int ray, bool occluded) const {
+    xb_hit out = miss();
+    if (occluded) out.t = 0.f;
+    hits[ray] = out;
+  }
+  __device__ __forceinline__ void finish_closest(const DevScene& sc, int ray, V3 o, V3 d, float tmin, float tmax,
+                                                 const HitState& h) const {
+    xb_hit out = miss();
+    if (h.inst >= 0) {
+      const Ray r{o, d, tmin, tmax};
+      FullHit f;
+      complete_hit(sc, r, h, f);
+      out.t = h.t; out.u = f.u; out.v = f.v;
+      out.prim_id = f.prim_id; out.instance_id = f.instance_id; out.mat_id = f.mat_id;
+      out.front_face = f.front_face ? 1 : 0;
+      out.pos[0] = f.pos.x; out.pos[1] = f.pos.y; out.pos[2] = f.pos.z;
+      out.normal[0] = f.normal.x; out.normal[1] = f.normal.y; out.normal[2] = f.normal.z;
+      out.geo_normal[0] = f.geo_normal.x; out.geo_normal[1] = f.geo_normal.y;
+      out.geo_normal[2] = f.geo_normal.z;
+    }
+    hits[ray] = out;
+  }
+  __device__ __forceinline__ unsigned long long* stats() const { return st; }
+};
+
+template <bool kAny>
+__global__ void __launch_bounds__(128) trace_api_persistent_kernel(DevScene sc, const xb_ray* rays, int n,
+                                                                   xb_hit* hits, unsigned long long* stats,
+                                                                   int refill) {
+  const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t chunk = (n + warps - 1) / warps;
+  const int64_t b = w * chunk < n ? w * chunk : (int64_t)n;
+  const int64_t e = b + chunk < n ? b + chunk : (int64_t)n;
+  ApiIO io{rays, hits, stats, (int)b, (int)e};
+  trace_persistent<kAny, true, 0>(sc, io, refill, false);
 }
 
 // ── BSDF queries (xb_bsdf_eval / xb_bsdf_sample) ───────────────────────────────
@@ -2185,6 +2255,10 @@ int xb_create(const xb_config* cfg, xb_renderer** out) {
   r->occ_pext = std::max(occ, 1);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shadow_persistent_kernel<false, 0>, 128, 0);
   r->occ_pshadow = std::max(occ, 1);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_api_persistent_kernel<false>, 128, 0);
+  r->occ_api[0] = std::max(occ, 1);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trace_api_persistent_kernel<true>, 128, 0);
+  r->occ_api[1] = std::max(occ, 1);
   r->thread_per_ray = (cfg->flags & XB_FLAG_THREAD_PER_RAY) != 0;
   {
     // Paths per wave: whole samples of every pixel, about 2^21 paths in flight by default.
@@ -2978,8 +3052,19 @@ int xb_trace_rays_device(xb_renderer* r, const xb_ray* rays, int64_t n, xb_hit* 
   if (mode != XB_TRACE_CLOSEST && mode != XB_TRACE_ANY) return set_err(r, XB_E_INVALID, "bad trace mode %d", mode);
   if (n == 0) return XB_OK;
   cudaStream_t s = stream ? (cudaStream_t)stream : r->stream;
-  const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)r->num_sms * 16);
-  trace_full_kernel<<<grid, 128, 0, s>>>(r->scene, rays, n, hits, mode, r->stats);
+  const int any = mode == XB_TRACE_ANY ? 1 : 0;
+  // persistent warps, each over its own contiguous range of the batch, where the renderer's
+  // tuning puts its own rays of that kind on persistent warps (bounce rays for closest hits)
+  const bool persistent = any ? r->tune.shadow_persistent == 1 : r->tune.extend_persistent_from_depth <= 1;
+  if (!r->thread_per_ray && persistent && n <= (int64_t)INT32_MAX / 2) {
+    const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)r->num_sms * r->occ_api[any]);
+    const int refill = std::max(1, r->tune.refill);
+    if (any) trace_api_persistent_kernel<true><<<grid, 128, 0, s>>>(r->scene, rays, (int)n, hits, r->stats, refill);
+    else trace_api_persistent_kernel<false><<<grid, 128, 0, s>>>(r->scene, rays, (int)n, hits, r->stats, refill);
+  } else {
+    const int grid = (int)std::min<int64_t>((n + 127) / 128, (int64_t)r->num_sms * 16);
+    trace_full_kernel<<<grid, 128, 0, s>>>(r->scene, rays, n, hits, mode, r->stats);
+  }
   CK(cudaGetLastError());
   return XB_OK;
 }

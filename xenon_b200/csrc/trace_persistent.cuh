@@ -35,12 +35,50 @@ struct TraceQueue {
   int far_first;            // any-hit: descend into the farther child first
 };
 
-template <bool kAny, bool kCount, int kSh>
-__device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const TraceQueue& q,
-                                                       int refill) {
+// Where a warp's rays come from and where their answers go: the renderer's queues, the rays
+// taken from a shared cursor (a TraceQueue; xb_trace_rays_device has its own, in renderer.cu).
+//   end()                   one past the last ray index this warp may take
+//   grab(lane, leader, k)   the first of k consecutive ray indices for the warp's idle lanes
+//                           (warp-uniform: every lane calls it with the same k)
+//   load<kAny>(ray, o, d, tmin, tmax), finish_any(ray, occluded),
+//   finish_closest(sc, ray, o, d, tmin, tmax, h), stats()
+struct QueueIO {
+  TraceQueue q;
+  int n;
+  __device__ __forceinline__ int end() const { return n; }
+  __device__ __forceinline__ int grab(int lane, int leader, int k) const {
+    int base = 0;
+    if (lane == leader) base = atomicAdd(q.fetch, k);
+    return __shfl_sync(0xffffffffu, base, leader);
+  }
+  template <bool kAny>
+  __device__ __forceinline__ void load(int ray, V3& o, V3& d, float& tmin, float& tmax) const {
+    const float4 a = q.ray_o[ray], b = q.ray_d[ray];
+    o = v3(a.x, a.y, a.z);
+    d = v3(b.x, b.y, b.z);
+    if (kAny) { tmin = kShadowEps; tmax = a.w; }
+    else { tmin = a.w; tmax = b.w; }
+  }
+  __device__ __forceinline__ void finish_any(int ray, bool occluded) const {
+    if (occluded) return;
+    const float4 c = q.contrib[ray];
+    const int p = __float_as_int(q.ray_d[ray].w);
+    float4 l = q.L[p];
+    l.x = l.x + c.x; l.y = l.y + c.y; l.z = l.z + c.z;
+    q.L[p] = l;
+  }
+  __device__ __forceinline__ void finish_closest(const DevScene&, int ray, V3, V3, float, float,
+                                                 const HitState& h) const {
+    q.hit[ray] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+    q.hit_inst[ray] = h.inst;
+  }
+  __device__ __forceinline__ unsigned long long* stats() const { return q.stats; }
+};
+
+template <bool kAny, bool kCount, int kSh, class IO>
+__device__ __forceinline__ void trace_persistent(const DevScene& sc, IO& io, int refill, bool far_first) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int n = *q.count;
   uint32_t tstack[kStackSize];
   uint32_t bstack_local[kStackSize];
   extern __shared__ uint32_t s_stack[];
@@ -67,20 +105,14 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
     // ── refill idle lanes ──
     const unsigned idle = __ballot_sync(FULL, ray < 0);
     if (!exhausted && __popc(idle) >= refill) {
-      int base = 0;
       const int leader = __ffs(idle) - 1;
-      if (lane == leader) base = atomicAdd(q.fetch, __popc(idle));
-      base = __shfl_sync(FULL, base, leader);
-      if (base >= n) exhausted = true;
+      const int base = io.grab(lane, leader, __popc(idle));
+      if (base >= io.end()) exhausted = true;
       if (ray < 0) {
         const int mine = base + __popc(idle & ((1u << lane) - 1u));
-        if (mine < n) {
+        if (mine < io.end()) {
           ray = mine;
-          const float4 o = q.ray_o[ray], d = q.ray_d[ray];
-          wo = v3(o.x, o.y, o.z);
-          wd = v3(d.x, d.y, d.z);
-          if (kAny) { tmin = kShadowEps; tmax = o.w; }
-          else { tmin = o.w; tmax = d.w; }
+          io.template load<kAny>(ray, wo, wd, tmin, tmax);
           winv = v3(1.f / wd.x, 1.f / wd.y, 1.f / wd.z);
           sign0 = wd.x < 0.f; sign1 = wd.y < 0.f; sign2 = wd.z < 0.f;
           tsp = 0; bsp = 0; bactive = false; cur_inst = -1; tl_count = 0; tl_i = 0; leaf_count = 0;
@@ -119,7 +151,7 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
               if (bsp + 1 > kStackSize) {
                 overflow = true;
                 bactive = false; bsp = 0; tsp = 0; tl_count = 0;   // abandon (reported as overflow)
-              } else if ((tl < tr) != (kAny && q.far_first)) {
+              } else if ((tl < tr) != (kAny && far_first)) {
                 bstack.put(bsp++, er); bcur = el;
               } else {
                 bstack.put(bsp++, el); bcur = er;
@@ -186,18 +218,8 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
         } else {
           // ray finished
           want = false;
-          if (kAny) {
-            if (!occluded) {
-              const float4 c = q.contrib[ray];
-              const int p = __float_as_int(q.ray_d[ray].w);
-              float4 l = q.L[p];
-              l.x = l.x + c.x; l.y = l.y + c.y; l.z = l.z + c.z;
-              q.L[p] = l;
-            }
-          } else {
-            q.hit[ray] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
-            q.hit_inst[ray] = h.inst;
-          }
+          if (kAny) io.finish_any(ray, occluded);
+          else io.finish_closest(sc, ray, wo, wd, tmin, tmax, h);
           ray = -1;
         }
       }
@@ -232,9 +254,9 @@ __device__ __forceinline__ void trace_queue_persistent(const DevScene& sc, const
       }
     }
   }
-  if (overflow) atomicAdd(q.stats + 3, 1ull);
+  if (overflow) atomicAdd(io.stats() + 3, 1ull);
   if (kCount) {
-    unsigned long long* dst = q.stats + (kAny ? 12 : 8);
+    unsigned long long* dst = io.stats() + (kAny ? 12 : 8);
     atomicAdd(dst + 0, (unsigned long long)cnt.nodes);
     atomicAdd(dst + 1, (unsigned long long)cnt.tris);
     atomicAdd(dst + 2, (unsigned long long)cnt.tlas);
