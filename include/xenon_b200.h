@@ -290,6 +290,12 @@ typedef struct xb_renderer xb_renderer;
                                        default one (the sky is weighted by 1 in
                                        src/render/cpu_tiled.cpp:40-54). Ignored while guiding is on.
                                        Changes the random-number draws (not in parity mode). */
+#define XB_FLAG_WATERTIGHT      16  /* watertight ray-triangle test (Woop, Benthin and Wald 2013:
+                                       shear to ray space, edge functions, FP64 re-evaluation of a
+                                       zero edge) in every query of the renderer, instead of the
+                                       reference's Moller-Trumbore (src/geometry/primitives.h:25-49),
+                                       which can let a ray through the shared edge or vertex of two
+                                       triangles. Off (parity): Moller-Trumbore, bit-exact hits */
 
 typedef struct xb_config {
   int32_t width, height;

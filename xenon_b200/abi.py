@@ -26,6 +26,7 @@ XB_FLAG_FP64_ACCUM = 1
 XB_FLAG_THREAD_PER_RAY = 2
 XB_FLAG_SUN_NEE = 4
 XB_FLAG_SKY_IS = 8
+XB_FLAG_WATERTIGHT = 16
 XB_MAT_CONDUCTOR, XB_MAT_TRANSMISSIVE, XB_MAT_SUBSURFACE, XB_MAT_DELTA, XB_MAT_EMISSIVE = 1, 2, 4, 8, 16
 
 # xb_material: 22 floats, field order of the C struct

@@ -115,6 +115,7 @@ struct DevScene {
   float sky_intensity;
   int32_t sun_nee;   // XB_FLAG_SUN_NEE: directional lights weighted as delta lights (else the reference's 1e8)
   const float* sky_cdf;   // XB_FLAG_SKY_IS: kSkyBins + 1 cumulative bin masses over y in [-1, 1] (or nullptr)
+  int32_t watertight;     // XB_FLAG_WATERTIGHT: ray_triangle_wt instead of Moller-Trumbore
 };
 
 // The sky's luminance distribution over directions. The gradient sky (Environment::evaluate)
@@ -226,6 +227,54 @@ __device__ __forceinline__ bool ray_triangle(V3 o, V3 d, float tmin, V3 v0, V3 v
   if (v < 0.f || u + v > 1.f) return false;
   t = inv_a * dot(e2, q);
   return t >= tmin && t <= t_max;
+}
+
+// Watertight ray-triangle test (Woop, Benthin, Wald, "Watertight Ray/Triangle Intersection",
+// JCGT 2(1), 2013): the vertices are translated to the ray origin and sheared so that the ray
+// runs along +z; the 2D edge functions U, V, W then decide the hit. Two triangles that share an
+// edge evaluate its edge function from the same two transformed vertices, in opposite order, so
+// (with no fused multiply-add: this file is compiled with -fmad=false) the values are exact
+// negatives and a ray cannot pass between them. A zero edge function is re-evaluated in FP64.
+// Same interface as ray_triangle (u, v: the weights of v1 and v2), and the same acceptance
+// tmin <= t <= t_max; inv = 1 / d.
+__device__ __forceinline__ bool ray_triangle_wt(V3 o, V3 d, V3 inv, float tmin, V3 v0, V3 v1, V3 v2,
+                                                float t_max, float& t, float& u, float& v) {
+  const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  const int kz = (ax > ay && ax > az) ? 0 : (ay > az ? 1 : 2);
+  int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
+  const float dz = comp(d, kz);
+  if (dz < 0.f) { const int k = kx; kx = ky; ky = k; }   // keeps the winding
+  const float sz = comp(inv, kz);
+  const float sx = comp(d, kx) * sz, sy = comp(d, ky) * sz;
+  const V3 A = v0 - o, B = v1 - o, C = v2 - o;
+  const float Ax = comp(A, kx) - sx * comp(A, kz), Ay = comp(A, ky) - sy * comp(A, kz);
+  const float Bx = comp(B, kx) - sx * comp(B, kz), By = comp(B, ky) - sy * comp(B, kz);
+  const float Cx = comp(C, kx) - sx * comp(C, kz), Cy = comp(C, ky) - sy * comp(C, kz);
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.f || V == 0.f || W == 0.f) {
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+  }
+  if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+  const float det = U + V + W;
+  if (det == 0.f) return false;
+  const float T = U * (sz * comp(A, kz)) + V * (sz * comp(B, kz)) + W * (sz * comp(C, kz));
+  const float rdet = 1.f / det;
+  t = T * rdet;
+  if (!(t >= tmin && t <= t_max)) return false;
+  u = V * rdet;
+  v = W * rdet;
+  return true;
+}
+
+// The scene's triangle test: Moller-Trumbore (the reference's, bit-exact), or the watertight one.
+__device__ __forceinline__ bool tri_hit(const DevScene& sc, V3 o, V3 d, V3 inv, float tmin, V3 v0, V3 v1,
+                                        V3 v2, float t_max, float& t, float& u, float& v) {
+  if (sc.watertight) return ray_triangle_wt(o, d, inv, tmin, v0, v1, v2, t_max, t, u, v);
+  return ray_triangle(o, d, tmin, v0, v1, v2, t_max, t, u, v);
 }
 
 // SSE minps / maxps: (a < b) ? a : b and (a > b) ? a : b (NaN → second operand)
@@ -390,7 +439,7 @@ __device__ __forceinline__ bool blas_closest(const DevScene& sc, int root, const
         const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
         if (kCount) cnt.tris++;
         float t, u, v;
-        if (ray_triangle(r.o, r.d, r.tmin, ld3(a), ld3(b), ld3(c), h.t, t, u, v)) {
+        if (tri_hit(sc, r.o, r.d, inv, r.tmin, ld3(a), ld3(b), ld3(c), h.t, t, u, v)) {
           h.t = t; h.u = u; h.v = v;
           h.prim = (int32_t)(child + i);
           h.inst = inst_idx;
@@ -443,7 +492,7 @@ __device__ __forceinline__ bool blas_any(const DevScene& sc, int root, const Ray
         const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
         if (kCount) cnt.tris++;
         float t, u, v;
-        if (ray_triangle(r.o, r.d, r.tmin, ld3(a), ld3(b), ld3(c), r.tmax, t, u, v)) return true;
+        if (tri_hit(sc, r.o, r.d, inv, r.tmin, ld3(a), ld3(b), ld3(c), r.tmax, t, u, v)) return true;
       }
       if (ptr == 0) return false;
       cur = stack.get(--ptr);

@@ -2520,6 +2520,7 @@ int xb_upload_scene(xb_renderer* r, const xb_scene_view* v) {
   sc.sky_inv_sharpness = 1.0f / v->sky.sharpness;
   sc.sky_intensity = v->sky.intensity;
   sc.sun_nee = (r->cfg.flags & XB_FLAG_SUN_NEE) != 0;
+  sc.watertight = (r->cfg.flags & XB_FLAG_WATERTIGHT) != 0;
   if ((r->cfg.flags & XB_FLAG_SKY_IS) && sc.sky_intensity > 0.f) {
     std::vector<float> cdf;
     if (sky_table(sc, cdf) && (rc = dev_upload(r, cdf, &sc.sky_cdf))) return rc;

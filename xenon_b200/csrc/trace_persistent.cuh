@@ -234,7 +234,7 @@ __device__ __forceinline__ void trace_persistent(const DevScene& sc, IO& io, int
         const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
         if (kCount) cnt.tris++;
         float t, u, v;
-        if (ray_triangle(lo, ld, tmin, ld3(a), ld3(b), ld3(c), kAny ? tmax : tbest, t, u, v)) {
+        if (tri_hit(sc, lo, ld, linv, tmin, ld3(a), ld3(b), ld3(c), kAny ? tmax : tbest, t, u, v)) {
           if (kAny) {
             occluded = true;
             break;
