@@ -49,6 +49,19 @@ def test_coordinate_descent_finds_the_minimum_and_measures_multi_sample_calls():
     assert len(firsts) == len(set(firsts))
 
 
+def test_plain_workloads_leave_the_guided_knobs_alone():
+    """guided_form changes nothing in a plain render, so a plain search must not move it (a
+    noise 'gain' there would slow down guided renders that share the tuning)."""
+    class Noisy(FakeRenderer):
+        BEST = dict(FakeRenderer.BEST, guided_form=2)
+    r = Noisy()
+    res = autotune.autotune(r, None, "fake", calls=1, spp_per_call=1, save=False, log=lambda *_: None)
+    assert res["tuning"]["guided_form"] == autotune.SPACE["guided_form"][0]
+    r = Noisy()
+    res = autotune.autotune(r, None, "fake", calls=1, spp_per_call=1, save=False, log=lambda *_: None, guided=True)
+    assert res["tuning"]["guided_form"] == 2
+
+
 def test_tuning_files_round_trip(tmp_path, monkeypatch):
     monkeypatch.setattr(autotune, "TUNING_DIR", str(tmp_path))
     assert autotune.load_tuning("fake", gpu="G") is None

@@ -12,6 +12,7 @@ two passes), and keeps the fastest setting:
   lane_stagger                   bounces a lane's first wave shades before the next lane's starts
   graph                          captured CUDA graphs of the bounce loop, or direct launches
   guided_form                    guided bounce as a bounce kernel + network pass, or one fused kernel
+                                 (searched for guided workloads only)
   shade_occupancy                blocks per SM the shading kernels are compiled to fit (registers)
   shared_stack                   BLAS stack entries per thread kept in shared memory (1: none, 16)
   pixel_order                    camera rays in scanline order or in 8x4 pixel tiles per warp
@@ -84,8 +85,13 @@ def measure(renderer, cam, calls: int, spp_per_call: int, first: int) -> float:
     return ms / (calls * spp_per_call)
 
 
+# Knobs that only guided bounces read: a plain workload leaves them as they are (any gain they
+# showed there would be noise, and a plain tuning also serves guided views of the same scene).
+GUIDED_ONLY = ("guided_form",)
+
+
 def autotune(renderer, cam, workload: str, calls: int = 3, spp_per_call: int = 8, passes: int = 2,
-             save: bool = True, log=print) -> dict:
+             save: bool = True, log=print, guided: bool = False) -> dict:
     best = dict(renderer.tuning())
     seq = [1000]
 
@@ -98,6 +104,8 @@ def autotune(renderer, cam, workload: str, calls: int = 3, spp_per_call: int = 8
     log(f"start {best_ms:.3f} ms/spp {best}")
     for _ in range(passes):
         for key, values in SPACE.items():
+            if key in GUIDED_ONLY and not guided:
+                continue
             for v in values:
                 if best.get(key) == v:
                     continue
@@ -150,7 +158,7 @@ if __name__ == "__main__":
         r.set_guiding(True, train_spp=64, steps_per_spp=32, keep_training_samples=2)
         r.render_frame(cam, 64)
         r.set_guiding(True, train_spp=-1)
-    res = autotune(r, cam, a.workload, calls=a.calls, spp_per_call=a.spp_per_call)
+    res = autotune(r, cam, a.workload, calls=a.calls, spp_per_call=a.spp_per_call, guided=a.workload == "config4g")
     print(json.dumps(res))
     if a.out:
         with open(a.out, "w") as f:
