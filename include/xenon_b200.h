@@ -622,6 +622,12 @@ int  xb_guide_mixture_sample(const float *lobes, int64_t rows, const float *u, f
  * Host buffers. No reference counterpart (the reference has no tensor-core code). */
 int  xb_tc_gemm_bf16(const uint16_t *A, const uint16_t *B, int64_t rows, int32_t n, float *D);
 
+/* The failure path of the bounded device waits (every tensor-core step waits on an mbarrier with
+ * a poll limit and reports XB_E_TIMEOUT instead of hanging): one warp waits on an mbarrier that
+ * nothing completes (arrive = 0: returns XB_E_TIMEOUT) or that it completes itself (arrive = 1:
+ * XB_OK). The context stays usable either way. */
+int  xb_selftest_wait(int32_t arrive);
+
 #ifdef __cplusplus
 }
 #endif

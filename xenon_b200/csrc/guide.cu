@@ -548,9 +548,38 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(const __nv_bfloat16* __res
   if (warp == 0) tmem_dealloc(tbase, 64);
 }
 
+// The bounded completion wait of every tensor-core step, on an mbarrier that nothing completes
+// (arrive = 0) or that one of its own threads completes (arrive = 1): the failed wait gives up
+// after `limit` polls and reports through *err, and the kernel returns.
+__global__ void wait_selftest_kernel(int arrive, uint32_t limit, int* err) {
+  __shared__ __align__(8) uint64_t mbar;
+  if (threadIdx.x == 0) mbar_init(&mbar, 1);
+  __syncthreads();
+  if (arrive && threadIdx.x == 0) mbar_arrive(&mbar);
+  const bool done = mbar_wait(&mbar, 0, limit);
+  if (!done && threadIdx.x == 0) atomicExch(err, 1);
+}
+
 }  // namespace
 
 extern "C" {
+
+int xb_selftest_wait(int32_t arrive) {
+  int* derr = nullptr;
+  if (cudaMalloc(&derr, sizeof(int)) != cudaSuccess) return xb::fail(XB_E_OOM, "xb_selftest_wait: out of device memory");
+  int herr = 0;
+  cudaError_t e = cudaMemset(derr, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    wait_selftest_kernel<<<1, 32>>>(arrive ? 1 : 0, 1u << 14, derr);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(derr);
+  if (e != cudaSuccess) return xb::fail(XB_E_CUDA, "xb_selftest_wait: %s", cudaGetErrorString(e));
+  if (herr) return xb::fail(XB_E_TIMEOUT, "xb_selftest_wait: the completion wait ran out (as asked)");
+  return XB_OK;
+}
 
 int xb_tc_gemm_bf16(const uint16_t* A, const uint16_t* B, int64_t rows, int32_t n, float* D) {
   if (!A || !B || !D || rows <= 0 || rows > (1 << 24) || (n != 16 && n != 32 && n != 48 && n != 64))

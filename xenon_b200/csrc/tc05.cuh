@@ -86,6 +86,10 @@ __device__ __forceinline__ bool mbar_test(uint64_t* mbar, uint32_t parity) {
       : "=r"(ok) : "r"(smem_u32(mbar)), "r"(parity) : "memory");
   return ok != 0;
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n"
+               :: "r"(smem_u32(mbar)) : "memory");
+}
 // Bounded wait: false if the phase did not complete within `limit` polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit = 1u << 22) {
   for (uint32_t i = 0; i < limit; ++i)

@@ -66,6 +66,7 @@ SIGNATURES = {
     "xb_bsdf_sample": ([_P, _I64, _P, _P, _P, _P, _P, _P], _I),
     "xb_bsdf_density": ([_P, _I64, _P, _P, _P], _I),
     "xb_tc_gemm_bf16": ([_P, _P, _I64, _I32, _P], _I),
+    "xb_selftest_wait": ([_I32], _I),
     "xb_render_views": ([_P, _P, _I32], _I),
     "xb_resolve_async": ([_P, _P], _I),
     "xb_sync": ([_P], _I),
