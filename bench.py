@@ -494,7 +494,7 @@ def sky_study(args, device: int) -> dict:
 
 
 def build_study(args) -> dict:
-    """BVH build of config 2's scene (1,310,722 triangles, binned SAH as the reference builds it):
+    """BVH build and refit of config 2's scene (1,310,722 triangles, binned SAH as the reference builds it):
     wall time of xb_scene_build (the BLAS, the TLAS and the flattened arrays; the mesh already
     added) with the recursive host build on one thread and on every host thread, and with the
     level-synchronous build on the device (XB_BUILD_DEVICE, host-to-device copy of the build items
@@ -517,6 +517,33 @@ def build_study(args) -> dict:
     out = {"triangles": desc.num_triangles, "host_1_thread_s": timed(build_threads=1),
            "host_all_threads_s": timed(build_threads=0), "device_s": timed(build_mode=abi.XB_BUILD_DEVICE),
            "host_threads": os.cpu_count()}
+    # refit of the displaced sphere's BLAS after its vertices moved (topology kept): on the device
+    # (xb_refit_mesh: positions copied in, three refit passes, TLAS rebuilt) against the host refit
+    # (xb_scene_refit_mesh) and a new upload; median of three after one untimed call each
+    hs = xb.HostScene.from_desc(desc)
+    m = int(np.argmax([len(mm.positions) for mm in desc.meshes]))
+    pos = np.asarray(desc.meshes[m].positions, np.float32)
+    moved = [(pos * np.float32(1.0 + 0.01 * k)).astype(np.float32) for k in range(1, 5)]
+    r = xb.Renderer(64, 64)
+    r.upload_scene(hs)
+
+    def med(fn):
+        fn(moved[0])
+        t = []
+        for p in moved[1:]:
+            t0 = time.perf_counter()
+            fn(p)
+            t.append(time.perf_counter() - t0)
+        return float(np.median(t))
+
+    out["refit_vertices"] = int(len(pos))
+    out["refit_device_s"] = med(lambda p: r.refit_mesh(m, p))
+
+    def host_refit(p):
+        hs.refit_mesh(m, p)
+        r.upload_scene(hs)
+    out["refit_host_and_upload_s"] = med(host_refit)
+    r.close()
     return out
 
 
