@@ -78,6 +78,31 @@ def test_config2_view_agrees_per_pixel(ref):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["config3_grid", "config4_room"])
+def test_config_views_agree_per_pixel(name, ref):
+    """Config 3 (the full 16x16 instance grid, random diffuse / conductor / dielectric materials,
+    sky + 4 quad lights, depth 12) and config 4 (the closed room, the light behind the baffle, the
+    500k-triangle glass sphere, depth 16) at 1/8 of their pixels, samples 1 and 2, per pixel
+    against the reference's render_frame_tiled with the same seeds."""
+    desc = CONFIGS[name]()
+    w, h = desc.width // 8, desc.height // 8
+    rr = ref.RefRenderer(w, h, desc.min_bounces, desc.max_bounces)
+    s, _ = rr.render(ref.RefScene(desc), desc.eye, desc.target, desc.fov, 1, 2)
+    want = s / 2
+    ok = np.isfinite(want).all(-1)   # the reference keeps non-finite path radiance
+    r = Renderer(w, h, desc.max_bounces, desc.min_bounces)
+    r.upload_scene(HostScene.from_desc(desc))
+    r.render_range(camera(desc.eye, desc.target, desc.fov, w / h), 1, 2)
+    got = r.resolve()
+    assert r.stats().overflow == 0
+    frac = per_pixel_agreement(got[ok], want[ok])
+    print(name, f"{w}x{h} per-pixel agreement", frac, "relmse", relmse(got[ok], want[ok]),
+          "reference non-finite pixels", int((~ok).sum()))
+    assert (~ok).sum() <= 0.001 * ok.size
+    assert frac > 0.97, frac
+
+
+@pytest.mark.gpu
 def test_config1_converged_at_full_size():
     """Config 1 (256x256 Cornell box) over samples 1..16384 against the reference's own render of
     the same samples: per-pixel relMSE below 1e-3."""
