@@ -445,9 +445,10 @@ typedef struct xb_tuning {
   int32_t guided_form;                  /* guided bounces: 1 (default) a plain-form bounce kernel
                                            plus a network pass over the guided vertices; 2 one
                                            fused kernel. Same image either way. */
-  int32_t shade_occupancy;              /* shading kernels compiled to fit 4, 8 (default) or 12
-                                           blocks of 128 threads per SM: fewer registers per
-                                           thread, the rest spilled to L1 (other values: 8) */
+  int32_t shade_occupancy;              /* shading kernels compiled to fit 4, 8 (default), 12 or
+                                           16 blocks of 128 threads per SM: fewer registers per
+                                           thread, the rest spilled to L1 (other values: 8; the
+                                           guided bounces take 4 or 8, 8 for 12 and 16) */
   int32_t shared_stack;                 /* traversal kernels: 16 = the first 16 entries of each
                                            thread's BLAS stack in shared memory (8 KB per block of
                                            128 threads), the rest in local memory; 1 (default, and

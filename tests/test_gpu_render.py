@@ -85,7 +85,7 @@ def test_traversal_variants_render_identically(builder):
     desc = builder()
     imgs = []
     for flags, tune in ((0, {}), (abi.XB_FLAG_THREAD_PER_RAY, {}), (0, {"overlap": 2}),
-                        (0, {"shade_occupancy": 4}), (0, {"shade_occupancy": 12}),
+                        (0, {"shade_occupancy": 4}), (0, {"shade_occupancy": 12}), (0, {"shade_occupancy": 16}),
                         (0, {"extend_persistent_from_depth": 1, "shadow_order": 2, "refill": 4}),
                         (0, {"shared_stack": 16}),
                         (0, {"shared_stack": 16, "extend_persistent_from_depth": 1, "shadow_persistent": 2}),

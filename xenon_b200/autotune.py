@@ -43,7 +43,7 @@ SPACE = {
     "lane_stagger": [1, 2, 3],
     "graph": [1, 2],
     "guided_form": [1, 2],
-    "shade_occupancy": [4, 8, 12],
+    "shade_occupancy": [4, 8, 12, 16],
     "shared_stack": [1, 16],
     "pixel_order": [1, 2],
     "refill": [2, 4, 8, 16, 24],

@@ -419,8 +419,8 @@ __device__ __forceinline__ void add_L(float4* L, int p, V3 c) {
 }
 
 // kOcc: the blocks of 128 threads the kernel is compiled to fit on one SM (xb_tuning
-// shade_occupancy): 4 keeps every value in registers (108), 8 and 12 cap them at 64 and 40 and
-// spill the rest to L1; the bounce is latency-bound, so more resident warps usually win.
+// shade_occupancy): 4 keeps every value in registers (108), 8, 12 and 16 cap them at 64, 40 and
+// 32 and spill the rest to L1; the bounce is latency-bound, so more resident warps usually win.
 // kOpaque: the form for scenes without delta, transmissive or subsurface materials (smaller
 // code: the bounce's largest stall is the instruction cache), the same results.
 template <int kOcc, bool kOpaque>
@@ -1605,7 +1605,8 @@ int apply_tuning(xb_renderer* r, const xb_tuning& t) {
   c.graph = std::min(2, pick(t.graph, c.graph, 1));
   c.guided_form = std::min(2, pick(t.guided_form, c.guided_form, 1));
   c.shade_occupancy = pick(t.shade_occupancy, c.shade_occupancy, 8);
-  if (c.shade_occupancy != 4 && c.shade_occupancy != 8 && c.shade_occupancy != 12) c.shade_occupancy = 8;
+  if (c.shade_occupancy != 4 && c.shade_occupancy != 8 && c.shade_occupancy != 12 && c.shade_occupancy != 16)
+    c.shade_occupancy = 8;
   c.pixel_order = std::min(2, pick(t.pixel_order, c.pixel_order, 2));
   c.shared_stack = pick(t.shared_stack, c.shared_stack, 1);
   if (c.shared_stack != 1 && c.shared_stack != kSharedStack) c.shared_stack = 1;
@@ -1860,10 +1861,12 @@ int trace_bounces(xb_renderer* r, const LaneRef& L, bool train, int rec_stride, 
       if (r->scene_opaque) {
         if (r->tune.shade_occupancy == 4) shade_kernel<4, true><<<r->grid_shade, 128, 0, L.s>>>(sa);
         else if (r->tune.shade_occupancy == 12) shade_kernel<12, true><<<r->grid_shade, 128, 0, L.s>>>(sa);
+        else if (r->tune.shade_occupancy == 16) shade_kernel<16, true><<<r->grid_shade, 128, 0, L.s>>>(sa);
         else shade_kernel<8, true><<<r->grid_shade, 128, 0, L.s>>>(sa);
       } else {
         if (r->tune.shade_occupancy == 4) shade_kernel<4, false><<<r->grid_shade, 128, 0, L.s>>>(sa);
         else if (r->tune.shade_occupancy == 12) shade_kernel<12, false><<<r->grid_shade, 128, 0, L.s>>>(sa);
+        else if (r->tune.shade_occupancy == 16) shade_kernel<16, false><<<r->grid_shade, 128, 0, L.s>>>(sa);
         else shade_kernel<8, false><<<r->grid_shade, 128, 0, L.s>>>(sa);
       }
     }
