@@ -53,5 +53,11 @@ void build_bvh_levels(std::vector<BuildItem>& items, int bins, uint32_t max_leaf
 // the device). Throws std::runtime_error on a CUDA error, std::invalid_argument on bad arguments.
 void build_bvh_device(const std::vector<BuildItem>& items, int bins, uint32_t max_leaf, bool leaf_cost,
                       std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
+// The device build of a triangle mesh's BLAS, its build items (each triangle's box in vertex
+// order and its centroid, as HostScene::build makes them) made on the device from the mesh's
+// vertices and indices: the same arrays as build_bvh_device over the host-made items.
+struct HostMesh;
+void build_bvh_device_mesh(const HostMesh& m, int bins, uint32_t max_leaf, bool leaf_cost,
+                           std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order);
 
 }  // namespace xb

@@ -25,6 +25,7 @@
 
 #include "bvh_build.h"
 #include "bvh_level_kernels.h"
+#include "scene_host.h"
 
 namespace xb {
 namespace {
@@ -341,6 +342,29 @@ __global__ void item_order(const LevelItem* items, uint32_t n, uint32_t* order) 
   if (i < n) order[i] = items[i].index;
 }
 
+// Triangle t's build item, as the host makes it (HostScene::build): the box of its three vertices
+// folded in index order with std::min / std::max semantics, and the centroid (mn + mx) * 0.5
+// (this file is compiled without fused multiply-add, so the arithmetic is the host's).
+__global__ void mesh_items(const float* vx, const float* vy, const float* vz, const int32_t* idx, uint32_t ntris,
+                           LevelItem* items) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntris) return;
+  RefitBox b;
+  refit_empty(b);
+  for (int k = 0; k < 3; ++k) {
+    const int32_t v = idx[3 * (size_t)t + k];
+    refit_grow(b, vx[v], vy[v], vz[v]);
+  }
+  LevelItem it;
+  for (int k = 0; k < 3; ++k) {
+    it.mn[k] = b.mn[k];
+    it.mx[k] = b.mx[k];
+    it.c[k] = (b.mn[k] + b.mx[k]) * 0.5f;
+  }
+  it.index = t;
+  items[t] = it;
+}
+
 __global__ void place_root(uint32_t* pos, uint32_t* pair) {
   pos[0] = 0;
   pair[0] = 1;
@@ -519,6 +543,35 @@ struct DeviceLevelBuild {
     n = (uint32_t)host_items.size();
     allocate();
     ck(cudaMemcpy(items, host_items.data(), (size_t)n * sizeof(LevelItem), cudaMemcpyHostToDevice), "upload items");
+    run(nodes, order_out);
+  }
+
+  // The same from a triangle mesh: its vertices and indices go up, the items are made on the
+  // device (the positions and indices are about half the bytes of the items).
+  void build(const HostMesh& m, std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order_out) {
+    n = (uint32_t)m.num_triangles();
+    allocate();
+    const size_t nv = (size_t)m.num_vertices();
+    float* dv = nullptr;
+    int32_t* di = nullptr;
+    ck(cudaMalloc(&dv, std::max<size_t>(nv, 1) * 3 * sizeof(float)), "allocate the mesh");
+    cudaError_t e = cudaMalloc(&di, (size_t)n * 3 * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemcpy(dv, m.vx.data(), nv * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dv + nv, m.vy.data(), nv * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dv + 2 * nv, m.vz.data(), nv * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(di, m.indices.data(), (size_t)n * 3 * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      mesh_items<<<blocks(n), 128>>>(dv, dv + nv, dv + 2 * nv, di, n, items);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(dv);
+    cudaFree(di);
+    ck(e, "build items from the mesh");
+    run(nodes, order_out);
+  }
+
+  void run(std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order_out) {
     ck(cudaMemset(left, 0xff, (size_t)n * sizeof(int64_t)), "clear rank tables");
     ck(cudaMemset(right, 0xff, (size_t)n * sizeof(int64_t)), "clear rank tables");
     ck(cudaMemset(tot, 0, sizeof(DepthTotals)), "clear depth totals");
@@ -569,6 +622,22 @@ void build_bvh_device(const std::vector<BuildItem>& items, int bins, uint32_t ma
   b.max_leaf = max_leaf;
   b.leaf_cost = leaf_cost;
   b.build(items, nodes, order);
+}
+
+void build_bvh_device_mesh(const HostMesh& m, int bins, uint32_t max_leaf, bool leaf_cost,
+                           std::vector<xb_bvh_node>& nodes, std::vector<uint32_t>& order) {
+  if (bins < 2 || bins > kLevelMaxBins) throw std::invalid_argument("build_bvh_device_mesh: bins");
+  if ((size_t)m.num_triangles() >= (1u << 31)) throw std::invalid_argument("build_bvh_device_mesh: too many triangles");
+  for (int32_t v : m.indices)
+    if (v < 0 || v >= m.num_vertices()) throw std::invalid_argument("build_bvh_device_mesh: index out of range");
+  nodes.clear();
+  order.clear();
+  if (m.num_triangles() == 0) return;
+  DeviceLevelBuild b;
+  b.bins = bins;
+  b.max_leaf = max_leaf;
+  b.leaf_cost = leaf_cost;
+  b.build(m, nodes, order);
 }
 
 }  // namespace xb

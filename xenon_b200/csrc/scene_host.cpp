@@ -358,6 +358,10 @@ void HostScene::build() {
   int par_depth = 0;
   while (par_depth < 4 && (2 << par_depth) <= threads) ++par_depth;
   auto build_mesh = [&](HostMesh& m) {
+    if (build_mode == 2) {   // the items are made on the device too
+      build_bvh_device_mesh(m, 12, 2, true, m.nodes, m.prims);
+      return;
+    }
     std::vector<BuildItem> items(m.num_triangles());
     for (int t = 0; t < m.num_triangles(); ++t) {
       Bounds b;
@@ -366,8 +370,7 @@ void HostScene::build() {
       b.grow(m.vertex(m.indices[3 * t + 2]));
       items[t] = {b, b.center(), (uint32_t)t};
     }
-    if (build_mode == 2) build_bvh_device(items, 12, 2, true, m.nodes, m.prims);
-    else if (build_mode == 1) build_bvh_levels(items, 12, 2, true, m.nodes, m.prims);
+    if (build_mode == 1) build_bvh_levels(items, 12, 2, true, m.nodes, m.prims);
     else BvhBuilder(12, 2, true, par_depth).build(items, m.nodes, m.prims);
   };
   std::atomic<size_t> next{0};
