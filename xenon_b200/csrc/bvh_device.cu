@@ -46,10 +46,12 @@ struct DepthTotals {
   uint32_t chunks;     // chunks of the depth's nodes
   uint32_t children;   // nodes of the next depth
   uint32_t medians;    // nodes split by the median (listed in med_list)
+  uint32_t big;        // nodes of more than kBlockNodeChunks chunks (listed in big_list)
   int32_t error;       // LevelArgs::error; 3 a child past the node array, 4 a node placed past it
 };
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kBlockNodeChunks = 256;   // larger nodes fold their chunks with a block
 
 // ── per-chunk and per-item passes: one thread each ──────────────────────────────────────────
 __global__ void lvl_bounds(LevelArgs a) {
@@ -110,7 +112,7 @@ __global__ void lvl_plane_w(LevelArgs a) {
   const uint32_t x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (x >= a.ntasks) return;   // the whole warp
   const LevelTask t = a.tasks[x];
-  if (t.nchunks == 0) return;   // split whole by lvl_small
+  if (t.nchunks == 0 || t.nchunks > kBlockNodeChunks) return;   // lvl_small / lvl_plane_blk
   RefitBox box, cb;
   refit_empty(box);
   refit_empty(cb);
@@ -129,7 +131,7 @@ __global__ void lvl_sah_w(LevelArgs a) {
   const uint32_t x = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (x >= a.ntasks) return;   // the whole warp
   const LevelTask t = a.tasks[x];
-  if (t.nchunks == 0 || a.out[x].state != 1) return;
+  if (t.nchunks == 0 || t.nchunks > kBlockNodeChunks || a.out[x].state != 1) return;   // lvl_sah_blk
   RefitBox bin_box[kLevelMaxBins];
   int bin_cnt[kLevelMaxBins];
   for (int k = 0; k < a.bins; ++k) { refit_empty(bin_box[k]); bin_cnt[k] = 0; }
@@ -169,6 +171,87 @@ __global__ void lvl_prefix_w(LevelArgs a) {
     run += a.chunk_pass[c];
   }
   if (lane == 0) lvl_prefix_finish(a, x, m);
+}
+
+// ── per-node folds of the largest nodes: one block each ─────────────────────────────────────
+// A node of more than kBlockNodeChunks chunks (the top levels: the root has n / 64) would leave a
+// warp folding hundreds of chunks per lane; these nodes, listed as the depth's chunk counts are
+// made, take a block of kFoldThreads instead. Thread t folds a contiguous run of chunks, each warp
+// folds its lanes left to right, and warp 0 folds the warps' results left to right: the
+// sequential fold again.
+constexpr int kFoldThreads = 256, kFoldWarps = kFoldThreads / 32;
+
+__global__ void __launch_bounds__(kFoldThreads) lvl_plane_blk(LevelArgs a, const uint32_t* big_list,
+                                                              const DepthTotals* tot) {
+  __shared__ RefitBox sbox[kFoldWarps], scb[kFoldWarps];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t i = blockIdx.x; i < tot->big; i += gridDim.x) {
+    const uint32_t x = big_list[i];
+    const LevelTask t = a.tasks[x];
+    const uint32_t per = (t.nchunks + kFoldThreads - 1) / kFoldThreads;
+    const uint32_t b = min(t.nchunks, threadIdx.x * per), e = min(t.nchunks, b + per);
+    RefitBox box, cb;
+    refit_empty(box);
+    refit_empty(cb);
+    for (uint32_t c = t.chunk0 + b; c < t.chunk0 + e; ++c) {
+      refit_grow(box, a.chunk_box[c]);
+      refit_grow(cb, a.chunk_cbox[c]);
+    }
+    warp_fold(box, lane);
+    warp_fold(cb, lane);
+    if (lane == 0) { sbox[w] = box; scb[w] = cb; }
+    __syncthreads();
+    if (w == 0) {
+      if (lane < kFoldWarps) { box = sbox[lane]; cb = scb[lane]; }
+      else { refit_empty(box); refit_empty(cb); }
+      warp_fold(box, lane);
+      warp_fold(cb, lane);
+      if (lane == 0) lvl_plane_finish(a, x, box, cb);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kFoldThreads) lvl_sah_blk(LevelArgs a, const uint32_t* big_list,
+                                                            const DepthTotals* tot) {
+  __shared__ RefitBox sbox[kFoldWarps][kLevelMaxBins];
+  __shared__ int scnt[kFoldWarps][kLevelMaxBins];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t i = blockIdx.x; i < tot->big; i += gridDim.x) {
+    const uint32_t x = big_list[i];
+    if (a.out[x].state != 1) continue;   // the whole block
+    const LevelTask t = a.tasks[x];
+    const uint32_t per = (t.nchunks + kFoldThreads - 1) / kFoldThreads;
+    const uint32_t b = min(t.nchunks, threadIdx.x * per), e = min(t.nchunks, b + per);
+    RefitBox bin_box[kLevelMaxBins];
+    int bin_cnt[kLevelMaxBins];
+    for (int k = 0; k < a.bins; ++k) { refit_empty(bin_box[k]); bin_cnt[k] = 0; }
+    for (uint32_t c = t.chunk0 + b; c < t.chunk0 + e; ++c)
+      for (int k = 0; k < a.bins; ++k) {
+        bin_cnt[k] += a.chunk_cnt[(size_t)c * a.bins + k];
+        refit_grow(bin_box[k], a.chunk_bins[(size_t)c * a.bins + k]);
+      }
+    for (int k = 0; k < a.bins; ++k) {
+      warp_fold(bin_box[k], lane);
+      bin_cnt[k] = warp_sum(bin_cnt[k]);
+      if (lane == 0) { sbox[w][k] = bin_box[k]; scnt[w][k] = bin_cnt[k]; }
+    }
+    __syncthreads();
+    if (w == 0) {
+      for (int k = 0; k < a.bins; ++k) {
+        RefitBox v;
+        int n = 0;
+        if (lane < kFoldWarps) { v = sbox[lane][k]; n = scnt[lane][k]; }
+        else refit_empty(v);
+        warp_fold(v, lane);
+        n = warp_sum(n);
+        bin_box[k] = v;
+        bin_cnt[k] = n;
+      }
+      if (lane == 0) lvl_sah_finish(a, x, bin_box, bin_cnt);
+    }
+    __syncthreads();
+  }
 }
 
 // ── exclusive prefix sums of uint32 counts (three launches) ────────────────────────────────
@@ -243,11 +326,14 @@ __global__ void scan_add(uint32_t* out, uint32_t n, const uint32_t* tile_sums) {
 }
 
 // ── the depth loop's own steps ─────────────────────────────────────────────────────────────
-__global__ void node_chunk_counts(const DevRec* recs, uint32_t begin, uint32_t ntasks, uint32_t* nch) {
+__global__ void node_chunk_counts(const DevRec* recs, uint32_t begin, uint32_t ntasks, uint32_t* nch,
+                                  uint32_t* big_list, DepthTotals* tot) {
   const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= ntasks) return;
   const DevRec r = recs[begin + x];
-  nch[x] = level_node_chunks(r.hi - r.lo);
+  const uint32_t c = level_node_chunks(r.hi - r.lo);
+  nch[x] = c;
+  if (c > kBlockNodeChunks) big_list[atomicAdd(&tot->big, 1u)] = x;
 }
 
 __global__ void node_tasks(const DevRec* recs, uint32_t begin, uint32_t ntasks, const uint32_t* nch,
@@ -394,6 +480,8 @@ struct Arena {
 
 unsigned blocks(size_t n, unsigned per = 128) { return (unsigned)((n + per - 1) / per); }
 
+constexpr unsigned kBigBlocks = 148;   // blocks of lvl_*_blk, each taking listed nodes in turn
+
 struct DeviceLevelBuild {
   uint32_t n = 0;
   int bins = 12;
@@ -411,7 +499,7 @@ struct DeviceLevelBuild {
   NodeOut* out;
   RefitBox *box, *cbox, *bin_box;
   int32_t* bin_cnt;
-  uint32_t *pass, *before, *counts, *offsets, *tile_sums, *med_list, *internal, *pos, *pair, *order;
+  uint32_t *pass, *before, *counts, *offsets, *tile_sums, *med_list, *big_list, *internal, *pos, *pair, *order;
   int64_t *left, *right;
   DepthTotals* tot;
   xb_bvh_node* dnodes;
@@ -429,6 +517,7 @@ struct DeviceLevelBuild {
     A.plan(counts, max_tasks);
     A.plan(offsets, max_tasks);
     A.plan(med_list, max_tasks);
+    A.plan(big_list, n / (kLevelChunk * kBlockNodeChunks) + 2);
     A.plan(tile_sums, blocks(max_tasks, kScanTile));
     A.plan(chunks, max_chunks);
     A.plan(box, max_chunks);
@@ -447,7 +536,7 @@ struct DeviceLevelBuild {
     A.plan(order, n);
     ck(cudaMalloc(&A.base, A.used), "allocate the build's arrays");
     A.place(items); A.place(recs); A.place(tasks); A.place(out); A.place(counts); A.place(offsets);
-    A.place(med_list); A.place(tile_sums); A.place(chunks); A.place(box); A.place(cbox); A.place(bin_box);
+    A.place(med_list); A.place(big_list); A.place(tile_sums); A.place(chunks); A.place(box); A.place(cbox); A.place(bin_box);
     A.place(bin_cnt); A.place(pass); A.place(before); A.place(left); A.place(right); A.place(tot);
     A.place(internal); A.place(pos); A.place(pair); A.place(dnodes); A.place(order);
   }
@@ -483,7 +572,8 @@ struct DeviceLevelBuild {
   uint32_t run_depth(uint32_t begin, uint32_t end) {
     const uint32_t ntasks = end - begin;
     if (ntasks > max_tasks) throw std::runtime_error("device BVH build: depth out of range");
-    node_chunk_counts<<<blocks(ntasks), 128>>>(recs, begin, ntasks, counts);
+    ck(cudaMemset(&tot->big, 0, sizeof(uint32_t)), "clear depth totals");
+    node_chunk_counts<<<blocks(ntasks), 128>>>(recs, begin, ntasks, counts, big_list, tot);
     scan(counts, offsets, ntasks, &tot->chunks);
     const uint32_t nchunks = read_totals().chunks;
     if (nchunks > max_chunks) throw std::runtime_error("device BVH build: chunk count out of range");
@@ -514,8 +604,10 @@ struct DeviceLevelBuild {
       node_chunks<<<blocks(nchunks), 128>>>(tasks, ntasks, nchunks, chunks);
       lvl_bounds<<<blocks(nchunks), 128>>>(a);
       lvl_plane_w<<<warps, 128>>>(a);
+      lvl_plane_blk<<<kBigBlocks, kFoldThreads>>>(a, big_list, tot);
       lvl_bins<<<blocks(nchunks), 128>>>(a);
       lvl_sah_w<<<warps, 128>>>(a);
+      lvl_sah_blk<<<kBigBlocks, kFoldThreads>>>(a, big_list, tot);
       lvl_pass<<<blocks(nchunks), 128>>>(a);
       lvl_prefix_w<<<warps, 128>>>(a);
       lvl_rank<<<blocks(nchunks), 128>>>(a);
